@@ -1,0 +1,267 @@
+/*
+ * nicp_gpu.h -- C ABI of the B200-native NICP registration path.
+ *
+ * One shared library (libnicp_b200.so, sm_100a) implements the yorsh87/nicp
+ * depth -> cloud -> projective-ICP path with hand-written CUDA kernels.  The
+ * reference's C++ plugin classes map onto these entry points (the header
+ * include/nicp_b200/nicp.hpp re-exposes them under the reference's class
+ * names):
+ *
+ *   reference (file:line inside yorsh87/nicp)            entry point here
+ *   -------------------------------------------------------------------------
+ *   DepthImageConverterIntegralImage::compute             nicp_cloud_from_depth_u16
+ *     (nicp/nicp/depthimageconverterintegralimage.cpp:18-64)  nicp_cloud_from_depth_f32
+ *     + DepthImage_convert_16UC1_to_32FC1 (imageutils.cpp:85-99)
+ *   PinholePointProjector::unProject                      nicp_unproject
+ *     (nicp/nicp/pinholepointprojector.cpp:68-91)
+ *   PinholePointProjector::projectIntervals               nicp_project_intervals
+ *     (nicp/nicp/pinholepointprojector.cpp:136-148)
+ *   PinholePointProjector::project                        nicp_project
+ *     (nicp/nicp/pinholepointprojector.cpp:33-66)
+ *   PinholePointProjector::_updateMatrices                nicp_projector_matrices
+ *     (nicp/nicp/pinholepointprojector.cpp:16-31)
+ *   CorrespondenceFinderProjective::compute               nicp_correspond
+ *     (nicp/nicp/correspondencefinderprojective.cpp:16-115)
+ *   Linearizer::update                                    nicp_linearize
+ *     (nicp/nicp/linearizer.cpp:21-134)
+ *   AlignerProjective::align (+ Aligner::_computeStatistics)   nicp_align
+ *     (nicp/nicp/alignerprojective.cpp:21-136, aligner.cpp:82-135)
+ *   Cloud accessors / transformInPlace                    nicp_cloud_download / _upload /
+ *     (nicp/nicp/cloud.h:20-193, cloud.cpp:191-204)         nicp_cloud_transform
+ *   (no counterpart: many pairs in one device-side loop)  nicp_build_batch / nicp_align_batch
+ *
+ * Conventions
+ *   - Every function returns an int status (NICP_OK on success); the text of
+ *     the last failure on a context is nicp_ctx_last_error().  No C++
+ *     exception crosses this boundary.
+ *   - Matrices are row-major.  Transforms are 4x4 isometries; row 3 is
+ *     forced to (0 0 0 1) as the reference does.
+ *   - Host buffers are caller-owned; device buffers (clouds, scratch) are
+ *     owned by the library.  Calls on one context are ordered on its CUDA
+ *     stream; functions that return data in host memory synchronize it.
+ *   - There is no CPU fallback: creating a context fails on a host without
+ *     an sm_100 GPU.
+ *   - A context is not thread-safe: use one per host thread.
+ */
+#ifndef NICP_GPU_H
+#define NICP_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NICP_API_VERSION 1
+
+enum {
+  NICP_OK = 0,
+  NICP_EINVAL = 1,   /* bad argument (null, size, range)                 */
+  NICP_ENOMEM = 2,   /* device or host allocation failed                 */
+  NICP_EBUDGET = 3,  /* request exceeds the configured HBM budget        */
+  NICP_ETIMEOUT = 4, /* a bounded device-side wait ran out               */
+  NICP_ECUDA = 5,    /* CUDA runtime error (text in nicp_ctx_last_error) */
+  NICP_ESTATE = 6    /* call not valid in the object's current state     */
+};
+
+typedef struct nicp_ctx nicp_ctx;
+typedef struct nicp_cloud nicp_cloud;
+
+/* PinholePointProjector state (pinholepointprojector.cpp:5-31,150-155;
+ * pointprojector.cpp:6-15,106-112; defaults from those constructors).  The
+ * effective camera matrix is (fx, fy, cx, cy) with its first two rows times
+ * `scaling`; the projection image is (rows, cols) times `scaling`. */
+typedef struct {
+  float fx, fy, cx, cy;
+  float scaling;
+  int rows, cols;
+  float min_distance, max_distance;
+  float baseline, alpha;
+} nicp_camera;
+
+enum { NICP_MOMENTS_F64 = 0, NICP_MOMENTS_F32 = 1, NICP_MOMENTS_TWOFLOAT = 2 };
+
+/* StatsCalculatorIntegralImage (statscalculatorintegralimage.cpp:12-18) and
+ * Point/NormalInformationMatrixCalculator (informationmatrixcalculator.h:
+ * 22-29,115-119,150-155) settings, plus the depth scale of the u16 input. */
+typedef struct {
+  float depth_scale;
+  float world_radius;
+  int min_image_radius, max_image_radius, min_points;
+  float curvature_threshold;
+  float pim_flat[3], pim_nonflat[3];
+  float pim_curvature_threshold;
+  float nim_flat[3], nim_nonflat[3];
+  float nim_curvature_threshold;
+  int moments_precision; /* NICP_MOMENTS_*; F64 is the default */
+  int keep_stats;        /* also store eigenvalues/eigenvectors per point */
+} nicp_cloud_params;
+
+/* CorrespondenceFinder(Projective) (correspondencefinder.cpp:9-18). */
+typedef struct {
+  float inlier_distance_threshold;
+  float inlier_normal_angular_threshold; /* cosine, default cosf(M_PI/6) */
+  float flat_curvature_threshold;
+  float inlier_curvature_ratio_threshold;
+  int demoted_to_gicp;
+  /* Emulates the reference's OpenMP partition with this many threads:
+   * the last rows % T image rows and the last K % T correspondences are
+   * skipped exactly as the reference skips them.  1 (default) = no drops. */
+  int parity_threads;
+} nicp_corr_params;
+
+/* Linearizer (linearizer.cpp:9-19). */
+typedef struct {
+  float inlier_max_chi2;
+  int robust_kernel;
+  int z_scaling;
+  float scale;
+  int demoted_to_gicp;
+} nicp_lin_params;
+
+/* Aligner (aligner.cpp:21-41) plus the device-loop controls. */
+typedef struct {
+  int outer_iterations, inner_iterations;
+  float lambda;
+  int min_inliers;
+  float translational_min_eigen_ratio, rotational_min_eigen_ratio;
+  int compute_statistics; /* run Aligner::_computeStatistics after the loop */
+  /* Stop a pair once the pose change of an outer iteration is below this
+   * (max-abs over translation and quaternion-vector parts).  0 = never,
+   * which is the reference's behaviour. */
+  double early_exit_eps;
+} nicp_align_params;
+
+typedef struct {
+  double T[16];          /* current -> reference */
+  float error;           /* Linearizer::error() of the last inner iteration */
+  int inliers;           /* Linearizer::inliers() of the last inner iteration */
+  int num_correspondences;
+  int outer_iterations_run;
+  double translational_ratio, rotational_ratio;
+  int solution_valid;    /* -1 when statistics were not computed */
+  int status;            /* NICP_OK or a per-pair error */
+} nicp_align_result;
+
+void nicp_default_camera(nicp_camera *c);
+void nicp_default_cloud_params(nicp_cloud_params *p);
+void nicp_default_corr_params(nicp_corr_params *p);
+void nicp_default_lin_params(nicp_lin_params *p);
+void nicp_default_align_params(nicp_align_params *p);
+
+/* ------------------------------------------------------------ context */
+/* stream: a cudaStream_t to run on, or NULL for a stream the context owns. */
+int nicp_ctx_create(int device, void *stream, nicp_ctx **out);
+int nicp_ctx_destroy(nicp_ctx *ctx);
+const char *nicp_ctx_last_error(const nicp_ctx *ctx);
+int nicp_ctx_synchronize(nicp_ctx *ctx);
+void *nicp_ctx_stream(nicp_ctx *ctx);
+/* Bytes of device memory currently held by the context and its clouds. */
+size_t nicp_ctx_device_bytes(const nicp_ctx *ctx);
+
+/* Per-kernel timing with CUDA events on the context stream.  When enabled,
+ * every launch of the kernels below is bracketed by events; reading
+ * synchronizes and resets the counters. */
+enum {
+  NICP_K_UNPROJECT = 0, NICP_K_MOMENTS_ROWS, NICP_K_MOMENTS_COLS, NICP_K_STATS,
+  NICP_K_ZBUFFER, NICP_K_RESOLVE, NICP_K_CORR_LIN, NICP_K_CORR_LIST, NICP_K_LIN_LIST,
+  NICP_K_SOLVE, NICP_K_TRANSFORM, NICP_K_COUNT
+};
+int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable);
+/* Kernels this context has launched so far (graph replays included). */
+unsigned long long nicp_ctx_kernel_launches(const nicp_ctx *ctx);
+int nicp_ctx_read_profile(nicp_ctx *ctx, int kernel, double *total_ms, int *launches);
+const char *nicp_kernel_name(int kernel);
+
+/* --------------------------------------------------------------- clouds */
+int nicp_cloud_create(nicp_ctx *ctx, nicp_cloud **out);
+int nicp_cloud_destroy(nicp_cloud *c);
+/* Number of points (synchronizes). */
+int nicp_cloud_size(nicp_cloud *c, int *n);
+/* Any output may be NULL.  points4/normals4: n*4 floats (w = 1 / 0);
+ * curvature: n; omega_p9/omega_n9: n*9 (3x3 blocks); eigval3: n*3;
+ * eigvec9: n*9 (columns are eigenvectors; needs keep_stats). */
+int nicp_cloud_download(nicp_cloud *c, float *points4, float *normals4, float *curvature,
+                        float *omega_p9, float *omega_n9, float *eigval3, float *eigvec9);
+int nicp_cloud_upload(nicp_cloud *c, int n, const float *points4, const float *normals4,
+                      const float *curvature, const float *omega_p9, const float *omega_n9);
+/* Cloud::transformInPlace (cloud.cpp:191-204). */
+int nicp_cloud_transform(nicp_cloud *c, const float T16[16]);
+
+/* DepthImageConverterIntegralImage::compute.  depth: rows x cols u16 with
+ * row pitch `pitch_bytes` (0 = packed), in host memory or, when
+ * depth_on_device != 0, in device memory.  sensor_offset may be NULL
+ * (identity).  index_out: optional host rows*cols int32 index image. */
+int nicp_cloud_from_depth_u16(nicp_ctx *ctx, const uint16_t *depth, int rows, int cols,
+                              size_t pitch_bytes, int depth_on_device, const nicp_camera *cam,
+                              const nicp_cloud_params *prm, const float *sensor_offset,
+                              nicp_cloud *out, int32_t *index_out);
+/* Same from a float depth image in metres (DepthImage). */
+int nicp_cloud_from_depth_f32(nicp_ctx *ctx, const float *depth, int rows, int cols,
+                              size_t pitch_bytes, int depth_on_device, const nicp_camera *cam,
+                              const nicp_cloud_params *prm, const float *sensor_offset,
+                              nicp_cloud *out, int32_t *index_out);
+
+/* ------------------------------------------------------------ projector */
+/* KRt and iKRt for projector transform T (both 4x4 row-major floats). */
+int nicp_projector_matrices(const nicp_camera *cam, const float T16[16], float KRt16[16],
+                            float iKRt16[16]);
+/* PinholePointProjector::unProject from a float depth image (host).
+ * points4_out: rows*cols*4 floats capacity; returns the count in *n. */
+int nicp_unproject(nicp_ctx *ctx, const float *depth, int rows, int cols, const nicp_camera *cam,
+                   const float T16[16], float *points4_out, int32_t *index_out, int *n);
+/* PinholePointProjector::projectIntervals: radius image (both Vec2i
+ * components are equal; -1 outside the depth range). */
+int nicp_project_intervals(nicp_ctx *ctx, const float *depth, int rows, int cols,
+                           const nicp_camera *cam, float world_radius, int32_t *radius_out);
+/* PinholePointProjector::project: z-buffer of the cloud seen from T into
+ * the (scaled) rows x cols image.  Host outputs; either may be NULL. */
+int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_camera *cam,
+                 const float T16[16], int32_t *index_out, float *depth_out);
+
+/* ------------------------------------------------- correspondences, H, b */
+/* CorrespondenceFinderProjective::compute with the given index images (host,
+ * rows x cols) and T (the aligner passes _T.inverse()).  pairs_out: host,
+ * capacity 2*rows*cols int32 (reference index, current index), row-major
+ * order.  *num_out = numCorrespondences(). */
+int nicp_correspond(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur,
+                    const int32_t *ref_index, const int32_t *cur_index, int rows, int cols,
+                    const float T16[16], const nicp_corr_params *prm, int32_t *pairs_out,
+                    int *num_out);
+/* Linearizer::update over a host correspondence list.  H36 is the full 6x6
+ * (H(3:6,0:3) = Htr^T, as the reference assembles it); the sums are
+ * accumulated in FP64.  parity_threads: the reference's K % T drop (1 = none). */
+int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur,
+                   const int32_t *pairs, int num_pairs, const float T16[16],
+                   const nicp_lin_params *prm, int parity_threads, double H36[36], double b6[6],
+                   double *error, int *inliers);
+
+/* -------------------------------------------------------------- aligner */
+/* AlignerProjective::align for one pair (one call, one pair).  guess,
+ * ref_offset, cur_offset may be NULL (identity). */
+int nicp_align(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const nicp_camera *cam,
+               const float guess16[16], const float ref_offset16[16], const float cur_offset16[16],
+               const nicp_corr_params *corr, const nicp_lin_params *lin,
+               const nicp_align_params *prm, nicp_align_result *out);
+
+/* ------------------------------------------------------------- batching */
+/* Builds n clouds in one pass of launches.  depth[i]: packed rows[i] x
+ * cols[i] u16 frames (host, or device when depth_on_device != 0). */
+int nicp_build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *rows,
+                     const int *cols, int depth_on_device, const nicp_camera *cams,
+                     const nicp_cloud_params *prm, nicp_cloud *const *out);
+/* Aligns n independent pairs in one device-side Gauss-Newton loop (all
+ * outer x inner iterations captured as one CUDA graph, 6x6 solves on the
+ * device, per-pair early exit).  guesses: n*16 floats or NULL.  Results are
+ * independent of batch composition: every pair's sums use a fixed tile
+ * order. */
+int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs,
+                     const nicp_cloud *const *curs, const nicp_camera *cams, const float *guesses,
+                     const nicp_corr_params *corr, const nicp_lin_params *lin,
+                     const nicp_align_params *prm, nicp_align_result *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1106 @@
+// capi.cu -- the C ABI of include/nicp_gpu.h: contexts, device clouds, the
+// workspace, frame and pair batching, CUDA-graph capture of the Gauss-Newton
+// loop, and the host side of Aligner::align.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "host_math.hpp"
+#include "kernels.hpp"
+#include "nicp_gpu.h"
+
+using namespace nicp;
+
+namespace {
+
+struct GraphEntry {
+  std::string key;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long kernels = 0;
+  std::vector<Profiler::Rec> recs;
+};
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Offsets into one device allocation, assigned in two passes (size, then place).
+struct Layout {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    off = align_up(off, 256);
+    size_t r = off;
+    off += bytes;
+    return r;
+  }
+};
+
+}  // namespace
+
+struct nicp_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  Profiler prof;
+  char *ws = nullptr;
+  size_t ws_cap = 0;
+  char *pin_up = nullptr;
+  size_t pin_up_cap = 0;
+  cudaEvent_t pin_up_ev = nullptr;
+  char *pin_down = nullptr;
+  size_t pin_down_cap = 0;
+  size_t cloud_bytes = 0;
+  std::vector<GraphEntry> graphs;
+  nicp_cloud *scratch_cloud = nullptr;
+};
+
+struct nicp_cloud {
+  nicp_ctx *ctx = nullptr;
+  char *mem = nullptr;
+  size_t bytes = 0;
+  int capacity = 0;  // points
+  int rows = 0, cols = 0;
+  bool has_eig = false;
+  float4 *pts = nullptr, *nrm = nullptr, *omg = nullptr;
+  float *eig = nullptr;
+  int *count = nullptr;
+  int32_t *index = nullptr;
+};
+
+// ------------------------------------------------------------------ helpers
+static int fail(nicp_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+#define CK(ctx, call)                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return fail((ctx), NICP_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+static int ensure_ws(nicp_ctx *ctx, size_t bytes) {
+  if (bytes <= ctx->ws_cap) return NICP_OK;
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  for (auto &g : ctx->graphs) cudaGraphExecDestroy(g.exec);
+  ctx->graphs.clear();
+  if (ctx->ws) cudaFree(ctx->ws);
+  ctx->ws = nullptr;
+  ctx->ws_cap = 0;
+  size_t cap = align_up(bytes + bytes / 4, 1 << 20);
+  if (cudaMalloc(&ctx->ws, cap) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, NICP_ENOMEM, "workspace allocation of " + std::to_string(cap) + " bytes failed");
+  }
+  ctx->ws_cap = cap;
+  return NICP_OK;
+}
+
+// Pinned upload staging: waits until the previous upload has been consumed.
+static int pin_up(nicp_ctx *ctx, size_t bytes, char **out) {
+  CK(ctx, cudaEventSynchronize(ctx->pin_up_ev));
+  if (bytes > ctx->pin_up_cap) {
+    if (ctx->pin_up) cudaFreeHost(ctx->pin_up);
+    ctx->pin_up = nullptr;
+    size_t cap = align_up(bytes + bytes / 4, 1 << 16);
+    CK(ctx, cudaMallocHost(&ctx->pin_up, cap));
+    ctx->pin_up_cap = cap;
+  }
+  *out = ctx->pin_up;
+  return NICP_OK;
+}
+
+static int pin_down(nicp_ctx *ctx, size_t bytes, char **out) {
+  if (bytes > ctx->pin_down_cap) {
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->pin_down) cudaFreeHost(ctx->pin_down);
+    ctx->pin_down = nullptr;
+    size_t cap = align_up(bytes + bytes / 4, 1 << 16);
+    CK(ctx, cudaMallocHost(&ctx->pin_down, cap));
+    ctx->pin_down_cap = cap;
+  }
+  *out = ctx->pin_down;
+  return NICP_OK;
+}
+
+static int cloud_reserve(nicp_cloud *c, int capacity, int rows, int cols, bool eig) {
+  nicp_ctx *ctx = c->ctx;
+  size_t P = (size_t)rows * cols;
+  if (capacity < 1) capacity = 1;
+  if (capacity <= c->capacity && P <= (size_t)c->rows * c->cols && (!eig || c->has_eig)) {
+    c->rows = rows;
+    c->cols = cols;
+    return NICP_OK;
+  }
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  if (c->mem) {
+    cudaFree(c->mem);
+    ctx->cloud_bytes -= c->bytes;
+  }
+  c->mem = nullptr;
+  Layout L;
+  size_t o_pts = L.take(16 * (size_t)capacity), o_nrm = L.take(16 * (size_t)capacity);
+  size_t o_omg = L.take(48 * (size_t)capacity);
+  size_t o_eig = eig ? L.take(48 * (size_t)capacity) : 0;
+  size_t o_cnt = L.take(sizeof(int));
+  size_t o_idx = L.take(4 * std::max<size_t>(P, 1));
+  if (cudaMalloc(&c->mem, L.off) != cudaSuccess) {
+    cudaGetLastError();
+    c->capacity = 0;
+    return fail(ctx, NICP_ENOMEM, "cloud allocation failed");
+  }
+  c->bytes = L.off;
+  ctx->cloud_bytes += c->bytes;
+  c->capacity = capacity;
+  c->rows = rows;
+  c->cols = cols;
+  c->has_eig = eig;
+  c->pts = (float4 *)(c->mem + o_pts);
+  c->nrm = (float4 *)(c->mem + o_nrm);
+  c->omg = (float4 *)(c->mem + o_omg);
+  c->eig = eig ? (float *)(c->mem + o_eig) : nullptr;
+  c->count = (int *)(c->mem + o_cnt);
+  c->index = (int32_t *)(c->mem + o_idx);
+  CK(ctx, cudaMemsetAsync(c->count, 0, sizeof(int), ctx->stream));
+  return NICP_OK;
+}
+
+static bool valid_camera(const nicp_camera *c) {
+  return c && c->rows > 0 && c->cols > 0 && c->scaling > 0 && std::isfinite(c->fx) && std::isfinite(c->fy) &&
+         cam_rows(*c) > 0 && cam_cols(*c) > 0;
+}
+
+static CorrParams corr_params(const nicp_corr_params &p) {
+  CorrParams c;
+  c.sq_thr = p.inlier_distance_threshold * p.inlier_distance_threshold;
+  c.cos_thr = p.inlier_normal_angular_threshold;
+  c.flat_thr = p.flat_curvature_threshold;
+  c.min_ratio = 1.0f / p.inlier_curvature_ratio_threshold;
+  c.max_ratio = p.inlier_curvature_ratio_threshold;
+  c.demoted = p.demoted_to_gicp;
+  c.row_limit_threads = std::max(1, p.parity_threads);
+  return c;
+}
+
+static LinParams lin_params(const nicp_lin_params &p) {
+  LinParams l;
+  l.max_chi2 = p.inlier_max_chi2;
+  l.robust = p.robust_kernel;
+  l.z_scaling = p.z_scaling;
+  l.scale = p.scale;
+  l.demoted = p.demoted_to_gicp;
+  return l;
+}
+
+static void rows12(const HM4 &M, float *o) {
+  for (int i = 0; i < 12; i++) o[i] = M.a[i];
+}
+
+// ------------------------------------------------------------------ defaults
+extern "C" void nicp_default_camera(nicp_camera *c) {
+  // PinholePointProjector() and PointProjector() constructors
+  c->fx = 1.0f; c->fy = 1.0f; c->cx = 0.5f; c->cy = 0.5f;
+  c->scaling = 1.0f;
+  c->rows = 0; c->cols = 0;
+  c->min_distance = 0.01f; c->max_distance = 6.0f;
+  c->baseline = 0.075f; c->alpha = 0.1f;
+}
+
+extern "C" void nicp_default_cloud_params(nicp_cloud_params *p) {
+  p->depth_scale = 0.001f;
+  p->world_radius = 0.1f;
+  p->min_image_radius = 10; p->max_image_radius = 30; p->min_points = 50;
+  p->curvature_threshold = 0.02f;
+  const float pf[3] = {1000.0f, 0.001f, 0.001f}, pn[3] = {1.0f, 0.1f, 0.1f};
+  const float nf[3] = {1000.0f, 0.001f, 0.001f}, nn[3] = {0.1f, 1.0f, 1.0f};
+  for (int i = 0; i < 3; i++) {
+    p->pim_flat[i] = pf[i]; p->pim_nonflat[i] = pn[i];
+    p->nim_flat[i] = nf[i]; p->nim_nonflat[i] = nn[i];
+  }
+  p->pim_curvature_threshold = 0.02f;
+  p->nim_curvature_threshold = 0.02f;
+  p->moments_precision = NICP_MOMENTS_F64;
+  p->keep_stats = 0;
+}
+
+extern "C" void nicp_default_corr_params(nicp_corr_params *p) {
+  p->inlier_distance_threshold = 1.0f;
+  p->inlier_normal_angular_threshold = cosf((float)(M_PI / 6));
+  p->flat_curvature_threshold = 0.2f;
+  p->inlier_curvature_ratio_threshold = 1.3f;
+  p->demoted_to_gicp = 0;
+  p->parity_threads = 1;
+}
+
+extern "C" void nicp_default_lin_params(nicp_lin_params *p) {
+  p->inlier_max_chi2 = 9e3f;
+  p->robust_kernel = 1;
+  p->z_scaling = 0;
+  p->scale = 1.0f;
+  p->demoted_to_gicp = 0;
+}
+
+extern "C" void nicp_default_align_params(nicp_align_params *p) {
+  p->outer_iterations = 10;
+  p->inner_iterations = 1;
+  p->lambda = 1e3f;
+  p->min_inliers = 100;
+  p->translational_min_eigen_ratio = 50.0f;
+  p->rotational_min_eigen_ratio = 50.0f;
+  p->compute_statistics = 1;
+  p->early_exit_eps = 0.0;
+}
+
+// ------------------------------------------------------------------ context
+extern "C" int nicp_ctx_create(int device, void *stream, nicp_ctx **out) {
+  if (!out) return NICP_EINVAL;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return NICP_ECUDA;
+  }
+  if (device < 0 || device >= n) return NICP_EINVAL;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) return NICP_ECUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return NICP_ECUDA;
+  auto *ctx = new nicp_ctx();
+  ctx->device = device;
+  if (stream) {
+    ctx->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete ctx;
+      return NICP_ECUDA;
+    }
+    ctx->own_stream = true;
+  }
+  if (cudaEventCreateWithFlags(&ctx->pin_up_ev, cudaEventDisableTiming) != cudaSuccess) {
+    delete ctx;
+    return NICP_ECUDA;
+  }
+  *out = ctx;
+  return NICP_OK;
+}
+
+extern "C" int nicp_ctx_destroy(nicp_ctx *ctx) {
+  if (!ctx) return NICP_EINVAL;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->scratch_cloud) nicp_cloud_destroy(ctx->scratch_cloud);
+  for (auto &g : ctx->graphs) cudaGraphExecDestroy(g.exec);
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->pin_up) cudaFreeHost(ctx->pin_up);
+  if (ctx->pin_down) cudaFreeHost(ctx->pin_down);
+  cudaEventDestroy(ctx->pin_up_ev);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return NICP_OK;
+}
+
+extern "C" const char *nicp_ctx_last_error(const nicp_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+extern "C" int nicp_ctx_synchronize(nicp_ctx *ctx) {
+  if (!ctx) return NICP_EINVAL;
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return NICP_OK;
+}
+
+extern "C" void *nicp_ctx_stream(nicp_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" size_t nicp_ctx_device_bytes(const nicp_ctx *ctx) { return ctx ? ctx->ws_cap + ctx->cloud_bytes : 0; }
+
+extern "C" int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable) {
+  if (!ctx) return NICP_EINVAL;
+  ctx->prof.enabled = enable != 0;
+  ctx->prof.recs.clear();
+  ctx->prof.next = 0;
+  return NICP_OK;
+}
+
+extern "C" int nicp_ctx_read_profile(nicp_ctx *ctx, int kernel, double *total_ms, int *launches) {
+  if (!ctx || kernel < 0 || kernel >= NICP_K_COUNT) return NICP_EINVAL;
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  double t = 0;
+  int n = 0;
+  std::vector<Profiler::Rec> keep;
+  for (auto &r : ctx->prof.recs) {
+    if (r.kernel != kernel) {
+      keep.push_back(r);
+      continue;
+    }
+    float ms = 0;
+    CK(ctx, cudaEventElapsedTime(&ms, r.a, r.b));
+    t += ms;
+    n += r.nkernels;
+  }
+  ctx->prof.recs.swap(keep);
+  if (ctx->prof.recs.empty()) ctx->prof.next = 0;
+  if (total_ms) *total_ms = t;
+  if (launches) *launches = n;
+  return NICP_OK;
+}
+
+extern "C" unsigned long long nicp_ctx_kernel_launches(const nicp_ctx *ctx) { return ctx ? ctx->prof.launches : 0; }
+
+extern "C" const char *nicp_kernel_name(int k) {
+  static const char *names[NICP_K_COUNT] = {"unproject", "moments_rows", "moments_cols", "stats_omega",
+                                            "zbuffer",   "resolve",      "corr_lin",     "corr_list",
+                                            "lin_list",  "solve",        "transform"};
+  return (k >= 0 && k < NICP_K_COUNT) ? names[k] : "?";
+}
+
+// ------------------------------------------------------------------ clouds
+extern "C" int nicp_cloud_create(nicp_ctx *ctx, nicp_cloud **out) {
+  if (!ctx || !out) return NICP_EINVAL;
+  auto *c = new nicp_cloud();
+  c->ctx = ctx;
+  *out = c;
+  return NICP_OK;
+}
+
+extern "C" int nicp_cloud_destroy(nicp_cloud *c) {
+  if (!c) return NICP_EINVAL;
+  if (c->mem) {
+    cudaStreamSynchronize(c->ctx->stream);
+    cudaFree(c->mem);
+    c->ctx->cloud_bytes -= c->bytes;
+  }
+  delete c;
+  return NICP_OK;
+}
+
+extern "C" int nicp_cloud_size(nicp_cloud *c, int *n) {
+  if (!c || !n) return NICP_EINVAL;
+  if (!c->mem) { *n = 0; return NICP_OK; }
+  nicp_ctx *ctx = c->ctx;
+  CK(ctx, cudaMemcpyAsync(n, c->count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return NICP_OK;
+}
+
+extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *curv, float *op9, float *on9, float *ev3,
+                                   float *U9) {
+  if (!c) return NICP_EINVAL;
+  nicp_ctx *ctx = c->ctx;
+  int n = 0;
+  int rc = nicp_cloud_size(c, &n);
+  if (rc) return rc;
+  if (n == 0) return NICP_OK;
+  if ((ev3 || U9) && !c->has_eig) return fail(ctx, NICP_ESTATE, "cloud was built without keep_stats");
+  std::vector<float4> nrm(n), omg(3 * (size_t)n);
+  std::vector<float> eig;
+  if (p4) CK(ctx, cudaMemcpyAsync(p4, c->pts, 16 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaMemcpyAsync(nrm.data(), c->nrm, 16 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaMemcpyAsync(omg.data(), c->omg, 48 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (ev3 || U9) {
+    eig.resize(12 * (size_t)n);
+    CK(ctx, cudaMemcpyAsync(eig.data(), c->eig, 48 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < n; i++) {
+    if (n4) { n4[4 * i] = nrm[i].x; n4[4 * i + 1] = nrm[i].y; n4[4 * i + 2] = nrm[i].z; n4[4 * i + 3] = 0.0f; }
+    if (curv) curv[i] = nrm[i].w;
+    const float *o = reinterpret_cast<const float *>(&omg[3 * (size_t)i]);
+    // (Op00 Op01 Op02 Op11)(Op12 Op22 On00 On01)(On02 On11 On12 On22)
+    if (op9) {
+      float *d = op9 + 9 * (size_t)i;
+      d[0] = o[0]; d[1] = o[1]; d[2] = o[2]; d[3] = o[1]; d[4] = o[3]; d[5] = o[4]; d[6] = o[2]; d[7] = o[4]; d[8] = o[5];
+    }
+    if (on9) {
+      float *d = on9 + 9 * (size_t)i;
+      d[0] = o[6]; d[1] = o[7]; d[2] = o[8]; d[3] = o[7]; d[4] = o[9]; d[5] = o[10]; d[6] = o[8]; d[7] = o[10]; d[8] = o[11];
+    }
+    if (ev3) for (int k = 0; k < 3; k++) ev3[3 * (size_t)i + k] = eig[12 * (size_t)i + k];
+    if (U9) for (int k = 0; k < 9; k++) U9[9 * (size_t)i + k] = eig[12 * (size_t)i + 3 + k];
+  }
+  return NICP_OK;
+}
+
+extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const float *n4, const float *curv,
+                                 const float *op9, const float *on9) {
+  if (!c || n < 0 || (n > 0 && (!p4 || !n4 || !curv))) return NICP_EINVAL;
+  nicp_ctx *ctx = c->ctx;
+  int rc = cloud_reserve(c, n, c->rows, c->cols, false);
+  if (rc) return rc;
+  std::vector<float4> pts(n), nrm(n), omg(3 * (size_t)n);
+  for (int i = 0; i < n; i++) {
+    pts[i] = make_float4(p4[4 * i], p4[4 * i + 1], p4[4 * i + 2], 1.0f);
+    nrm[i] = make_float4(n4[4 * i], n4[4 * i + 1], n4[4 * i + 2], curv[i]);
+    float o[12] = {0};
+    if (op9) { const float *s = op9 + 9 * (size_t)i; o[0] = s[0]; o[1] = s[1]; o[2] = s[2]; o[3] = s[4]; o[4] = s[5]; o[5] = s[8]; }
+    if (on9) { const float *s = on9 + 9 * (size_t)i; o[6] = s[0]; o[7] = s[1]; o[8] = s[2]; o[9] = s[4]; o[10] = s[5]; o[11] = s[8]; }
+    std::memcpy(&omg[3 * (size_t)i], o, sizeof(o));
+  }
+  if (n > 0) {
+    CK(ctx, cudaMemcpyAsync(c->pts, pts.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(c->nrm, nrm.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(c->omg, omg.data(), 48 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CK(ctx, cudaMemcpyAsync(c->count, &n, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return NICP_OK;
+}
+
+extern "C" int nicp_cloud_transform(nicp_cloud *c, const float T16[16]) {
+  if (!c || !T16) return NICP_EINVAL;
+  nicp_ctx *ctx = c->ctx;
+  if (!c->mem) return NICP_OK;
+  HM4 m = HM4::from(T16);
+  bool ident = true;
+  HM4 I = HM4::identity();
+  for (int i = 0; i < 16; i++) ident = ident && (m.a[i] == I.a[i]);
+  if (ident) return NICP_OK;  // cloud.cpp:194
+  char *pin;
+  int rc = pin_up(ctx, 64, &pin);
+  if (rc) return rc;
+  rows12(m, (float *)pin);
+  Layout L;
+  size_t o = L.take(48);
+  if ((rc = ensure_ws(ctx, L.off))) return rc;
+  CK(ctx, cudaMemcpyAsync(ctx->ws + o, pin, 48, cudaMemcpyHostToDevice, ctx->stream));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, ctx->stream));
+  launch_cloud_transform(c->pts, c->nrm, c->omg, c->has_eig ? c->eig : nullptr, c->count, c->capacity,
+                         (const float *)(ctx->ws + o), ctx->stream, &ctx->prof);
+  CK(ctx, cudaGetLastError());
+  return NICP_OK;
+}
+
+// ------------------------------------------------------------------ cloud build
+namespace {
+struct FrameIn {
+  const void *depth;
+  bool u16;
+  bool on_device;
+  size_t pitch;
+  int rows, cols;
+  const float *transform;  // projector transform for the unprojection (null = identity)
+};
+}  // namespace
+
+// Builds clouds for frames [0, n) in chunks that bound the integral-image scratch.
+static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_camera *cams, const nicp_cloud_params *prm,
+                        nicp_cloud *const *clouds, bool unproject_only) {
+  cudaStream_t s = ctx->stream;
+  const size_t msz = moment_bytes(prm->moments_precision);
+  const size_t kChunkMoments = (size_t)3 << 30;  // bytes of integral image per chunk
+  int rc;
+  for (int i = 0; i < n; i++) {
+    if (!fin[i].depth || fin[i].rows <= 0 || fin[i].cols <= 0 || !clouds[i] || !valid_camera(&cams[i]))
+      return fail(ctx, NICP_EINVAL, "bad frame " + std::to_string(i));
+    if ((long long)fin[i].rows * fin[i].cols > (1ll << 30)) return fail(ctx, NICP_EINVAL, "frame too large");
+    if ((rc = cloud_reserve(clouds[i], fin[i].rows * fin[i].cols, fin[i].rows, fin[i].cols, prm->keep_stats != 0)))
+      return rc;
+  }
+  int i0 = 0;
+  while (i0 < n) {
+    int i1 = i0;
+    size_t mom = 0;
+    while (i1 < n) {
+      size_t m = (size_t)fin[i1].rows * fin[i1].cols * 10 * msz;
+      if (i1 > i0 && mom + m > kChunkMoments) break;
+      mom += m;
+      i1++;
+    }
+    int nf = i1 - i0;
+    Layout L;
+    std::vector<size_t> o_stage(nf, 0), o_tiles(nf), o_mom(nf);
+    size_t o_frames = L.take(sizeof(FrameDev) * nf);
+    for (int k = 0; k < nf; k++) {
+      const FrameIn &f = fin[i0 + k];
+      size_t P = (size_t)f.rows * f.cols;
+      size_t esz = f.u16 ? 2 : 4;
+      bool packed = f.pitch == 0 || f.pitch == f.cols * esz;
+      bool aligned = ((uintptr_t)f.depth & 15) == 0;
+      if (!f.on_device || !packed || !aligned) o_stage[k] = L.take(P * esz) + 1;  // +1: "staged"
+      o_tiles[k] = L.take(4 * ((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
+      o_mom[k] = unproject_only ? 0 : L.take(P * 10 * msz);
+    }
+    if ((rc = ensure_ws(ctx, L.off))) return rc;
+    char *pin;
+    if ((rc = pin_up(ctx, sizeof(FrameDev) * nf, &pin))) return rc;
+    FrameDev *fd = reinterpret_cast<FrameDev *>(pin);
+    int tiles = 0, rowsum = 0, stiles = 0, colctas = 0;
+    for (int k = 0; k < nf; k++) {
+      const FrameIn &f = fin[i0 + k];
+      const nicp_camera &cam = cams[i0 + k];
+      nicp_cloud *cl = clouds[i0 + k];
+      size_t P = (size_t)f.rows * f.cols;
+      size_t esz = f.u16 ? 2 : 4;
+      const void *src = f.depth;
+      if (o_stage[k]) {
+        char *dst = ctx->ws + (o_stage[k] - 1);
+        size_t pitch = f.pitch ? f.pitch : f.cols * esz;
+        CK(ctx, cudaMemcpy2DAsync(dst, f.cols * esz, f.depth, pitch, f.cols * esz, f.rows,
+                                  f.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        src = dst;
+      }
+      FrameDev &d = fd[k];
+      std::memset(&d, 0, sizeof(d));
+      d.depth_u16 = f.u16 ? (const uint16_t *)src : nullptr;
+      d.depth_f32 = f.u16 ? nullptr : (const float *)src;
+      d.rows = f.rows;
+      d.cols = f.cols;
+      d.tile_base = tiles;
+      d.row_base = rowsum;
+      d.stat_tile_base = stiles;
+      d.col_base = colctas;
+      tiles += (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels);
+      rowsum += f.rows;
+      stiles += (int)((P + kStatsThreads - 1) / kStatsThreads);
+      colctas += 10 * ((f.cols + 31) / 32);
+      d.depth_scale = prm->depth_scale;
+      d.min_d = cam.min_distance;
+      d.max_d = cam.max_distance;
+      HM4 KRt, iKRt;
+      projector_matrices(cam, HM4::from(f.transform), KRt, iKRt);
+      rows12(iKRt, d.iKRt);
+      cam_K(cam, d.K);
+      d.world_radius = prm->world_radius;
+      d.min_radius = prm->min_image_radius;
+      d.max_radius = prm->max_image_radius;
+      d.min_points = prm->min_points;
+      d.curv_thr = prm->curvature_threshold;
+      for (int q = 0; q < 3; q++) {
+        d.pim_flat[q] = prm->pim_flat[q]; d.pim_nonflat[q] = prm->pim_nonflat[q];
+        d.nim_flat[q] = prm->nim_flat[q]; d.nim_nonflat[q] = prm->nim_nonflat[q];
+      }
+      d.pim_thr = prm->pim_curvature_threshold;
+      d.nim_thr = prm->nim_curvature_threshold;
+      d.keep_stats = prm->keep_stats && cl->has_eig;
+      d.index = cl->index;
+      d.pts = cl->pts;
+      d.nrm = cl->nrm;
+      d.omg = cl->omg;
+      d.eig = cl->eig;
+      d.count = cl->count;
+      d.tile_counts = (int *)(ctx->ws + o_tiles[k]);
+      d.moments = unproject_only ? nullptr : (void *)(ctx->ws + o_mom[k]);
+    }
+    FrameDev *dfr = (FrameDev *)(ctx->ws + o_frames);
+    CK(ctx, cudaMemcpyAsync(dfr, pin, sizeof(FrameDev) * nf, cudaMemcpyHostToDevice, s));
+    CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+    launch_unproject(dfr, nf, tiles, s, &ctx->prof);
+    if (!unproject_only) {
+      launch_moments(prm->moments_precision, dfr, nf, rowsum, colctas, s, &ctx->prof);
+      launch_stats(prm->moments_precision, dfr, nf, stiles, s, &ctx->prof);
+    }
+    CK(ctx, cudaGetLastError());
+    i0 = i1;
+  }
+  return NICP_OK;
+}
+
+static int build_one(nicp_ctx *ctx, const void *depth, bool u16, int rows, int cols, size_t pitch, int on_device,
+                     const nicp_camera *cam, const nicp_cloud_params *prm, const float *offset, nicp_cloud *out,
+                     int32_t *index_out) {
+  if (!ctx || !out || !prm) return NICP_EINVAL;
+  if (out->ctx != ctx) return fail(ctx, NICP_EINVAL, "cloud belongs to another context");
+  FrameIn f{depth, u16, on_device != 0, pitch, rows, cols, nullptr};
+  int rc = build_frames(ctx, 1, &f, cam, prm, &out, false);
+  if (rc) return rc;
+  if (offset && (rc = nicp_cloud_transform(out, offset))) return rc;
+  if (index_out) {
+    CK(ctx, cudaMemcpyAsync(index_out, out->index, 4 * (size_t)rows * cols, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return NICP_OK;
+}
+
+extern "C" int nicp_cloud_from_depth_u16(nicp_ctx *ctx, const uint16_t *depth, int rows, int cols, size_t pitch,
+                                         int on_device, const nicp_camera *cam, const nicp_cloud_params *prm,
+                                         const float *offset, nicp_cloud *out, int32_t *index_out) {
+  return build_one(ctx, depth, true, rows, cols, pitch, on_device, cam, prm, offset, out, index_out);
+}
+
+extern "C" int nicp_cloud_from_depth_f32(nicp_ctx *ctx, const float *depth, int rows, int cols, size_t pitch,
+                                         int on_device, const nicp_camera *cam, const nicp_cloud_params *prm,
+                                         const float *offset, nicp_cloud *out, int32_t *index_out) {
+  return build_one(ctx, depth, false, rows, cols, pitch, on_device, cam, prm, offset, out, index_out);
+}
+
+extern "C" int nicp_build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *rows, const int *cols,
+                                int on_device, const nicp_camera *cams, const nicp_cloud_params *prm,
+                                nicp_cloud *const *out) {
+  if (!ctx || n < 0 || (n > 0 && (!depth || !rows || !cols || !cams || !prm || !out))) return NICP_EINVAL;
+  std::vector<FrameIn> f(n);
+  for (int i = 0; i < n; i++) {
+    if (out[i] && out[i]->ctx != ctx) return fail(ctx, NICP_EINVAL, "cloud belongs to another context");
+    f[i] = FrameIn{depth[i], true, on_device != 0, 0, rows[i], cols[i], nullptr};
+  }
+  return build_frames(ctx, n, f.data(), cams, prm, out, false);
+}
+
+// ------------------------------------------------------------------ projector API
+extern "C" int nicp_projector_matrices(const nicp_camera *cam, const float T16[16], float KRt16[16], float iKRt16[16]) {
+  if (!cam || !KRt16 || !iKRt16) return NICP_EINVAL;
+  HM4 K, iK;
+  projector_matrices(*cam, HM4::from(T16), K, iK);
+  std::memcpy(KRt16, K.a, sizeof(K.a));
+  std::memcpy(iKRt16, iK.a, sizeof(iK.a));
+  return NICP_OK;
+}
+
+extern "C" int nicp_unproject(nicp_ctx *ctx, const float *depth, int rows, int cols, const nicp_camera *cam,
+                              const float T16[16], float *points4_out, int32_t *index_out, int *n) {
+  if (!ctx || !depth || !cam || !n) return NICP_EINVAL;
+  int rc;
+  if (!ctx->scratch_cloud && (rc = nicp_cloud_create(ctx, &ctx->scratch_cloud))) return rc;
+  nicp_cloud_params prm;
+  nicp_default_cloud_params(&prm);
+  FrameIn f{depth, false, false, 0, rows, cols, T16};
+  nicp_cloud *c = ctx->scratch_cloud;
+  if ((rc = build_frames(ctx, 1, &f, cam, &prm, &c, true))) return rc;
+  if ((rc = nicp_cloud_size(c, n))) return rc;
+  if (points4_out && *n) {
+    CK(ctx, cudaMemcpyAsync(points4_out, c->pts, 16 * (size_t)*n, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (index_out) CK(ctx, cudaMemcpyAsync(index_out, c->index, 4 * (size_t)rows * cols, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return NICP_OK;
+}
+
+extern "C" int nicp_project_intervals(nicp_ctx *ctx, const float *depth, int rows, int cols, const nicp_camera *cam,
+                                      float world_radius, int32_t *radius_out) {
+  if (!ctx || !depth || !cam || !radius_out || rows <= 0 || cols <= 0) return NICP_EINVAL;
+  size_t P = (size_t)rows * cols;
+  Layout L;
+  size_t o_d = L.take(4 * P), o_k = L.take(36), o_o = L.take(4 * P);
+  int rc;
+  if ((rc = ensure_ws(ctx, L.off))) return rc;
+  char *pin;
+  if ((rc = pin_up(ctx, 36, &pin))) return rc;
+  cam_K(*cam, (float *)pin);
+  CK(ctx, cudaMemcpyAsync(ctx->ws + o_k, pin, 36, cudaMemcpyHostToDevice, ctx->stream));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, ctx->stream));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + o_d, depth, 4 * P, cudaMemcpyHostToDevice, ctx->stream));
+  launch_intervals((const float *)(ctx->ws + o_d), (int)P, (const float *)(ctx->ws + o_k), cam->min_distance,
+                   cam->max_distance, world_radius, (int32_t *)(ctx->ws + o_o), ctx->stream, &ctx->prof);
+  CK(ctx, cudaGetLastError());
+  CK(ctx, cudaMemcpyAsync(radius_out, ctx->ws + o_o, 4 * P, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return NICP_OK;
+}
+
+// ------------------------------------------------------------------ pair workspace
+namespace {
+struct PairPlan {
+  int n = 0;
+  size_t o_extra = 0;
+  bool keep_ref = false, list_mode = false;
+  int total_tiles = 0, total_pt_tiles = 0;
+  size_t o_pairs = 0, o_states = 0, o_krt = 0, o_guess = 0, o_roff = 0, o_zbuf = 0, zbuf_bytes = 0;
+  std::vector<size_t> o_cur, o_ref, o_part, o_list, o_ltc, o_np;
+  std::vector<int> P, tiles;
+};
+}  // namespace
+
+// Lays out per-pair buffers; cams[i] gives the projection image of pair i.
+static int plan_pairs(nicp_ctx *ctx, int n, const nicp_camera *cams, const nicp_cloud *const *refs, bool keep_ref,
+                      bool list_mode, PairPlan &pl, size_t extra_bytes = 0) {
+  pl.n = n;
+  pl.keep_ref = keep_ref;
+  pl.list_mode = list_mode;
+  Layout L;
+  pl.o_pairs = L.take(sizeof(PairDev) * n);
+  pl.o_states = L.take(sizeof(PairState) * n);
+  pl.o_krt = L.take(48 * (size_t)n);
+  pl.o_guess = L.take(128 * (size_t)n);
+  pl.o_roff = L.take(128 * (size_t)n);
+  size_t ztot = 0;
+  pl.P.resize(n);
+  pl.tiles.resize(n);
+  for (int i = 0; i < n; i++) {
+    if (!valid_camera(&cams[i])) return fail(ctx, NICP_EINVAL, "bad camera for pair " + std::to_string(i));
+    size_t P = (size_t)cam_rows(cams[i]) * cam_cols(cams[i]);
+    if (P > (1u << 30)) return fail(ctx, NICP_EINVAL, "projection image too large");
+    pl.P[i] = (int)P;
+    pl.tiles[i] = (int)((P + kCorrTilePixels - 1) / kCorrTilePixels);
+    ztot += align_up(8 * P, 256);
+  }
+  pl.o_zbuf = L.take(ztot);
+  pl.zbuf_bytes = ztot;
+  pl.o_cur.resize(n); pl.o_ref.resize(n); pl.o_part.resize(n);
+  pl.o_list.resize(n); pl.o_ltc.resize(n); pl.o_np.resize(n);
+  pl.total_tiles = 0;
+  pl.total_pt_tiles = 0;
+  for (int i = 0; i < n; i++) {
+    size_t P = pl.P[i];
+    pl.o_cur[i] = L.take(4 * P);
+    pl.o_ref[i] = (keep_ref || list_mode) ? L.take(4 * P) : 0;
+    pl.o_part[i] = L.take(8 * kPartialWords * (size_t)pl.tiles[i]);
+    pl.o_list[i] = list_mode ? L.take(8 * P) : 0;
+    pl.o_ltc[i] = list_mode ? L.take(4 * (size_t)pl.tiles[i]) : 0;
+    pl.o_np[i] = L.take(4);
+    pl.total_tiles += pl.tiles[i];
+    int cap = std::max(refs[i] ? refs[i]->capacity : 0, 1);
+    pl.total_pt_tiles += (cap + kPointsPerCta - 1) / kPointsPerCta;
+  }
+  pl.o_extra = L.take(std::max<size_t>(extra_bytes, 1));
+  return ensure_ws(ctx, L.off);
+}
+
+// Fills the PairDev descriptors in host memory.
+static void fill_pairs(nicp_ctx *ctx, const PairPlan &pl, const nicp_camera *cams, const nicp_cloud *const *refs,
+                       const nicp_cloud *const *curs, PairDev *pd) {
+  char *ws = ctx->ws;
+  int tb = 0, pb = 0;
+  size_t zoff = pl.o_zbuf;
+  for (int i = 0; i < pl.n; i++) {
+    PairDev &d = pd[i];
+    std::memset(&d, 0, sizeof(d));
+    const nicp_cloud *r = refs[i], *c = curs[i];
+    d.ref_pts = r ? r->pts : nullptr;
+    d.ref_nrm = r ? r->nrm : nullptr;
+    d.ref_count = r ? r->count : nullptr;
+    d.cur_pts = c ? c->pts : nullptr;
+    d.cur_nrm = c ? c->nrm : nullptr;
+    d.cur_omg = c ? c->omg : nullptr;
+    d.cur_count = c ? c->count : nullptr;
+    d.rows = cam_rows(cams[i]);
+    d.cols = cam_cols(cams[i]);
+    d.tile_base = tb;
+    d.pt_tile_base = pb;
+    d.ref_capacity = std::max(r ? r->capacity : 0, 1);
+    tb += pl.tiles[i];
+    pb += (d.ref_capacity + kPointsPerCta - 1) / kPointsPerCta;
+    d.min_d = cams[i].min_distance;
+    d.max_d = cams[i].max_distance;
+    cam_K(cams[i], d.K);
+    d.cur_index = (int32_t *)(ws + pl.o_cur[i]);
+    d.ref_index = pl.o_ref[i] ? (int32_t *)(ws + pl.o_ref[i]) : nullptr;
+    d.zbuf = (unsigned long long *)(ws + zoff);
+    zoff += align_up(8 * (size_t)pl.P[i], 256);
+    d.partials = (double *)(ws + pl.o_part[i]);
+    d.pairs = pl.o_list[i] ? (int32_t *)(ws + pl.o_list[i]) : nullptr;
+    d.list_tile_counts = pl.o_ltc[i] ? (int *)(ws + pl.o_ltc[i]) : nullptr;
+    d.num_pairs = (int *)(ws + pl.o_np[i]);
+    d.state = (PairState *)(ws + pl.o_states) + i;
+  }
+}
+
+// ------------------------------------------------------------------ correspondences / linearizer API
+extern "C" int nicp_correspond(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const int32_t *ref_index,
+                               const int32_t *cur_index, int rows, int cols, const float T16[16],
+                               const nicp_corr_params *prm, int32_t *pairs_out, int *num_out) {
+  if (!ctx || !ref || !cur || !ref_index || !cur_index || rows <= 0 || cols <= 0 || !T16 || !prm || !num_out)
+    return NICP_EINVAL;
+  nicp_camera cam;
+  nicp_default_camera(&cam);
+  cam.rows = rows;
+  cam.cols = cols;
+  PairPlan pl;
+  int rc;
+  if ((rc = plan_pairs(ctx, 1, &cam, &ref, false, true, pl))) return rc;
+  char *pin;
+  if ((rc = pin_up(ctx, sizeof(PairDev) + 48, &pin))) return rc;
+  PairDev *pd = (PairDev *)pin;
+  fill_pairs(ctx, pl, &cam, &ref, &cur, pd);
+  float *T12 = (float *)(pin + sizeof(PairDev));
+  rows12(HM4::from(T16), T12);
+  cudaStream_t s = ctx->stream;
+  size_t P = (size_t)rows * cols;
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_pairs, pin, sizeof(PairDev), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_krt, T12, 48, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_ref[0], ref_index, 4 * P, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_cur[0], cur_index, 4 * P, cudaMemcpyHostToDevice, s));
+  launch_corr_list((const PairDev *)(ctx->ws + pl.o_pairs), 1, pl.total_tiles, corr_params(*prm), 0,
+                   (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
+  CK(ctx, cudaGetLastError());
+  CK(ctx, cudaMemcpyAsync(num_out, ctx->ws + pl.o_np[0], 4, cudaMemcpyDeviceToHost, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  if (pairs_out && *num_out > 0) {
+    CK(ctx, cudaMemcpyAsync(pairs_out, ctx->ws + pl.o_list[0], 8 * (size_t)*num_out, cudaMemcpyDeviceToHost, s));
+    CK(ctx, cudaStreamSynchronize(s));
+  }
+  return NICP_OK;
+}
+
+extern "C" int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const int32_t *pairs,
+                              int num_pairs, const float T16[16], const nicp_lin_params *prm, int parity_threads,
+                              double H36[36], double b6[6], double *error, int *inliers) {
+  if (!ctx || !ref || !cur || (num_pairs > 0 && !pairs) || num_pairs < 0 || !T16 || !prm) return NICP_EINVAL;
+  // list slots are tiled like pixels: a one-row image of num_pairs pixels
+  nicp_camera cam;
+  nicp_default_camera(&cam);
+  cam.rows = 1;
+  cam.cols = std::max(num_pairs, 1);
+  PairPlan pl;
+  int rc;
+  if ((rc = plan_pairs(ctx, 1, &cam, &ref, false, true, pl))) return rc;
+  char *pin;
+  if ((rc = pin_up(ctx, sizeof(PairDev) + 48 + 4, &pin))) return rc;
+  PairDev *pd = (PairDev *)pin;
+  fill_pairs(ctx, pl, &cam, &ref, &cur, pd);
+  float *T12 = (float *)(pin + sizeof(PairDev));
+  rows12(HM4::from(T16), T12);
+  int *np = (int *)(pin + sizeof(PairDev) + 48);
+  *np = num_pairs;
+  cudaStream_t s = ctx->stream;
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_pairs, pin, sizeof(PairDev), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_krt, T12, 48, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_np[0], np, 4, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+  if (num_pairs > 0)
+    CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_list[0], pairs, 8 * (size_t)num_pairs, cudaMemcpyHostToDevice, s));
+  const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
+  launch_lin_list(dpd, 1, pl.total_tiles, lin_params(*prm), std::max(1, parity_threads), 0,
+                  (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
+  launch_solve(dpd, 1, 0.0f, 2, 0.0, 1, s, &ctx->prof);
+  CK(ctx, cudaGetLastError());
+  char *pd_host;
+  if ((rc = pin_down(ctx, sizeof(PairState), &pd_host))) return rc;
+  CK(ctx, cudaMemcpyAsync(pd_host, ctx->ws + pl.o_states, sizeof(PairState), cudaMemcpyDeviceToHost, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  const PairState *st = (const PairState *)pd_host;
+  if (H36) std::memcpy(H36, st->H, sizeof(st->H));
+  if (b6) std::memcpy(b6, st->b, sizeof(st->b));
+  if (error) *error = st->error;
+  if (inliers) *inliers = st->inliers;
+  return NICP_OK;
+}
+
+// ------------------------------------------------------------------ projection API
+extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_camera *cam, const float T16[16],
+                            int32_t *index_out, float *depth_out) {
+  if (!ctx || !cloud || !cam || !valid_camera(cam)) return NICP_EINVAL;
+  PairPlan pl;
+  int rc;
+  size_t P = (size_t)cam_rows(*cam) * cam_cols(*cam);
+  if ((rc = plan_pairs(ctx, 1, cam, &cloud, false, false, pl, 4 * P))) return rc;
+  size_t o_depth = pl.o_extra;
+  char *pin;
+  if ((rc = pin_up(ctx, sizeof(PairDev) + 48, &pin))) return rc;
+  const nicp_cloud *cur = cloud;
+  fill_pairs(ctx, pl, cam, &cloud, &cur, (PairDev *)pin);
+  HM4 KRt, iKRt;
+  projector_matrices(*cam, HM4::from(T16), KRt, iKRt);
+  float *k12 = (float *)(pin + sizeof(PairDev));
+  rows12(KRt, k12);
+  cudaStream_t s = ctx->stream;
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_pairs, pin, sizeof(PairDev), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_krt, k12, 48, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+  CK(ctx, cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s));
+  const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
+  launch_zbuffer(dpd, 1, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
+  launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ctx->ws + o_depth), s, &ctx->prof);
+  CK(ctx, cudaGetLastError());
+  if (index_out) CK(ctx, cudaMemcpyAsync(index_out, ctx->ws + pl.o_cur[0], 4 * P, cudaMemcpyDeviceToHost, s));
+  if (depth_out) CK(ctx, cudaMemcpyAsync(depth_out, ctx->ws + o_depth, 4 * P, cudaMemcpyDeviceToHost, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  return NICP_OK;
+}
+
+// ------------------------------------------------------------------ aligner
+namespace {
+struct AlignCall {
+  int n;
+  const nicp_cloud *const *refs;
+  const nicp_cloud *const *curs;
+  const nicp_camera *cams;
+  const float *guesses;      // n*16 or null
+  const float *ref_offsets;  // n*16 or null
+  const float *cur_offsets;  // n*16 or null
+  const nicp_corr_params *corr;
+  const nicp_lin_params *lin;
+  const nicp_align_params *prm;
+  bool graph;
+};
+}  // namespace
+
+// Enqueues the whole Gauss-Newton loop for the planned pairs.
+static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) {
+  cudaStream_t s = ctx->stream;
+  const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
+  CorrParams cp = corr_params(*a.corr);
+  LinParams lp = lin_params(*a.lin);
+  const nicp_align_params &p = *a.prm;
+  int outer = p.outer_iterations, inner = p.inner_iterations;
+  bool stats = p.compute_statistics != 0;
+  cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s);
+  launch_init_pairs(dpd, pl.n, (const double *)(ctx->ws + pl.o_guess), (const double *)(ctx->ws + pl.o_roff), s,
+                    &ctx->prof);
+  // current cloud, seen from its sensor offset, projected once (alignerprojective.cpp:36-39)
+  launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
+  launch_resolve(dpd, pl.n, pl.total_tiles, 0, nullptr, s, &ctx->prof);
+  for (int i = 0; i < outer; i++) {
+    launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 1, nullptr, s, &ctx->prof);
+    if (pl.list_mode) {
+      launch_resolve(dpd, pl.n, pl.total_tiles, 1, nullptr, s, &ctx->prof);
+      launch_corr_list(dpd, pl.n, pl.total_tiles, cp, 1, nullptr, s, &ctx->prof);
+      for (int k = 0; k < inner; k++) {
+        launch_lin_list(dpd, pl.n, pl.total_tiles, lp, std::max(1, a.corr->parity_threads), 1, nullptr, s, &ctx->prof);
+        launch_solve(dpd, pl.n, p.lambda, (k == inner - 1) ? 1 : 0, p.early_exit_eps, 0, s, &ctx->prof);
+      }
+    } else {
+      for (int k = 0; k < inner; k++) {
+        int flags = (k == 0) ? (1 | 2 | (pl.keep_ref ? 4 : 0)) : 0;
+        launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, flags, s, &ctx->prof);
+        launch_solve(dpd, pl.n, p.lambda, (k == inner - 1) ? 1 : 0, p.early_exit_eps, 0, s, &ctx->prof);
+      }
+    }
+  }
+  if (stats) {
+    // Aligner::_computeStatistics: one more linearization at the final pose
+    // with the last correspondences (aligner.cpp:90-95)
+    if (pl.list_mode)
+      launch_lin_list(dpd, pl.n, pl.total_tiles, lp, std::max(1, a.corr->parity_threads), 2, nullptr, s, &ctx->prof);
+    else
+      launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, 8, s, &ctx->prof);
+    launch_solve(dpd, pl.n, 0.0f, 4, 0.0, 1, s, &ctx->prof);
+  }
+}
+
+static std::string graph_key(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) {
+  std::string k;
+  auto put = [&](const void *p, size_t n) { k.append((const char *)p, n); };
+  put(&ctx->ws, sizeof(ctx->ws));
+  put(&pl.n, sizeof(int));
+  put(&pl.keep_ref, 1);
+  put(&pl.list_mode, 1);
+  put(&pl.total_tiles, sizeof(int));
+  put(&pl.total_pt_tiles, sizeof(int));
+  put(&pl.zbuf_bytes, sizeof(size_t));
+  put(a.corr, sizeof(*a.corr));
+  put(a.lin, sizeof(*a.lin));
+  put(a.prm, sizeof(*a.prm));
+  bool pe = ctx->prof.enabled;
+  put(&pe, 1);
+  return k;
+}
+
+static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out) {
+  if (!ctx || a.n < 0 || !a.cams || !a.corr || !a.lin || !a.prm || (a.n > 0 && (!a.refs || !a.curs || !out)))
+    return NICP_EINVAL;
+  if (a.n == 0) return NICP_OK;
+  const nicp_align_params &p = *a.prm;
+  if (p.outer_iterations < 0 || p.inner_iterations < 1 || p.outer_iterations > 1000 || p.inner_iterations > 100)
+    return fail(ctx, NICP_EINVAL, "iteration counts out of range");
+  for (int i = 0; i < a.n; i++) {
+    if (!a.refs[i] || !a.curs[i] || !a.refs[i]->mem || !a.curs[i]->mem)
+      return fail(ctx, NICP_EINVAL, "pair " + std::to_string(i) + " has an empty cloud");
+    if (a.refs[i]->ctx != ctx || a.curs[i]->ctx != ctx) return fail(ctx, NICP_EINVAL, "cloud of another context");
+  }
+  bool list_mode = a.corr->parity_threads > 1;
+  bool keep_ref = p.inner_iterations > 1 || p.compute_statistics;
+  // point tiles cover the larger of the two clouds: the current cloud is
+  // projected once with the same grid as the reference cloud
+  std::vector<const nicp_cloud *> big(a.n);
+  for (int j = 0; j < a.n; j++) big[j] = (a.curs[j]->capacity > a.refs[j]->capacity) ? a.curs[j] : a.refs[j];
+  PairPlan pl;
+  int rc;
+  if ((rc = plan_pairs(ctx, a.n, a.cams, big.data(), keep_ref, list_mode, pl))) return rc;
+  size_t up = sizeof(PairDev) * a.n + 48 * (size_t)a.n + 256 * (size_t)a.n;
+  char *pin;
+  if ((rc = pin_up(ctx, up, &pin))) return rc;
+  PairDev *pd = (PairDev *)pin;
+  fill_pairs(ctx, pl, a.cams, big.data(), a.curs, pd);
+  for (int i = 0; i < a.n; i++) {
+    pd[i].ref_pts = a.refs[i]->pts;
+    pd[i].ref_nrm = a.refs[i]->nrm;
+    pd[i].ref_count = a.refs[i]->count;
+  }
+  float *krt = (float *)(pin + sizeof(PairDev) * a.n);
+  double *gs = (double *)(pin + sizeof(PairDev) * a.n + 48 * (size_t)a.n);
+  double *ro = gs + 16 * (size_t)a.n;
+  for (int i = 0; i < a.n; i++) {
+    HM4 KRt, iKRt;
+    projector_matrices(a.cams[i], HM4::from(a.cur_offsets ? a.cur_offsets + 16 * i : nullptr), KRt, iKRt);
+    rows12(KRt, krt + 12 * i);
+    HM4 G = HM4::from(a.guesses ? a.guesses + 16 * i : nullptr);
+    HM4 R = HM4::from(a.ref_offsets ? a.ref_offsets + 16 * i : nullptr);
+    for (int k = 0; k < 16; k++) {
+      gs[16 * i + k] = G.a[k];
+      ro[16 * i + k] = R.a[k];
+    }
+  }
+  cudaStream_t s = ctx->stream;
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_pairs, pd, sizeof(PairDev) * a.n, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_krt, krt, 48 * (size_t)a.n, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_guess, gs, 128 * (size_t)a.n, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_roff, ro, 128 * (size_t)a.n, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+  if (a.graph) {
+    std::string key = graph_key(ctx, pl, a);
+    GraphEntry *ge = nullptr;
+    for (auto &g : ctx->graphs)
+      if (g.key == key) ge = &g;
+    if (!ge) {
+      GraphEntry g;
+      g.key = key;
+      size_t rec0 = ctx->prof.recs.size();
+      unsigned long long l0 = ctx->prof.launches;
+      cudaGraph_t graph;
+      CK(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      ctx->prof.capturing = true;
+      enqueue_loop(ctx, pl, a);
+      ctx->prof.capturing = false;
+      cudaError_t e = cudaStreamEndCapture(s, &graph);
+      if (e != cudaSuccess) return fail(ctx, NICP_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(ctx, NICP_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+      g.kernels = ctx->prof.launches - l0;
+      ctx->prof.launches = l0;
+      g.recs.assign(ctx->prof.recs.begin() + rec0, ctx->prof.recs.end());
+      ctx->prof.recs.resize(rec0);
+      if (ctx->graphs.size() >= 16) {
+        cudaGraphExecDestroy(ctx->graphs.front().exec);
+        ctx->graphs.erase(ctx->graphs.begin());
+      }
+      ctx->graphs.push_back(g);
+      ge = &ctx->graphs.back();
+    }
+    CK(ctx, cudaGraphLaunch(ge->exec, s));
+    ctx->prof.launches += ge->kernels;
+    if (ctx->prof.enabled) ctx->prof.recs.insert(ctx->prof.recs.end(), ge->recs.begin(), ge->recs.end());
+  } else {
+    enqueue_loop(ctx, pl, a);
+  }
+  CK(ctx, cudaGetLastError());
+  char *res;
+  if ((rc = pin_down(ctx, sizeof(PairState) * a.n, &res))) return rc;
+  CK(ctx, cudaMemcpyAsync(res, ctx->ws + pl.o_states, sizeof(PairState) * a.n, cudaMemcpyDeviceToHost, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  const PairState *st = (const PairState *)res;
+  for (int i = 0; i < a.n; i++) {
+    nicp_align_result &r = out[i];
+    std::memcpy(r.T, st[i].T, sizeof(r.T));
+    r.error = st[i].error;
+    r.inliers = st[i].inliers;
+    r.num_correspondences = st[i].num_corr;
+    r.outer_iterations_run = st[i].iterations;
+    r.status = st[i].status;
+    r.translational_ratio = r.rotational_ratio = 0;
+    r.solution_valid = -1;
+    if (p.compute_statistics) {
+      solution_statistics(st[i].Hstat, st[i].T, &r.translational_ratio, &r.rotational_ratio);
+      r.solution_valid = !(r.rotational_ratio > p.rotational_min_eigen_ratio ||
+                           r.translational_ratio > p.translational_min_eigen_ratio);
+    }
+  }
+  return NICP_OK;
+}
+
+extern "C" int nicp_align(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const nicp_camera *cam,
+                          const float guess16[16], const float ref_offset16[16], const float cur_offset16[16],
+                          const nicp_corr_params *corr, const nicp_lin_params *lin, const nicp_align_params *prm,
+                          nicp_align_result *out) {
+  AlignCall a{1, &ref, &cur, cam, guess16, ref_offset16, cur_offset16, corr, lin, prm, false};
+  return align_impl(ctx, a, out);
+}
+
+extern "C" int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs, const nicp_cloud *const *curs,
+                                const nicp_camera *cams, const float *guesses, const nicp_corr_params *corr,
+                                const nicp_lin_params *lin, const nicp_align_params *prm, nicp_align_result *out) {
+  AlignCall a{n, refs, curs, cams, guesses, nullptr, nullptr, corr, lin, prm, true};
+  return align_impl(ctx, a, out);
+}

@@ -1,0 +1,418 @@
+// common.cuh -- device-side data layout and arithmetic shared by the NICP kernels.
+//
+// Data layout in HBM (one cloud):
+//   pts[V]   float4 (x, y, z, 1)                          16 B / point
+//   nrm[V]   float4 (nx, ny, nz, curvature)               16 B / point
+//   omg[3V]  float4 x3: (Op00 Op01 Op02 Op11) (Op12 Op22 On00 On01)
+//                       (On02 On11 On12 On22)              48 B / point
+//   eig[12V] optional: eigenvalues (3) + eigenvectors (9, row-major, columns
+//            are vectors) for parity dumps of the reference's Stats.
+// Images are packed row-major (pitch == cols).
+//
+// Arithmetic that decides a discrete outcome (which pixel a point lands on,
+// which index a z-buffer keeps, whether a correspondence passes a gate) is
+// written with __fmul_rn/__fadd_rn so the compiler cannot contract it into
+// FMAs: products and sums round exactly as the reference's SSE (no FMA)
+// build rounds them, in one fixed order -- sequential over the inner index,
+// ((a0*b0 + a1*b1) + a2*b2) + a3*b3.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nicp {
+
+constexpr int kCorrTilePixels = 1024;   // pixels per CTA in the pair-image kernels
+constexpr int kCorrThreads = 256;       // 4 pixels per thread
+constexpr int kUnprojTilePixels = 4096; // 16 pixels per thread, 256 threads
+constexpr int kStatsThreads = 256;
+constexpr int kPartialWords = 32;       // doubles per CTA partial (21 H + 6 b + chi2 + inliers + C + K + pad)
+constexpr int kPointsPerCta = 256;      // z-buffer kernel: one point per thread
+
+// ---- per-frame descriptor for the cloud-build kernels
+struct FrameDev {
+  const uint16_t *depth_u16;  // packed rows*cols, or null when depth_f32 is used
+  const float *depth_f32;
+  int rows, cols;
+  int tile_base;              // first unprojection tile of this frame in the grid
+  int row_base;               // first image row of this frame in the row grid
+  int stat_tile_base;         // first stats tile of this frame
+  int col_base;               // first column-scan CTA of this frame (10 planes x strips)
+  float depth_scale;
+  float min_d, max_d;
+  float iKRt[12];             // unprojection matrix (rows 0..2 of 4x4)
+  float K[9];                 // effective camera matrix
+  float world_radius;
+  int min_radius, max_radius, min_points;
+  float curv_thr;
+  float pim_flat[3], pim_nonflat[3], pim_thr;
+  float nim_flat[3], nim_nonflat[3], nim_thr;
+  int keep_stats;
+  // outputs
+  int32_t *index;             // rows*cols
+  float4 *pts, *nrm, *omg;
+  float *eig;
+  int *count;                 // device scalar: number of points
+  // scratch
+  int *tile_counts;           // per unprojection tile
+  void *moments;              // 10 planes of rows*cols values (double / float / float2)
+};
+
+// ---- per-pair device state of the Gauss-Newton loop
+struct PairState {
+  double T[16];        // current estimate, current -> reference
+  double invT[16];     // inner-loop variable (alignerprojective.cpp:66-96)
+  double Tstart[16];   // T at the start of the outer iteration (early exit)
+  double ref_offset[16];
+  float KRt[12];       // projects the reference cloud with T * ref_offset
+  float Tgate[12];     // float T^-1 used by the correspondence gates
+  float Tlin[12];      // float invT used by the linearizer
+  float Tgate_used[12]; // gating transform of the last completed outer iteration
+  double H[36], b[6];  // last system (before lambda)
+  double Hstat[36];    // system of the statistics pass (Aligner::_computeStatistics)
+  float error;
+  int inliers;
+  int num_corr;
+  int candidates;
+  int iterations;
+  int done;
+  int status;
+  int pad;
+};
+
+struct PairDev {
+  const float4 *ref_pts, *ref_nrm;
+  const int *ref_count;
+  const float4 *cur_pts, *cur_nrm, *cur_omg;
+  const int *cur_count;
+  int rows, cols;       // projection image (scaled)
+  int tile_base;        // first pixel tile of this pair in the grid
+  int pt_tile_base;     // first point tile (reference cloud) in the grid
+  int ref_capacity;     // upper bound on reference points
+  float min_d, max_d;
+  float K[9];
+  int32_t *cur_index;   // rows*cols, current cloud projected once
+  int32_t *ref_index;   // rows*cols, kept when inner > 1 or statistics are wanted
+  unsigned long long *zbuf;  // rows*cols reference z-buffer (all ones when empty)
+  double *partials;     // ntiles * kPartialWords
+  int32_t *pairs;       // list mode: 2 * rows*cols
+  int *list_tile_counts;
+  int *num_pairs;       // list mode: device scalar K
+  PairState *state;
+};
+
+struct CorrParams {
+  float sq_thr, cos_thr, flat_thr, min_ratio, max_ratio;
+  int demoted;
+  int row_limit_threads;  // parity threads T (rows beyond T*(rows/T) skipped)
+};
+
+struct LinParams {
+  float max_chi2;
+  int robust;
+  int z_scaling;
+  float scale;
+  int demoted;
+};
+
+// ------------------------------------------------------------ float helpers
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsb(float a, float b) { return __fsub_rn(a, b); }
+
+// rows 0..2 of a 4x4 with row 3 = (0 0 0 1), applied to (x, y, z, w)
+__device__ __forceinline__ float row4(const float *A, float x, float y, float z, float w) {
+  float s = fm(A[0], x);
+  s = fa(s, fm(A[1], y));
+  s = fa(s, fm(A[2], z));
+  s = fa(s, fm(A[3], w));
+  return s;
+}
+
+__device__ __forceinline__ float3 xform_point(const float *A, float4 p) {
+  return make_float3(row4(A, p.x, p.y, p.z, 1.0f), row4(A + 4, p.x, p.y, p.z, 1.0f),
+                     row4(A + 8, p.x, p.y, p.z, 1.0f));
+}
+__device__ __forceinline__ float3 xform_normal(const float *A, float4 n) {
+  return make_float3(row4(A, n.x, n.y, n.z, 0.0f), row4(A + 4, n.x, n.y, n.z, 0.0f),
+                     row4(A + 8, n.x, n.y, n.z, 0.0f));
+}
+// ((a0*b0 + a1*b1) + a2*b2) + 0*0 -- the w terms of the reference's 4-vectors are zero
+__device__ __forceinline__ float dot3x(float ax, float ay, float az, float bx, float by, float bz) {
+  float s = fm(ax, bx);
+  s = fa(s, fm(ay, by));
+  s = fa(s, fm(az, bz));
+  s = fa(s, 0.0f);
+  return s;
+}
+
+// Monotone 32-bit key of a float (total order as unsigned).
+__device__ __forceinline__ uint32_t float_key(float d) {
+  uint32_t u = __float_as_uint(d);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// pinholepointprojector.h:253-262 plus the range/image checks of
+// pinholepointprojector.cpp:54-58.
+__device__ __forceinline__ bool project_pixel(const float *KRt, float4 p, int rows, int cols, float min_d,
+                                              float max_d, int &x, int &y, float &d) {
+  float ix = row4(KRt, p.x, p.y, p.z, 1.0f);
+  float iy = row4(KRt + 4, p.x, p.y, p.z, 1.0f);
+  d = row4(KRt + 8, p.x, p.y, p.z, 1.0f);
+  if (!(d >= min_d && d <= max_d)) return false;
+  float inv = __frcp_rn(d);
+  float px = roundf(fm(ix, inv)), py = roundf(fm(iy, inv));
+  if (!(fabsf(px) < 1073741824.0f) || !(fabsf(py) < 1073741824.0f)) return false;
+  x = (int)px;
+  y = (int)py;
+  return x >= 0 && x < cols && y >= 0 && y < rows;
+}
+
+// pinholepointprojector.h:293-302: (int)max(K*(R,R,0) * (1/d)); -1 outside the range.
+__device__ __forceinline__ int interval_radius(const float *K, float d, float min_d, float max_d, float R) {
+  if (d < min_d || d > max_d) return -1;
+  float p0 = fa(fa(fm(K[0], R), fm(K[1], R)), fm(K[2], 0.0f));
+  float p1 = fa(fa(fm(K[3], R), fm(K[4], R)), fm(K[5], 0.0f));
+  float inv = __frcp_rn(d);
+  float a = fm(p0, inv), b = fm(p1, inv);
+  float m = (a < b) ? b : a;
+  return (int)m;
+}
+
+// imageutils.cpp:85-99 followed by pinholepointprojector.h:275-280.
+__device__ __forceinline__ float depth_of(const FrameDev &f, int pix) {
+  if (f.depth_u16) {
+    uint16_t u = f.depth_u16[pix];
+    return u ? fm(f.depth_scale, (float)(int)u) : 0.0f;
+  }
+  return f.depth_f32[pix];
+}
+__device__ __forceinline__ bool depth_valid(float d, float min_d, float max_d) {
+  return !(d == 0.0f || d < min_d || d > max_d);
+}
+__device__ __forceinline__ float4 unproject_pixel(const float *iKRt, int c, int r, float d) {
+  float qx = fm((float)c, d), qy = fm((float)r, d);
+  return make_float4(row4(iKRt, qx, qy, d, 1.0f), row4(iKRt + 4, qx, qy, d, 1.0f),
+                     row4(iKRt + 8, qx, qy, d, 1.0f), 1.0f);
+}
+
+// ------------------------------------------------------------ FP64 linear algebra
+// Same algorithms as the oracle restatement: symmetric 3x3 eigensolver from
+// the trigonometric roots of the characteristic cubic (Smith 1961) with
+// eigenvectors from cross products / the orthogonal complement (Eberly
+// 2014); LDL^T with symmetric diagonal pivoting (Golub & Van Loan 4.2).
+__device__ __forceinline__ void d_cross(const double *a, const double *b, double *c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ double d_dot(const double *a, const double *b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+__device__ inline void d_null_vector(const double *B, double mu, double *v) {
+  double r0[3] = {B[0] - mu, B[1], B[2]};
+  double r1[3] = {B[1], B[3] - mu, B[4]};
+  double r2[3] = {B[2], B[4], B[5] - mu};
+  double c0[3], c1[3], c2[3];
+  d_cross(r0, r1, c0);
+  d_cross(r0, r2, c1);
+  d_cross(r1, r2, c2);
+  double d0 = d_dot(c0, c0), d1 = d_dot(c1, c1), d2 = d_dot(c2, c2);
+  const double *best = c0;
+  double db = d0;
+  if (d1 > db) { best = c1; db = d1; }
+  if (d2 > db) { best = c2; db = d2; }
+  if (!(db > 0.0)) { v[0] = 1; v[1] = 0; v[2] = 0; return; }
+  double inv = 1.0 / sqrt(db);
+  v[0] = best[0] * inv; v[1] = best[1] * inv; v[2] = best[2] * inv;
+}
+
+__device__ inline void d_plane_vector(const double *B, const double *e, double mu, double *v) {
+  double u[3];
+  if (fabs(e[0]) > fabs(e[1])) {
+    double il = 1.0 / sqrt(e[0] * e[0] + e[2] * e[2]);
+    u[0] = -e[2] * il; u[1] = 0; u[2] = e[0] * il;
+  } else {
+    double il = 1.0 / sqrt(e[1] * e[1] + e[2] * e[2]);
+    u[0] = 0; u[1] = e[2] * il; u[2] = -e[1] * il;
+  }
+  double w[3];
+  d_cross(e, u, w);
+  double Bu[3] = {B[0] * u[0] + B[1] * u[1] + B[2] * u[2], B[1] * u[0] + B[3] * u[1] + B[4] * u[2],
+                  B[2] * u[0] + B[4] * u[1] + B[5] * u[2]};
+  double Bw[3] = {B[0] * w[0] + B[1] * w[1] + B[2] * w[2], B[1] * w[0] + B[3] * w[1] + B[4] * w[2],
+                  B[2] * w[0] + B[4] * w[1] + B[5] * w[2]};
+  double m00 = d_dot(u, Bu) - mu, m01 = d_dot(u, Bw), m11 = d_dot(w, Bw) - mu;
+  double n0 = m00 * m00 + m01 * m01, n1 = m01 * m01 + m11 * m11;
+  double a, b;
+  if (n0 >= n1) {
+    if (n0 > 0) { double il = 1.0 / sqrt(n0); a = -m01 * il; b = m00 * il; }
+    else { a = 1; b = 0; }
+  } else {
+    double il = 1.0 / sqrt(n1); a = -m11 * il; b = m01 * il;
+  }
+  v[0] = a * u[0] + b * w[0];
+  v[1] = a * u[1] + b * w[1];
+  v[2] = a * u[2] + b * w[2];
+}
+
+// A = {a00 a01 a02 a11 a12 a22}; lam ascending; U row-major, column k <-> lam[k].
+__device__ inline void d_eig3(const double *A, double *lam, double *U) {
+  double amax = fabs(A[0]);
+  for (int i = 1; i < 6; i++) amax = fmax(amax, fabs(A[i]));
+  if (!(amax > 0.0)) {
+    lam[0] = lam[1] = lam[2] = 0;
+    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    return;
+  }
+  double is = 1.0 / amax;
+  double B[6];
+  for (int i = 0; i < 6; i++) B[i] = A[i] * is;
+  double m = (B[0] + B[3] + B[5]) / 3.0;
+  double b00 = B[0] - m, b11 = B[3] - m, b22 = B[5] - m;
+  double off = B[1] * B[1] + B[2] * B[2] + B[4] * B[4];
+  double p2 = b00 * b00 + b11 * b11 + b22 * b22 + 2.0 * off;
+  if (!(p2 > 0.0)) {
+    lam[0] = lam[1] = lam[2] = m * amax;
+    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    return;
+  }
+  double p = sqrt(p2 / 6.0);
+  double ip = 1.0 / p;
+  double c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip, c01 = B[1] * ip, c02 = B[2] * ip, c12 = B[4] * ip;
+  double det = c00 * (c11 * c22 - c12 * c12) - c01 * (c01 * c22 - c12 * c02) + c02 * (c01 * c12 - c11 * c02);
+  double q = det / 2.0;
+  q = fmin(1.0, fmax(-1.0, q));
+  double phi = acos(q) / 3.0;
+  const double tpi3 = 2.0943951023931954923;
+  double l2 = m + 2.0 * p * cos(phi);
+  double l0 = m + 2.0 * p * cos(phi + tpi3);
+  double l1 = 3.0 * m - l0 - l2;
+  double t;
+  if (l1 < l0) { t = l1; l1 = l0; l0 = t; }
+  if (l2 < l1) { t = l2; l2 = l1; l1 = t; }
+  if (l1 < l0) { t = l1; l1 = l0; l0 = t; }
+  double v0[3], v1[3], v2[3];
+  if (l1 - l0 >= l2 - l1) {
+    d_null_vector(B, l0, v0);
+    d_plane_vector(B, v0, l1, v1);
+    d_cross(v0, v1, v2);
+  } else {
+    d_null_vector(B, l2, v2);
+    d_plane_vector(B, v2, l1, v1);
+    d_cross(v1, v2, v0);
+  }
+  lam[0] = l0 * amax; lam[1] = l1 * amax; lam[2] = l2 * amax;
+  for (int r = 0; r < 3; r++) { U[r * 3 + 0] = v0[r]; U[r * 3 + 1] = v1[r]; U[r * 3 + 2] = v2[r]; }
+}
+
+// Solve A x = b for a symmetric 6x6 A given by its lower triangle.
+__device__ inline void d_ldlt_solve6(const double *A, const double *b, double *x) {
+  double M[6][6];
+  int perm[6];
+  for (int i = 0; i < 6; i++) {
+    perm[i] = i;
+    for (int j = 0; j < 6; j++) M[i][j] = (i >= j) ? A[i * 6 + j] : A[j * 6 + i];
+  }
+  double d[6];
+  for (int k = 0; k < 6; k++) {
+    int piv = k;
+    double best = fabs(M[k][k]);
+    for (int i = k + 1; i < 6; i++)
+      if (fabs(M[i][i]) > best) { best = fabs(M[i][i]); piv = i; }
+    if (piv != k) {
+      for (int j = 0; j < 6; j++) { double t = M[k][j]; M[k][j] = M[piv][j]; M[piv][j] = t; }
+      for (int i = 0; i < 6; i++) { double t = M[i][k]; M[i][k] = M[i][piv]; M[i][piv] = t; }
+      int t = perm[k]; perm[k] = perm[piv]; perm[piv] = t;
+    }
+    d[k] = M[k][k];
+    double col[6];
+    for (int i = k + 1; i < 6; i++) col[i] = M[i][k];
+    for (int i = k + 1; i < 6; i++) M[i][k] = col[i] / d[k];
+    for (int i = k + 1; i < 6; i++)
+      for (int j = k + 1; j <= i; j++) {
+        M[i][j] = M[i][j] - M[i][k] * col[j];
+        M[j][i] = M[i][j];
+      }
+  }
+  double y[6];
+  for (int i = 0; i < 6; i++) y[i] = b[perm[i]];
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < i; j++) y[i] = y[i] - M[i][j] * y[j];
+  for (int i = 0; i < 6; i++) y[i] = y[i] / d[i];
+  for (int i = 5; i >= 0; i--)
+    for (int j = i + 1; j < 6; j++) y[i] = y[i] - M[j][i] * y[j];
+  for (int i = 0; i < 6; i++) x[perm[i]] = y[i];
+}
+
+// bm_se3.h:10-52 in FP64.
+__device__ inline void d_v2t(const double *x, double *T) {
+  double qx = x[3], qy = x[4], qz = x[5];
+  double qw = sqrt(fmax(0.0, 1.0 - (qx * qx + qy * qy + qz * qz)));
+  T[0] = qw * qw + qx * qx - qy * qy - qz * qz;
+  T[1] = 2 * (qx * qy - qw * qz);
+  T[2] = 2 * (qx * qz + qw * qy);
+  T[4] = 2 * (qx * qy + qz * qw);
+  T[5] = qw * qw - qx * qx + qy * qy - qz * qz;
+  T[6] = 2 * (qy * qz - qx * qw);
+  T[8] = 2 * (qx * qz - qy * qw);
+  T[9] = 2 * (qy * qz + qx * qw);
+  T[10] = qw * qw - qx * qx - qy * qy + qz * qz;
+  T[3] = x[0]; T[7] = x[1]; T[11] = x[2];
+  T[12] = 0; T[13] = 0; T[14] = 0; T[15] = 1;
+}
+
+// Shepperd's method, normalised, vector part with w >= 0.
+__device__ inline void d_t2v(const double *T, double *x) {
+  double R[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) R[i][j] = T[i * 4 + j];
+  double qx, qy, qz, qw;
+  double tr = R[0][0] + R[1][1] + R[2][2];
+  if (tr > 0) {
+    double s = sqrt(tr + 1.0);
+    qw = 0.5 * s;
+    s = 0.5 / s;
+    qx = (R[2][1] - R[1][2]) * s;
+    qy = (R[0][2] - R[2][0]) * s;
+    qz = (R[1][0] - R[0][1]) * s;
+  } else {
+    int i = 0;
+    if (R[1][1] > R[0][0]) i = 1;
+    if (R[2][2] > R[i][i]) i = 2;
+    int j = (i + 1) % 3, k = (j + 1) % 3;
+    double s = sqrt(R[i][i] - R[j][j] - R[k][k] + 1.0);
+    double q[3];
+    q[i] = 0.5 * s;
+    s = 0.5 / s;
+    qw = (R[k][j] - R[j][k]) * s;
+    q[j] = (R[j][i] + R[i][j]) * s;
+    q[k] = (R[k][i] + R[i][k]) * s;
+    qx = q[0]; qy = q[1]; qz = q[2];
+  }
+  double n = sqrt(qx * qx + qy * qy + qz * qz + qw * qw);
+  qx /= n; qy /= n; qz /= n; qw /= n;
+  if (qw < 0) { qx = -qx; qy = -qy; qz = -qz; }
+  x[0] = T[3]; x[1] = T[7]; x[2] = T[11];
+  x[3] = qx; x[4] = qy; x[5] = qz;
+}
+
+__device__ inline void d_mm4(const double *A, const double *B, double *C) {
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++)
+      C[i * 4 + j] = A[i * 4 + 0] * B[0 * 4 + j] + A[i * 4 + 1] * B[1 * 4 + j] + A[i * 4 + 2] * B[2 * 4 + j] +
+                     A[i * 4 + 3] * B[3 * 4 + j];
+}
+
+__device__ inline void d_iso_inverse(const double *T, double *R) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) R[i * 4 + j] = T[j * 4 + i];
+  for (int i = 0; i < 3; i++)
+    R[i * 4 + 3] = -(R[i * 4 + 0] * T[3] + R[i * 4 + 1] * T[7] + R[i * 4 + 2] * T[11]);
+  R[12] = 0; R[13] = 0; R[14] = 0; R[15] = 1;
+}
+
+}  // namespace nicp

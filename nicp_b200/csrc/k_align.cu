@@ -1,0 +1,572 @@
+// k_align.cu -- projective ICP kernels (AlignerProjective::align and its parts).
+//
+//   k_zbuffer    PinholePointProjector::project (pinholepointprojector.cpp:33-66):
+//                one thread per point, 64-bit atomicMin of (depth key << 32 | index)
+//                into a per-pair z-buffer.  The serial reference keeps the first
+//                point with the strictly smallest depth, i.e. the minimum of
+//                (depth, index) -- exactly what the packed minimum keeps.
+//   k_resolve    z-buffer -> index image (+ depth image), resetting the z-buffer.
+//   k_corr_lin   fused CorrespondenceFinderProjective::_computeSingle
+//                (correspondencefinderprojective.cpp:23-115) and Linearizer::update
+//                (linearizer.cpp:21-134): per pixel, gate the pair, and if accepted
+//                add its 21 H + 6 b + chi2 + inlier terms.  Per-thread sums in FP32
+//                over 4 pixels, then FP64: warp butterfly reduce-scatter, shared
+//                memory, one partial per CTA tile (fixed tile -> partial mapping).
+//   k_corr_count / k_corr_write
+//                the same gates with ordered compaction into the reference's
+//                row-major correspondence list (parity / list mode).
+//   k_lin_list   Linearizer::update over a correspondence list (with the
+//                reference's K % T drop when T > 1).
+//   k_solve      per pair: fixed-order FP64 sum of the tile partials, H + lambda I,
+//                6x6 LDL^T, pose update and renormalisation (alignerprojective.cpp:
+//                72-100), early exit, and the float matrices of the next iteration.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace nicp {
+
+__device__ __forceinline__ int find_pair(const PairDev *pairs, int n, int key, bool points) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    int b = points ? pairs[mid].pt_tile_base : pairs[mid].tile_base;
+    if (b <= key) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------------ z-buffer
+// mode 0: project the current cloud with pair.KRt_cur-equivalent `explicit_KRt`
+// (one matrix for all pairs, host-computed); mode 1: the reference cloud with
+// the pair state's KRt.
+__global__ void __launch_bounds__(kPointsPerCta)
+    k_zbuffer(const PairDev *__restrict__ pairs, int npairs, int mode, const float *__restrict__ explicit_KRt) {
+  int pi = find_pair(pairs, npairs, blockIdx.x, true);
+  const PairDev &pd = pairs[pi];
+  const PairState *st = pd.state;
+  if (mode == 1 && st->done) return;
+  int i = (blockIdx.x - pd.pt_tile_base) * kPointsPerCta + threadIdx.x;
+  const float4 *pts = mode ? pd.ref_pts : pd.cur_pts;
+  int n = mode ? *pd.ref_count : *pd.cur_count;
+  if (i >= n) return;
+  float K[12];
+  const float *src = mode ? st->KRt : explicit_KRt + 12 * pi;
+#pragma unroll
+  for (int k = 0; k < 12; k++) K[k] = src[k];
+  int x, y;
+  float d;
+  if (!project_pixel(K, pts[i], pd.rows, pd.cols, pd.min_d, pd.max_d, x, y, d)) return;
+  unsigned long long key = ((unsigned long long)float_key(d) << 32) | (unsigned)i;
+  atomicMin(pd.zbuf + (size_t)y * pd.cols + x, key);
+}
+
+// z-buffer -> int index image (and optional depth image, FLT_MAX where empty);
+// the z-buffer is left all ones for its next use.
+__global__ void k_resolve(const PairDev *__restrict__ pairs, int npairs, int to_ref, float *depth_out) {
+  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  const PairDev &pd = pairs[pi];
+  int P = pd.rows * pd.cols;
+  int pix0 = (blockIdx.x - pd.tile_base) * kCorrTilePixels + threadIdx.x * 4;
+  int32_t *dst = to_ref ? pd.ref_index : pd.cur_index;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int p = pix0 + k;
+    if (p >= P) break;
+    unsigned long long z = pd.zbuf[p];
+    pd.zbuf[p] = ~0ull;
+    dst[p] = (z == ~0ull) ? -1 : (int)(unsigned)(z & 0xffffffffull);
+    if (depth_out) depth_out[p] = (z == ~0ull) ? 3.402823466e+38f : key_float((uint32_t)(z >> 32));
+  }
+}
+
+// ------------------------------------------------------------ gates + terms
+struct Acc {
+  // 0..5 Htt lower (00 10 11 20 21 22), 6..14 Htr row-major, 15..20 Hrr lower,
+  // 21..23 bt, 24..26 br, 27 chi2, 28 inliers, 29 candidates, 30 accepted
+  float v[31];
+};
+
+// correspondencefinderprojective.cpp:59-101.  T12: rows 0..2 of the gating
+// transform (the aligner passes _T.inverse()).
+__device__ __forceinline__ bool gate(const CorrParams &cp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
+                                     float4 cn) {
+  if (!cp.demoted) {
+    if (dot3x(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) return false;
+    if (dot3x(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return false;
+  }
+  float3 rp = xform_point(T12, rp0);
+  float dx = fsb(cpt.x, rp.x), dy = fsb(cpt.y, rp.y), dz = fsb(cpt.z, rp.z);
+  if (dot3x(dx, dy, dz, dx, dy, dz) > cp.sq_thr) return false;
+  if (!cp.demoted) {
+    float3 rn = xform_normal(T12, rn0);
+    if (dot3x(cn.x, cn.y, cn.z, rn.x, rn.y, rn.z) < cp.cos_thr) return false;
+    float kr = rn0.w, kc = cn.w;
+    if (kr < cp.flat_thr) kr = cp.flat_thr;
+    if (kc < cp.flat_thr) kc = cp.flat_thr;
+    float ratio = __double2float_rn(__ddiv_rn(__dadd_rn((double)kr, 1e-5), __dadd_rn((double)kc, 1e-5)));
+    if (ratio < cp.min_ratio || ratio > cp.max_ratio) return false;
+  }
+  return true;
+}
+
+// linearizer.cpp:59-100 for one correspondence, FP32.
+__device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
+                                         float4 cn, const float4 *omg, Acc &acc) {
+  float3 rp = xform_point(T12, rp0);
+  float3 rn = xform_normal(T12, rn0);
+  float4 o0 = omg[0], o1 = omg[1], o2 = omg[2];
+  // symmetric 3x3 as (00 01 02 11 12 22)
+  float Op[6] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y};
+  float On[6] = {o1.z, o1.w, o2.x, o2.y, o2.z, o2.w};
+#pragma unroll
+  for (int k = 0; k < 6; k++) On[k] = lp.scale * On[k];
+  if (lp.z_scaling) {
+    float f = 1.0f / fabsf(cpt.z);
+#pragma unroll
+    for (int k = 0; k < 6; k++) { Op[k] *= f; On[k] *= f; }
+  }
+  if (lp.demoted) {
+#pragma unroll
+    for (int k = 0; k < 6; k++) On[k] = 0.0f;
+  }
+  float pe[3] = {rp.x - cpt.x, rp.y - cpt.y, rp.z - cpt.z};
+  float ne[3] = {rn.x - cn.x, rn.y - cn.y, rn.z - cn.z};
+  float ep[3] = {Op[0] * pe[0] + Op[1] * pe[1] + Op[2] * pe[2], Op[1] * pe[0] + Op[3] * pe[1] + Op[4] * pe[2],
+                 Op[2] * pe[0] + Op[4] * pe[1] + Op[5] * pe[2]};
+  float en[3] = {On[0] * ne[0] + On[1] * ne[1] + On[2] * ne[2], On[1] * ne[0] + On[3] * ne[1] + On[4] * ne[2],
+                 On[2] * ne[0] + On[4] * ne[1] + On[5] * ne[2]};
+  float le = (pe[0] * ep[0] + pe[1] * ep[1] + pe[2] * ep[2]) + (ne[0] * en[0] + ne[1] * en[1] + ne[2] * en[2]);
+  float ks = 1.0f;
+  if (le > lp.max_chi2) {
+    if (lp.robust) ks = lp.max_chi2 / le;
+    else return;
+  }
+  acc.v[27] += ks * le;
+  acc.v[28] += 1.0f;
+  // skew(v) = [[0, c, -b], [-c, 0, a], [b, -a, 0]], (a, b, c) = 2 v
+  float a = 2.0f * rp.x, b = 2.0f * rp.y, c = 2.0f * rp.z;
+  float an = 2.0f * rn.x, bn = 2.0f * rn.y, cn2 = 2.0f * rn.z;
+  // Htt += Op * ks
+  acc.v[0] += Op[0] * ks; acc.v[1] += Op[1] * ks; acc.v[2] += Op[3] * ks;
+  acc.v[3] += Op[2] * ks; acc.v[4] += Op[4] * ks; acc.v[5] += Op[5] * ks;
+  // Htr += (Op Sp) ks: (Op S)_i0 = -c Op_i1 + b Op_i2; _i1 = c Op_i0 - a Op_i2; _i2 = -b Op_i0 + a Op_i1
+  const float Om[3][3] = {{Op[0], Op[1], Op[2]}, {Op[1], Op[3], Op[4]}, {Op[2], Op[4], Op[5]}};
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    acc.v[6 + i * 3 + 0] += (-c * Om[i][1] + b * Om[i][2]) * ks;
+    acc.v[6 + i * 3 + 1] += (c * Om[i][0] - a * Om[i][2]) * ks;
+    acc.v[6 + i * 3 + 2] += (-b * Om[i][0] + a * Om[i][1]) * ks;
+  }
+  // Hrr += (S^T O S) for the point and the normal terms
+  const float Nm[3][3] = {{On[0], On[1], On[2]}, {On[1], On[3], On[4]}, {On[2], On[4], On[5]}};
+  float Ap[3][3], An[3][3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    Ap[0][j] = -c * Om[1][j] + b * Om[2][j];
+    Ap[1][j] = c * Om[0][j] - a * Om[2][j];
+    Ap[2][j] = -b * Om[0][j] + a * Om[1][j];
+    An[0][j] = -cn2 * Nm[1][j] + bn * Nm[2][j];
+    An[1][j] = cn2 * Nm[0][j] - an * Nm[2][j];
+    An[2][j] = -bn * Nm[0][j] + an * Nm[1][j];
+  }
+  float R[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    R[i][0] = (-c * Ap[i][1] + b * Ap[i][2]) + (-cn2 * An[i][1] + bn * An[i][2]);
+    R[i][1] = (c * Ap[i][0] - a * Ap[i][2]) + (cn2 * An[i][0] - an * An[i][2]);
+    R[i][2] = (-b * Ap[i][0] + a * Ap[i][1]) + (-bn * An[i][0] + an * An[i][1]);
+  }
+  acc.v[15] += R[0][0] * ks; acc.v[16] += R[1][0] * ks; acc.v[17] += R[1][1] * ks;
+  acc.v[18] += R[2][0] * ks; acc.v[19] += R[2][1] * ks; acc.v[20] += R[2][2] * ks;
+  // bt += ks ep; br += ks (Sp^T ep + Sn^T en), S^T e = (2v) x e
+  acc.v[21] += ks * ep[0]; acc.v[22] += ks * ep[1]; acc.v[23] += ks * ep[2];
+  float u0 = b * ep[2] - c * ep[1], u1 = c * ep[0] - a * ep[2], u2 = a * ep[1] - b * ep[0];
+  float w0 = bn * en[2] - cn2 * en[1], w1 = cn2 * en[0] - an * en[2], w2 = an * en[1] - bn * en[0];
+  acc.v[24] += ks * (u0 + w0); acc.v[25] += ks * (u1 + w1); acc.v[26] += ks * (u2 + w2);
+}
+
+// Reduces every thread's Acc to one FP64 partial of the CTA (fixed order).
+__device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) {
+  __shared__ double wsum[kCorrThreads / 32][32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double v[32];
+#pragma unroll
+  for (int k = 0; k < 31; k++) v[k] = (double)acc.v[k];
+  v[31] = 0.0;
+  // butterfly reduce-scatter: lane L ends with the warp total of element L
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int j = 0; j < off; j++) {
+      double send = upper ? v[j] : v[j + off];
+      double keep = upper ? v[j + off] : v[j];
+      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  wsum[wid][lane] = v[0];
+  __syncthreads();
+  if (wid == 0) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kCorrThreads / 32; w++) s += wsum[w][lane];
+    out[lane] = s;
+  }
+}
+
+// flags: bit0 read the reference index from the z-buffer (else ref_index),
+// bit1 reset the z-buffer after reading, bit2 keep the resolved reference
+// index image, bit3 statistics pass (gate with Tgate_used; ignores `done`).
+__global__ void __launch_bounds__(kCorrThreads)
+    k_corr_lin(const PairDev *__restrict__ pairs, int npairs, CorrParams cp, LinParams lp, int flags) {
+  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  const PairDev &pd = pairs[pi];
+  PairState *st = pd.state;
+  bool stats_pass = flags & 8;
+  if (st->done && !stats_pass) return;
+  int tile = blockIdx.x - pd.tile_base;
+  int cols = pd.cols, P = pd.rows * cols;
+  int rmax = pd.rows;
+  if (cp.row_limit_threads > 1) rmax = (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
+  float Tg[12], Tl[12];
+  const float *gsrc = stats_pass ? st->Tgate_used : st->Tgate;
+#pragma unroll
+  for (int k = 0; k < 12; k++) { Tg[k] = gsrc[k]; Tl[k] = st->Tlin[k]; }
+  const int nref = *pd.ref_count, ncur = *pd.cur_count;
+  Acc acc;
+#pragma unroll
+  for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
+  int pix0 = tile * kCorrTilePixels + threadIdx.x * 4;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int p = pix0 + k;
+    if (p >= P) break;
+    int ri;
+    if (flags & 1) {
+      unsigned long long z = pd.zbuf[p];
+      if (flags & 2) pd.zbuf[p] = ~0ull;
+      ri = (z == ~0ull) ? -1 : (int)(unsigned)(z & 0xffffffffull);
+      if (flags & 4) pd.ref_index[p] = ri;
+    } else {
+      ri = pd.ref_index[p];
+    }
+    int ci = pd.cur_index[p];
+    if (ri < 0 || ci < 0 || ri >= nref || ci >= ncur) continue;
+    if (p / cols >= rmax) continue;
+    acc.v[29] += 1.0f;
+    float4 rp = pd.ref_pts[ri], rn = pd.ref_nrm[ri];
+    float4 cpt = pd.cur_pts[ci], cn = pd.cur_nrm[ci];
+    if (!gate(cp, Tg, rp, rn, cpt, cn)) continue;
+    acc.v[30] += 1.0f;
+    lin_terms(lp, Tl, rp, rn, cpt, cn, pd.cur_omg + 3 * (size_t)ci, acc);
+  }
+  block_reduce_store(acc, pd.partials + (size_t)tile * kPartialWords);
+}
+
+// ------------------------------------------------------------ list mode
+__device__ __forceinline__ unsigned list_mask(const PairDev &pd, const CorrParams &cp, const float *Tg, int pix0,
+                                              int P, int rmax) {
+  unsigned m = 0;
+  const int nref = *pd.ref_count, ncur = *pd.cur_count;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int p = pix0 + k;
+    if (p >= P) break;
+    int ri = pd.ref_index[p], ci = pd.cur_index[p];
+    if (ri < 0 || ci < 0 || ri >= nref || ci >= ncur || p / pd.cols >= rmax) continue;
+    if (gate(cp, Tg, pd.ref_pts[ri], pd.ref_nrm[ri], pd.cur_pts[ci], pd.cur_nrm[ci])) m |= 1u << k;
+  }
+  return m;
+}
+
+__global__ void __launch_bounds__(kCorrThreads) k_corr_count(const PairDev *__restrict__ pairs, int npairs, CorrParams cp,
+                                                             int use_state_T, const float *__restrict__ explicit_T) {
+  __shared__ int red[32];
+  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  const PairDev &pd = pairs[pi];
+  if (use_state_T && pd.state->done) return;
+  int tile = blockIdx.x - pd.tile_base;
+  int P = pd.rows * pd.cols;
+  int rmax = pd.rows;
+  if (cp.row_limit_threads > 1) rmax = (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
+  float Tg[12];
+  const float *src = use_state_T ? pd.state->Tgate : explicit_T + 12 * pi;
+#pragma unroll
+  for (int k = 0; k < 12; k++) Tg[k] = src[k];
+  unsigned m = list_mask(pd, cp, Tg, tile * kCorrTilePixels + threadIdx.x * 4, P, rmax);
+  int v = __popc(m);
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int i = 0; i < kCorrThreads / 32; i++) t += red[i];
+    pd.list_tile_counts[tile] = t;
+  }
+}
+
+__global__ void __launch_bounds__(kCorrThreads) k_corr_write(const PairDev *__restrict__ pairs, int npairs, CorrParams cp,
+                                                             int use_state_T, const float *__restrict__ explicit_T) {
+  __shared__ int red[32];
+  __shared__ int wsum[kCorrThreads / 32];
+  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  const PairDev &pd = pairs[pi];
+  if (use_state_T && pd.state->done) return;
+  int tile = blockIdx.x - pd.tile_base;
+  int P = pd.rows * pd.cols;
+  int ntiles = (P + kCorrTilePixels - 1) / kCorrTilePixels;
+  int rmax = pd.rows;
+  if (cp.row_limit_threads > 1) rmax = (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
+  float Tg[12];
+  const float *src = use_state_T ? pd.state->Tgate : explicit_T + 12 * pi;
+#pragma unroll
+  for (int k = 0; k < 12; k++) Tg[k] = src[k];
+  int before = 0;
+  for (int t = threadIdx.x; t < tile; t += blockDim.x) before += pd.list_tile_counts[t];
+  for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = before;
+  __syncthreads();
+  before = 0;
+  for (int i = 0; i < kCorrThreads / 32; i++) before += red[i];
+  int pix0 = tile * kCorrTilePixels + threadIdx.x * 4;
+  unsigned m = list_mask(pd, cp, Tg, pix0, P, rmax);
+  int cnt = __popc(m);
+  int inc = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) wsum[wid] = inc;
+  __syncthreads();
+  int woff = 0, btot = 0;
+  for (int i = 0; i < kCorrThreads / 32; i++) {
+    if (i < wid) woff += wsum[i];
+    btot += wsum[i];
+  }
+  int o = before + woff + inc - cnt;
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+    if (m & (1u << k)) {
+      int p = pix0 + k;
+      pd.pairs[2 * o] = pd.ref_index[p];
+      pd.pairs[2 * o + 1] = pd.cur_index[p];
+      o++;
+    }
+  if (tile == ntiles - 1 && threadIdx.x == 0) *pd.num_pairs = before + btot;
+}
+
+// Linearizer::update over pd.pairs[0, K - K % T).  Tiles cover list slots.
+// use_state_T: 0 explicit T, 1 the pair state's Tlin (skipping converged
+// pairs), 2 the state's Tlin for every pair (statistics pass).
+__global__ void __launch_bounds__(kCorrThreads) k_lin_list(const PairDev *__restrict__ pairs, int npairs, LinParams lp,
+                                                           int parity_threads, int use_state_T,
+                                                           const float *__restrict__ explicit_T) {
+  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  const PairDev &pd = pairs[pi];
+  if (use_state_T == 1 && pd.state->done) return;
+  int tile = blockIdx.x - pd.tile_base;
+  int K = *pd.num_pairs;
+  if (parity_threads > 1) K = (K / parity_threads) * parity_threads;
+  float Tl[12];
+  const float *src = use_state_T ? pd.state->Tlin : explicit_T + 12 * pi;
+#pragma unroll
+  for (int k = 0; k < 12; k++) Tl[k] = src[k];
+  const int nref = *pd.ref_count, ncur = *pd.cur_count;
+  Acc acc;
+#pragma unroll
+  for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
+  int i0 = tile * kCorrTilePixels + threadIdx.x * 4;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int i = i0 + k;
+    if (i >= K) break;
+    int ri = pd.pairs[2 * i], ci = pd.pairs[2 * i + 1];
+    if (ri < 0 || ci < 0 || ri >= nref || ci >= ncur) continue;
+    acc.v[29] += 1.0f;
+    acc.v[30] += 1.0f;
+    lin_terms(lp, Tl, pd.ref_pts[ri], pd.ref_nrm[ri], pd.cur_pts[ci], pd.cur_nrm[ci], pd.cur_omg + 3 * (size_t)ci,
+              acc);
+  }
+  block_reduce_store(acc, pd.partials + (size_t)tile * kPartialWords);
+}
+
+// ------------------------------------------------------------ solve
+__device__ inline void float12_of(const double *T, float *o) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 4; j++) o[i * 4 + j] = (float)T[i * 4 + j];
+}
+
+// KRt of the projector placed at X (pinholepointprojector.cpp:16-31), in FP64.
+__device__ inline void krt_of(const float *K, const double *X, float *o) {
+  double t[16];
+  d_iso_inverse(X, t);
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 3; j++)
+      o[i * 4 + j] = (float)((double)K[i * 3 + 0] * t[0 * 4 + j] + (double)K[i * 3 + 1] * t[1 * 4 + j] +
+                             (double)K[i * 3 + 2] * t[2 * 4 + j]);
+    o[i * 4 + 3] = (float)((double)K[i * 3 + 0] * t[3] + (double)K[i * 3 + 1] * t[7] + (double)K[i * 3 + 2] * t[11]);
+  }
+}
+
+// Prepares the matrices of an outer iteration from st->T.
+__device__ inline void begin_outer(const PairDev &pd, PairState *st) {
+  for (int k = 0; k < 16; k++) st->Tstart[k] = st->T[k];
+  double X[16];
+  d_mm4(st->T, st->ref_offset, X);
+  krt_of(pd.K, X, st->KRt);
+  d_iso_inverse(st->T, st->invT);
+  float12_of(st->invT, st->Tgate);
+  float12_of(st->invT, st->Tlin);
+}
+
+__global__ void k_init_pairs(const PairDev *__restrict__ pairs, int npairs, const double *__restrict__ guesses,
+                             const double *__restrict__ ref_offsets) {
+  int pi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pi >= npairs) return;
+  const PairDev &pd = pairs[pi];
+  PairState *st = pd.state;
+  for (int k = 0; k < 16; k++) {
+    st->T[k] = guesses[16 * pi + k];
+    st->ref_offset[k] = ref_offsets[16 * pi + k];
+  }
+  st->T[12] = 0; st->T[13] = 0; st->T[14] = 0; st->T[15] = 1;
+  st->error = 0; st->inliers = 0; st->num_corr = 0; st->candidates = 0;
+  st->iterations = 0; st->done = 0; st->status = 0;
+  for (int k = 0; k < 36; k++) st->H[k] = 0;
+  for (int k = 0; k < 6; k++) st->b[k] = 0;
+  begin_outer(pd, st);
+  for (int k = 0; k < 12; k++) st->Tgate_used[k] = st->Tgate[k];
+}
+
+// mode: bit0 last inner iteration of the outer loop, bit1 reduce only (no
+// pose update: Linearizer results of a list pass), bit2 statistics pass
+// (reduce into Hstat only).
+__global__ void __launch_bounds__(128) k_solve(const PairDev *__restrict__ pairs, int npairs, float lambda, int mode,
+                                              double early_eps, int ignore_done) {
+  __shared__ double part[4][32];
+  __shared__ double tot[32];
+  const PairDev &pd = pairs[blockIdx.x];
+  PairState *st = pd.state;
+  if (st->done && !ignore_done) return;
+  int P = pd.rows * pd.cols;
+  int nt = (P + kCorrTilePixels - 1) / kCorrTilePixels;
+  int e = threadIdx.x & 31, g = threadIdx.x >> 5;
+  double s = 0.0;
+  for (int t = g; t < nt; t += 4) s += pd.partials[(size_t)t * kPartialWords + e];
+  part[g][e] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) tot[e] = ((part[0][e] + part[1][e]) + part[2][e]) + part[3][e];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const int li[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
+  double H[36], b[6];
+  for (int q = 0; q < 6; q++) {
+    int i = li[q][0], j = li[q][1];
+    H[i * 6 + j] = H[j * 6 + i] = tot[q];
+    H[(3 + i) * 6 + 3 + j] = H[(3 + j) * 6 + 3 + i] = tot[15 + q];
+  }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      H[i * 6 + 3 + j] = tot[6 + i * 3 + j];
+      H[(3 + j) * 6 + i] = tot[6 + i * 3 + j];
+    }
+  for (int i = 0; i < 3; i++) { b[i] = tot[21 + i]; b[3 + i] = tot[24 + i]; }
+  if (mode & 4) {
+    for (int k = 0; k < 36; k++) st->Hstat[k] = H[k];
+    return;
+  }
+  for (int k = 0; k < 36; k++) st->H[k] = H[k];
+  for (int k = 0; k < 6; k++) st->b[k] = b[k];
+  st->error = (float)tot[27];
+  st->inliers = (int)tot[28];
+  st->candidates = (int)tot[29];
+  st->num_corr = (int)tot[30];
+  if (mode & 2) return;
+  // H += lambda I; dx = H^-1 (-b); invT = v2t(dx) invT  (alignerprojective.cpp:72-95)
+  double A[36], nb[6], dx[6];
+  for (int k = 0; k < 36; k++) A[k] = H[k];
+  for (int i = 0; i < 6; i++) { A[i * 6 + i] += (double)lambda; nb[i] = -b[i]; }
+  d_ldlt_solve6(A, nb, dx);
+  double dT[16], nT[16];
+  d_v2t(dx, dT);
+  d_mm4(dT, st->invT, nT);
+  for (int k = 0; k < 16; k++) st->invT[k] = nT[k];
+  st->invT[12] = 0; st->invT[13] = 0; st->invT[14] = 0; st->invT[15] = 1;
+  float12_of(st->invT, st->Tlin);
+  if (!(mode & 1)) return;
+  // T = invT^-1, renormalised through t2v/v2t (alignerprojective.cpp:98-100)
+  double T[16], x[6];
+  d_iso_inverse(st->invT, T);
+  d_t2v(T, x);
+  d_v2t(x, st->T);
+  st->iterations += 1;
+  for (int k = 0; k < 12; k++) st->Tgate_used[k] = st->Tgate[k];
+  if (early_eps > 0) {
+    double Si[16], D[16], dv[6];
+    d_iso_inverse(st->Tstart, Si);
+    d_mm4(st->T, Si, D);
+    d_t2v(D, dv);
+    double m = 0;
+    for (int k = 0; k < 6; k++) m = fmax(m, fabs(dv[k]));
+    if (m < early_eps) st->done = 1;
+  }
+  begin_outer(pd, st);
+}
+
+// ------------------------------------------------------------ launchers
+void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int mode, const float *explicit_KRt,
+                    cudaStream_t s, Profiler *prof) {
+  if (total_pt_tiles <= 0) return;
+  prof->begin(NICP_K_ZBUFFER, s);
+  k_zbuffer<<<total_pt_tiles, kPointsPerCta, 0, s>>>(d_pairs, npairs, mode, explicit_KRt);
+  prof->end(NICP_K_ZBUFFER, s);
+}
+
+void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out, cudaStream_t s,
+                    Profiler *prof) {
+  prof->begin(NICP_K_RESOLVE, s);
+  k_resolve<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, to_ref, depth_out);
+  prof->end(NICP_K_RESOLVE, s);
+}
+
+void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
+                     int flags, cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_CORR_LIN, s);
+  k_corr_lin<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, cp, lp, flags);
+  prof->end(NICP_K_CORR_LIN, s);
+}
+
+void launch_corr_list(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, int use_state_T,
+                      const float *explicit_T, cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_CORR_LIST, s);
+  k_corr_count<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, cp, use_state_T, explicit_T);
+  k_corr_write<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, cp, use_state_T, explicit_T);
+  prof->end(NICP_K_CORR_LIST, s, 2);
+}
+
+void launch_lin_list(const PairDev *d_pairs, int npairs, int total_tiles, const LinParams &lp, int parity_threads,
+                     int use_state_T, const float *explicit_T, cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_LIN_LIST, s);
+  k_lin_list<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, lp, parity_threads, use_state_T, explicit_T);
+  prof->end(NICP_K_LIN_LIST, s);
+}
+
+void launch_init_pairs(const PairDev *d_pairs, int npairs, const double *d_guesses, const double *d_ref_offsets,
+                       cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_SOLVE, s);
+  k_init_pairs<<<(npairs + 63) / 64, 64, 0, s>>>(d_pairs, npairs, d_guesses, d_ref_offsets);
+  prof->end(NICP_K_SOLVE, s);
+}
+
+void launch_solve(const PairDev *d_pairs, int npairs, float lambda, int mode, double early_eps, int ignore_done,
+                  cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_SOLVE, s);
+  k_solve<<<npairs, 128, 0, s>>>(d_pairs, npairs, lambda, mode, early_eps, ignore_done);
+  prof->end(NICP_K_SOLVE, s);
+}
+
+}  // namespace nicp

@@ -1,0 +1,554 @@
+// k_cloud.cu -- depth image -> cloud kernels (DepthImageConverterIntegralImage::compute).
+//
+//   k_unproject_count / k_unproject_write
+//       u16 (or f32) depth -> index image + points, with the reference's
+//       row-major point numbering (pinholepointprojector.cpp:93-134).  Each
+//       CTA owns a 4096-pixel tile; 16 pixels per thread are read with two
+//       128-bit loads.  The first pass counts valid pixels per tile, the second
+//       re-reads the tile (from L2), sums the counts of the preceding tiles of
+//       its frame and writes indices and points at their final positions.
+//   k_moments_rows / k_moments_cols
+//       integral image of the 10 unique point moments (n, Sx, Sy, Sz, Sxx,
+//       Sxy, Sxz, Syy, Syz, Szz) -- pointintegralimage.cpp:7-44 -- as 10
+//       planes.  Rows: one CTA per image row, block scans with carries.
+//       Columns: one CTA per (plane, 32-column strip); each warp scans a band
+//       of rows, band totals are combined through shared memory.
+//   k_stats
+//       one thread per pixel: interval radius, 4-corner box query, 3x3
+//       covariance, FP64 eigensolve, curvature, oriented normal, and both
+//       information matrices (statscalculatorintegralimage.cpp:20-82,
+//       informationmatrixcalculator.cpp:9-57).
+//   k_cloud_transform
+//       Cloud::transformInPlace (cloud.cpp:191-204).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace nicp {
+
+// ------------------------------------------------------------ frame lookup
+template <int Field>
+__device__ __forceinline__ int frame_base(const FrameDev &f) {
+  if (Field == 0) return f.tile_base;
+  if (Field == 1) return f.row_base;
+  if (Field == 2) return f.stat_tile_base;
+  return f.col_base;
+}
+
+// Largest i with base(frames[i]) <= key.
+template <int Field>
+__device__ __forceinline__ int find_frame(const FrameDev *frames, int n, int key) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (frame_base<Field>(frames[mid]) <= key) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------------ unprojection
+// Loads the depth of 16 consecutive pixels starting at pix0; pixels at or
+// beyond P read as 0 (invalid).
+__device__ __forceinline__ void load16(const FrameDev &f, int pix0, int P, float d[16]) {
+  if (f.depth_u16) {
+    if (pix0 + 16 <= P && ((reinterpret_cast<uintptr_t>(f.depth_u16 + pix0) & 15) == 0)) {
+      const uint4 *src = reinterpret_cast<const uint4 *>(f.depth_u16 + pix0);
+      uint4 a = __ldg(src), b = __ldg(src + 1);
+      uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        uint32_t lo = w[k] & 0xffffu, hi = w[k] >> 16;
+        d[2 * k] = lo ? fm(f.depth_scale, (float)(int)lo) : 0.0f;
+        d[2 * k + 1] = hi ? fm(f.depth_scale, (float)(int)hi) : 0.0f;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        int p = pix0 + k;
+        uint16_t u = (p < P) ? f.depth_u16[p] : 0;
+        d[k] = u ? fm(f.depth_scale, (float)(int)u) : 0.0f;
+      }
+    }
+  } else {
+    if (pix0 + 16 <= P && ((reinterpret_cast<uintptr_t>(f.depth_f32 + pix0) & 15) == 0)) {
+      const float4 *src = reinterpret_cast<const float4 *>(f.depth_f32 + pix0);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        float4 v = __ldg(src + k);
+        d[4 * k] = v.x; d[4 * k + 1] = v.y; d[4 * k + 2] = v.z; d[4 * k + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        int p = pix0 + k;
+        d[k] = (p < P) ? f.depth_f32[p] : 0.0f;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int block_sum_int(int v, int *smem) {
+  // 256 threads
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) smem[wid] = v;
+  __syncthreads();
+  int t = 0;
+  for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += smem[i];
+  return t;
+}
+
+__global__ void __launch_bounds__(256) k_unproject_count(const FrameDev *__restrict__ frames, int nframes) {
+  __shared__ int red[32];
+  int fi = find_frame<0>(frames, nframes, blockIdx.x);
+  const FrameDev &f = frames[fi];
+  int tile = blockIdx.x - f.tile_base;
+  int P = f.rows * f.cols;
+  int pix0 = tile * kUnprojTilePixels + threadIdx.x * 16;
+  float d[16];
+  load16(f, pix0, P, d);
+  int cnt = 0;
+#pragma unroll
+  for (int k = 0; k < 16; k++) cnt += depth_valid(d[k], f.min_d, f.max_d) ? 1 : 0;
+  int tot = block_sum_int(cnt, red);
+  if (threadIdx.x == 0) f.tile_counts[tile] = tot;
+}
+
+__global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restrict__ frames, int nframes) {
+  __shared__ int red[32];
+  __shared__ int wsum[8];
+  int fi = find_frame<0>(frames, nframes, blockIdx.x);
+  const FrameDev &f = frames[fi];
+  int tile = blockIdx.x - f.tile_base;
+  int P = f.rows * f.cols;
+  int ntiles = (P + kUnprojTilePixels - 1) / kUnprojTilePixels;
+  // points numbered before this tile
+  int before = 0;
+  for (int t = threadIdx.x; t < tile; t += blockDim.x) before += f.tile_counts[t];
+  before = block_sum_int(before, red);
+  int pix0 = tile * kUnprojTilePixels + threadIdx.x * 16;
+  float d[16];
+  load16(f, pix0, P, d);
+  unsigned mask = 0;
+#pragma unroll
+  for (int k = 0; k < 16; k++) mask |= (depth_valid(d[k], f.min_d, f.max_d) ? 1u : 0u) << k;
+  int cnt = __popc(mask);
+  // exclusive block scan of cnt
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int inc = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) wsum[wid] = inc;
+  __syncthreads();
+  int woff = 0, btot = 0;
+  for (int i = 0; i < 8; i++) {
+    if (i < wid) woff += wsum[i];
+    btot += wsum[i];
+  }
+  int idx = before + woff + inc - cnt;
+  int out[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    out[k] = -1;
+    if (mask & (1u << k)) {
+      int p = pix0 + k;
+      int r = p / f.cols, c = p - r * f.cols;
+      f.pts[idx] = unproject_pixel(f.iKRt, c, r, d[k]);
+      out[k] = idx++;
+    }
+  }
+  if (pix0 + 16 <= P && ((reinterpret_cast<uintptr_t>(f.index + pix0) & 15) == 0)) {
+    int4 *dst = reinterpret_cast<int4 *>(f.index + pix0);
+#pragma unroll
+    for (int k = 0; k < 4; k++) dst[k] = make_int4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      if (pix0 + k < P) f.index[pix0 + k] = out[k];
+  }
+  if (tile == ntiles - 1 && threadIdx.x == 0) *f.count = before + btot;
+}
+
+// ------------------------------------------------------------ moments
+// Storage policies for the integral image.
+struct MomF64 {
+  typedef double T;
+  __device__ static double load(const void *base, size_t i) { return static_cast<const double *>(base)[i]; }
+  __device__ static void store(void *base, size_t i, double v) { static_cast<double *>(base)[i] = v; }
+};
+struct MomF32 {
+  typedef float T;
+  __device__ static double load(const void *base, size_t i) { return (double)static_cast<const float *>(base)[i]; }
+  __device__ static void store(void *base, size_t i, double v) { static_cast<float *>(base)[i] = (float)v; }
+};
+// Two-float: an unevaluated sum hi + lo of two floats (about 48 significant
+// bits); values travel as double inside the kernels and are split on store.
+struct MomTwoFloat {
+  typedef float2 T;
+  __device__ static double load(const void *base, size_t i) {
+    float2 v = static_cast<const float2 *>(base)[i];
+    return (double)v.x + (double)v.y;
+  }
+  __device__ static void store(void *base, size_t i, double v) {
+    float hi = (float)v;
+    float lo = (float)(v - (double)hi);
+    static_cast<float2 *>(base)[i] = make_float2(hi, lo);
+  }
+};
+
+// The arithmetic type the moments are accumulated in for each storage.
+template <class M> struct MomAcc { typedef double T; };
+template <> struct MomAcc<MomF32> { typedef float T; };
+
+__device__ __forceinline__ void point_moments(float4 p, bool valid, double m[10]) {
+  double x = p.x, y = p.y, z = p.z;
+  double v = valid ? 1.0 : 0.0;
+  m[0] = v;
+  m[1] = v * x; m[2] = v * y; m[3] = v * z;
+  m[4] = v * x * x; m[5] = v * x * y; m[6] = v * x * z;
+  m[7] = v * y * y; m[8] = v * y * z; m[9] = v * z * z;
+}
+__device__ __forceinline__ void point_moments(float4 p, bool valid, float m[10]) {
+  float x = p.x, y = p.y, z = p.z;
+  float v = valid ? 1.0f : 0.0f;
+  m[0] = v;
+  m[1] = v * x; m[2] = v * y; m[3] = v * z;
+  m[4] = v * fm(x, x); m[5] = v * fm(x, y); m[6] = v * fm(x, z);
+  m[7] = v * fm(y, y); m[8] = v * fm(y, z); m[9] = v * fm(z, z);
+}
+
+constexpr int kRowThreads = 128;
+constexpr int kRowPix = 4;
+
+// One CTA per image row: inclusive prefix along x of the 10 moments.  Each
+// thread keeps the points of its 4 pixels; the moments are formed twice
+// (for the thread total, then at store time) to keep register use low.
+template <class M>
+__global__ void __launch_bounds__(kRowThreads) k_moments_rows(const FrameDev *__restrict__ frames, int nframes) {
+  typedef typename MomAcc<M>::T A;
+  __shared__ A wtot[kRowThreads / 32][10];
+  int fi = find_frame<1>(frames, nframes, blockIdx.x);
+  const FrameDev &f = frames[fi];
+  int r = blockIdx.x - f.row_base;
+  int cols = f.cols;
+  size_t P = (size_t)f.rows * cols;
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  A carry[10];
+#pragma unroll
+  for (int m = 0; m < 10; m++) carry[m] = A(0);
+  for (int x0 = 0; x0 < cols; x0 += kRowThreads * kRowPix) {
+    int c0 = x0 + threadIdx.x * kRowPix;
+    float4 pt[kRowPix];
+    unsigned vmask = 0;
+    A acc[10];
+#pragma unroll
+    for (int m = 0; m < 10; m++) acc[m] = A(0);
+#pragma unroll
+    for (int k = 0; k < kRowPix; k++) {
+      int c = c0 + k;
+      bool in = c < cols;
+      float d = in ? depth_of(f, r * cols + c) : 0.0f;
+      bool valid = in && depth_valid(d, f.min_d, f.max_d);
+      pt[k] = valid ? unproject_pixel(f.iKRt, c, r, d) : make_float4(0, 0, 0, 0);
+      vmask |= (valid ? 1u : 0u) << k;
+      A mk[10];
+      point_moments(pt[k], valid, mk);
+#pragma unroll
+      for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
+    }
+    // warp inclusive scan of the thread totals; acc becomes the exclusive offset
+#pragma unroll
+    for (int m = 0; m < 10; m++) {
+      A inc = acc[m];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        A y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc = inc + y;
+      }
+      if (lane == 31) wtot[wid][m] = inc;
+      acc[m] = inc - acc[m];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 10; m++) {
+      A off = carry[m] + acc[m], tot = A(0);
+      for (int w = 0; w < kRowThreads / 32; w++) {
+        A t = wtot[w][m];
+        if (w < wid) off = off + t;
+        tot = tot + t;
+      }
+      acc[m] = off;
+      carry[m] = carry[m] + tot;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kRowPix; k++) {
+      int c = c0 + k;
+      A mk[10];
+      point_moments(pt[k], (vmask >> k) & 1u, mk);
+#pragma unroll
+      for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
+      if (c < cols) {
+        size_t i = (size_t)r * cols + c;
+#pragma unroll
+        for (int m = 0; m < 10; m++) M::store(f.moments, m * P + i, (double)acc[m]);
+      }
+    }
+  }
+}
+
+constexpr int kColWarps = 8;
+constexpr int kColBatch = 8;
+
+// One CTA per (plane, 32-column strip): inclusive prefix along y.  Each warp
+// scans a band of rows (lane = column), loading kColBatch rows ahead; band
+// totals are combined through shared memory and added in a second pass.
+template <class M>
+__global__ void __launch_bounds__(32 * kColWarps) k_moments_cols(const FrameDev *__restrict__ frames, int nframes) {
+  typedef typename MomAcc<M>::T A;
+  __shared__ A btot[kColWarps][32];
+  int fi = find_frame<3>(frames, nframes, blockIdx.x);
+  const FrameDev &f = frames[fi];
+  int local = blockIdx.x - f.col_base;
+  int strips = (f.cols + 31) / 32;
+  int plane = local / strips, strip = local - plane * strips;
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = strip * 32 + lane;
+  int rows = f.rows, cols = f.cols;
+  size_t P = (size_t)rows * cols;
+  int band = (rows + kColWarps - 1) / kColWarps;
+  int y0 = wid * band, y1 = min(rows, y0 + band);
+  size_t base = (size_t)plane * P + x;
+  A s = A(0);
+  if (x < cols) {
+    for (int y = y0; y < y1; y += kColBatch) {
+      A v[kColBatch];
+#pragma unroll
+      for (int k = 0; k < kColBatch; k++)
+        v[k] = (y + k < y1) ? (A)M::load(f.moments, base + (size_t)(y + k) * cols) : A(0);
+#pragma unroll
+      for (int k = 0; k < kColBatch; k++) {
+        s = s + v[k];
+        if (y + k < y1) M::store(f.moments, base + (size_t)(y + k) * cols, (double)s);
+      }
+    }
+  }
+  btot[wid][lane] = s;
+  __syncthreads();
+  A carry = A(0);
+  for (int w = 0; w < wid; w++) carry = carry + btot[w][lane];
+  if (x < cols && wid > 0) {
+    for (int y = y0; y < y1; y += kColBatch) {
+      A v[kColBatch];
+#pragma unroll
+      for (int k = 0; k < kColBatch; k++)
+        v[k] = (y + k < y1) ? (A)M::load(f.moments, base + (size_t)(y + k) * cols) : A(0);
+#pragma unroll
+      for (int k = 0; k < kColBatch; k++)
+        if (y + k < y1) M::store(f.moments, base + (size_t)(y + k) * cols, (double)(v[k] + carry));
+    }
+  }
+}
+
+// ------------------------------------------------------------ stats + omegas
+template <class M>
+__global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restrict__ frames, int nframes) {
+  int fi = find_frame<2>(frames, nframes, blockIdx.x);
+  const FrameDev &f = frames[fi];
+  int pix = (blockIdx.x - f.stat_tile_base) * kStatsThreads + threadIdx.x;
+  int rows = f.rows, cols = f.cols;
+  int P = rows * cols;
+  if (pix >= P) return;
+  int idx = f.index[pix];
+  if (idx < 0) return;
+  int r = pix / cols, c = pix - r * cols;
+  float d = depth_of(f, pix);
+  float4 nout = make_float4(0.f, 0.f, 0.f, 0.f);
+  float om[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) om[k] = 0.f;
+  double lam[3] = {0, 0, 0};
+  double U[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  bool reached = false;
+  int rad = interval_radius(f.K, d, f.min_d, f.max_d, f.world_radius);
+  if (rad >= 0 && rad >= f.min_radius) {
+    if (rad > f.max_radius) rad = f.max_radius;
+    // pointintegralimage.cpp:53-66
+    int xm = min(max(c - rad - 1, 0), cols - 1), xM = min(max(c + rad - 1, 0), cols - 1);
+    int ym = min(max(r - rad - 1, 0), rows - 1), yM = min(max(r + rad - 1, 0), rows - 1);
+    size_t iA = (size_t)yM * cols + xM, iB = (size_t)ym * cols + xm;
+    size_t iC = (size_t)yM * cols + xm, iD = (size_t)ym * cols + xM;
+    double S[10];
+#pragma unroll
+    for (int m = 0; m < 10; m++) {
+      size_t o = (size_t)m * P;
+      double s = M::load(f.moments, o + iA) + M::load(f.moments, o + iB);
+      s = s - M::load(f.moments, o + iC);
+      s = s - M::load(f.moments, o + iD);
+      S[m] = s;
+    }
+    int n = (int)S[0];
+    if (n >= f.min_points) {
+      double dn = 1.0 / S[0];
+      double mu0 = S[1] * dn, mu1 = S[2] * dn, mu2 = S[3] * dn;
+      double C[6] = {S[4] * dn - mu0 * mu0, S[5] * dn - mu0 * mu1, S[6] * dn - mu0 * mu2,
+                     S[7] * dn - mu1 * mu1, S[8] * dn - mu1 * mu2, S[9] * dn - mu2 * mu2};
+      d_eig3(C, lam, U);
+      if (lam[0] < 0) lam[0] = 0;
+      reached = true;
+      double kappa = lam[0] / (((lam[0] + lam[1]) + lam[2]) + 1e-9);
+      nout.w = (float)kappa;
+      if (kappa < (double)f.curv_thr) {
+        float4 p = unproject_pixel(f.iKRt, c, r, d);
+        double nx = U[0], ny = U[3], nz = U[6];
+        if (nx * p.x + ny * p.y + nz * p.z > 0) { nx = -nx; ny = -ny; nz = -nz; }
+        nout.x = (float)nx; nout.y = (float)ny; nout.z = (float)nz;
+        // information matrices: Omega = U diag(D) U^T
+        double Dp[3], Dn[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          Dp[k] = (kappa < (double)f.pim_thr) ? f.pim_flat[k] : f.pim_nonflat[k];
+          Dn[k] = (kappa < (double)f.nim_thr) ? f.nim_flat[k] : f.nim_nonflat[k];
+        }
+        const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+          int i = ii[e], j = jj[e];
+          double sp = 0, sn = 0;
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            double uu = U[i * 3 + k] * U[j * 3 + k];
+            sp += Dp[k] * uu;
+            sn += Dn[k] * uu;
+          }
+          om[e] = (float)sp;
+          om[6 + e] = (float)sn;
+        }
+      }
+    }
+  }
+  f.nrm[idx] = nout;
+  float4 *o = f.omg + 3 * (size_t)idx;
+  o[0] = make_float4(om[0], om[1], om[2], om[3]);
+  o[1] = make_float4(om[4], om[5], om[6], om[7]);
+  o[2] = make_float4(om[8], om[9], om[10], om[11]);
+  if (f.keep_stats) {
+    float *e = f.eig + 12 * (size_t)idx;
+    if (!reached) { lam[0] = lam[1] = lam[2] = 0; }
+    e[0] = (float)lam[0]; e[1] = (float)lam[1]; e[2] = (float)lam[2];
+#pragma unroll
+    for (int k = 0; k < 9; k++) e[3 + k] = (float)U[k];
+  }
+}
+
+// ------------------------------------------------------------ transform
+__global__ void k_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, const int *count, int capacity,
+                                  const float *__restrict__ m12) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= capacity || i >= *count) return;
+  float A[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) A[k] = m12[k];
+  float3 p = xform_point(A, pts[i]);
+  pts[i] = make_float4(p.x, p.y, p.z, 1.0f);
+  float4 n0 = nrm[i];
+  float3 n = xform_normal(A, n0);
+  nrm[i] = make_float4(n.x, n.y, n.z, n0.w);
+  // Omega' = (R Omega) R^T over the 3x3 block
+  float4 o0 = omg[3 * i], o1 = omg[3 * i + 1], o2 = omg[3 * i + 2];
+  float Op[9] = {o0.x, o0.y, o0.z, o0.y, o0.w, o1.x, o0.z, o1.x, o1.y};
+  float On[9] = {o1.z, o1.w, o2.x, o1.w, o2.y, o2.z, o2.x, o2.z, o2.w};
+  float R[9] = {A[0], A[1], A[2], A[4], A[5], A[6], A[8], A[9], A[10]};
+  float res[2][6];
+  for (int w = 0; w < 2; w++) {
+    const float *O = w ? On : Op;
+    float RO[9];
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++)
+        RO[a * 3 + b] = fa(fa(fm(R[a * 3 + 0], O[0 * 3 + b]), fm(R[a * 3 + 1], O[1 * 3 + b])), fm(R[a * 3 + 2], O[2 * 3 + b]));
+    const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
+    for (int e = 0; e < 6; e++) {
+      int a = ii[e], b = jj[e];
+      res[w][e] = fa(fa(fm(RO[a * 3 + 0], R[b * 3 + 0]), fm(RO[a * 3 + 1], R[b * 3 + 1])), fm(RO[a * 3 + 2], R[b * 3 + 2]));
+    }
+  }
+  omg[3 * i] = make_float4(res[0][0], res[0][1], res[0][2], res[0][3]);
+  omg[3 * i + 1] = make_float4(res[0][4], res[0][5], res[1][0], res[1][1]);
+  omg[3 * i + 2] = make_float4(res[1][2], res[1][3], res[1][4], res[1][5]);
+  if (eig) {
+    float *e = eig + 12 * (size_t)i;
+    float U[9];
+    for (int k = 0; k < 9; k++) U[k] = e[3 + k];
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++)
+        e[3 + a * 3 + b] = fa(fa(fm(R[a * 3 + 0], U[0 * 3 + b]), fm(R[a * 3 + 1], U[1 * 3 + b])), fm(R[a * 3 + 2], U[2 * 3 + b]));
+  }
+}
+
+// PinholePointProjector::projectIntervals (pinholepointprojector.cpp:136-148).
+__global__ void k_intervals(const float *__restrict__ depth, int P, const float *__restrict__ K9, float min_d, float max_d,
+                            float R, int32_t *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  float K[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) K[k] = K9[k];
+  out[i] = interval_radius(K, depth[i], min_d, max_d, R);
+}
+
+// ------------------------------------------------------------ launchers
+void launch_intervals(const float *d_depth, int P, const float *d_K9, float min_d, float max_d, float R, int32_t *d_out,
+                      cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_STATS, s);
+  if (P > 0) k_intervals<<<(P + 255) / 256, 256, 0, s>>>(d_depth, P, d_K9, min_d, max_d, R, d_out);
+  prof->end(NICP_K_STATS, s);
+}
+
+void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_UNPROJECT, s);
+  k_unproject_count<<<total_tiles, 256, 0, s>>>(d_frames, nframes);
+  k_unproject_write<<<total_tiles, 256, 0, s>>>(d_frames, nframes);
+  prof->end(NICP_K_UNPROJECT, s, 2);
+}
+
+void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_rows, int total_col_ctas,
+                    cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_MOMENTS_ROWS, s);
+  if (precision == NICP_MOMENTS_F32) k_moments_rows<MomF32><<<total_rows, kRowThreads, 0, s>>>(d_frames, nframes);
+  else if (precision == NICP_MOMENTS_TWOFLOAT) k_moments_rows<MomTwoFloat><<<total_rows, kRowThreads, 0, s>>>(d_frames, nframes);
+  else k_moments_rows<MomF64><<<total_rows, kRowThreads, 0, s>>>(d_frames, nframes);
+  prof->end(NICP_K_MOMENTS_ROWS, s);
+  prof->begin(NICP_K_MOMENTS_COLS, s);
+  if (precision == NICP_MOMENTS_F32) k_moments_cols<MomF32><<<total_col_ctas, 32 * kColWarps, 0, s>>>(d_frames, nframes);
+  else if (precision == NICP_MOMENTS_TWOFLOAT) k_moments_cols<MomTwoFloat><<<total_col_ctas, 32 * kColWarps, 0, s>>>(d_frames, nframes);
+  else k_moments_cols<MomF64><<<total_col_ctas, 32 * kColWarps, 0, s>>>(d_frames, nframes);
+  prof->end(NICP_K_MOMENTS_COLS, s);
+}
+
+void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_STATS, s);
+  if (precision == NICP_MOMENTS_F32) k_stats<MomF32><<<total_tiles, kStatsThreads, 0, s>>>(d_frames, nframes);
+  else if (precision == NICP_MOMENTS_TWOFLOAT) k_stats<MomTwoFloat><<<total_tiles, kStatsThreads, 0, s>>>(d_frames, nframes);
+  else k_stats<MomF64><<<total_tiles, kStatsThreads, 0, s>>>(d_frames, nframes);
+  prof->end(NICP_K_STATS, s);
+}
+
+void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, const int *count, int capacity,
+                            const float *d_m12, cudaStream_t s, Profiler *prof) {
+  prof->begin(NICP_K_TRANSFORM, s);
+  int blocks = (capacity + 255) / 256;
+  if (blocks > 0) k_cloud_transform<<<blocks, 256, 0, s>>>(pts, nrm, omg, eig, count, capacity, d_m12);
+  prof->end(NICP_K_TRANSFORM, s);
+}
+
+size_t moment_bytes(int precision) {
+  if (precision == NICP_MOMENTS_F32) return 4;
+  return 8;  // double or two-float
+}
+
+}  // namespace nicp

@@ -1,0 +1,94 @@
+// kernels.hpp -- host-side launchers of the NICP kernels and the event profiler.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "nicp_gpu.h"
+
+namespace nicp {
+
+// Brackets kernel launches with CUDA events on the launching stream.  Events
+// recorded during stream capture become graph nodes and are re-recorded on
+// every replay of that graph.
+struct Profiler {
+  struct Rec {
+    int kernel;
+    int nkernels;
+    cudaEvent_t a, b;
+  };
+  bool enabled = false;
+  bool capturing = false;            // events taken now belong to a graph
+  std::vector<cudaEvent_t> pool;     // reusable events of direct launches
+  std::vector<cudaEvent_t> owned;    // events baked into captured graphs
+  size_t next = 0;
+  std::vector<Rec> recs;
+  cudaEvent_t open[NICP_K_COUNT] = {};
+  int open_kernels[NICP_K_COUNT] = {};
+  unsigned long long launches = 0;  // kernels launched through the launchers
+
+  cudaEvent_t take() {
+    if (capturing) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      owned.push_back(e);
+      return e;
+    }
+    if (next == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[next++];
+  }
+  void begin(int k, cudaStream_t s) {
+    if (!enabled) return;
+    open[k] = take();
+    cudaEventRecord(open[k], s);
+  }
+  void end(int k, cudaStream_t s, int nk = 1) {
+    launches += nk;
+    if (!enabled) return;
+    cudaEvent_t b = take();
+    cudaEventRecord(b, s);
+    recs.push_back(Rec{k, nk, open[k], b});
+  }
+  ~Profiler() {
+    for (auto e : pool) cudaEventDestroy(e);
+    for (auto e : owned) cudaEventDestroy(e);
+  }
+};
+
+void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof);
+void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_rows, int total_col_ctas,
+                    cudaStream_t s, Profiler *prof);
+void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s,
+                  Profiler *prof);
+void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, const int *count, int capacity,
+                            const float *d_m12, cudaStream_t s, Profiler *prof);
+size_t moment_bytes(int precision);
+void launch_intervals(const float *d_depth, int P, const float *d_K9, float min_d, float max_d, float R, int32_t *d_out,
+                      cudaStream_t s, Profiler *prof);
+
+// Host-side Aligner::_computeStatistics (FP64): translational / rotational
+// eigen-ratios of the solution information matrix.
+void solution_statistics(const double H36[36], const double T16[16], double *translational_ratio,
+                         double *rotational_ratio);
+
+void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int mode, const float *explicit_KRt,
+                    cudaStream_t s, Profiler *prof);
+void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out, cudaStream_t s,
+                    Profiler *prof);
+void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
+                     int flags, cudaStream_t s, Profiler *prof);
+void launch_corr_list(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, int use_state_T,
+                      const float *explicit_T, cudaStream_t s, Profiler *prof);
+void launch_lin_list(const PairDev *d_pairs, int npairs, int total_tiles, const LinParams &lp, int parity_threads,
+                     int use_state_T, const float *explicit_T, cudaStream_t s, Profiler *prof);
+void launch_init_pairs(const PairDev *d_pairs, int npairs, const double *d_guesses, const double *d_ref_offsets,
+                       cudaStream_t s, Profiler *prof);
+void launch_solve(const PairDev *d_pairs, int npairs, float lambda, int mode, double early_eps, int ignore_done,
+                  cudaStream_t s, Profiler *prof);
+
+}  // namespace nicp

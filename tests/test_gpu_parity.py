@@ -1,0 +1,342 @@
+"""Parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+Bars (stated per test): bit-exact for index images, points and
+correspondence lists given identical inputs; normals and curvature within
+1e-5 of the FP64 oracle; H and b within 1e-5 relative of the FP64 oracle on
+identical clouds and correspondences; final pose within 1e-5 rad and 0.05 mm
+of the FP64 oracle pipeline.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from nicp_b200 import _lib as L
+from nicp_b200 import api, synth
+from oracle import oracle as O
+
+from helpers import (angle_between, cams, converter, float_T, gpu_cloud, oracle_cloud_from_gpu, perturb,
+                     projector)
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(3, "320x240"), (11, "640x480")]
+
+
+@pytest.fixture(scope="module", params=CASES, ids=[c[1] for c in CASES])
+def pair(request, ctx):
+    seed, name = request.param
+    d1, d2, Tgt, cam = synth.render_pair(seed, name)
+    return dict(d1=d1, d2=d2, Tgt=Tgt, cam=cam, seed=seed)
+
+
+def test_unproject_bitexact(ctx, pair):
+    """Index image and points equal the REF32 oracle bit for bit
+    (pinholepointprojector.cpp:93-134 with imageutils.cpp:85-99)."""
+    proj, conv = converter(pair["cam"], ctx)
+    cloud, idx = gpu_cloud(ctx, conv, pair["d1"])
+    pc, oc = cams(pair["cam"])
+    ocl, oidx = O.build_cloud(O.REF32, pair["d1"], oc)
+    assert np.array_equal(idx, oidx)
+    g = cloud.download()
+    assert len(g["points"]) == len(ocl)
+    assert np.array_equal(g["points"], ocl.get("points").astype(np.float32))
+
+
+def test_unproject_api_bitexact(ctx, pair):
+    """PinholePointProjector::unProject on a float depth image."""
+    proj = projector(pair["cam"], ctx)
+    d = np.zeros(pair["d1"].shape, np.float32)
+    O.load().orc_convert_u16(pair["d1"].ctypes.data_as(O.C.POINTER(O.C.c_uint16)), d.shape[0], d.shape[1],
+                             np.float32(0.001), d.ctypes.data_as(O.C.POINTER(O.C.c_float)))
+    pts, idx = proj.unProject(d)
+    pc, oc = cams(pair["cam"])
+    ocl, oidx = O.build_cloud(O.REF32, pair["d1"], oc)
+    assert np.array_equal(idx, oidx)
+    assert np.array_equal(pts, ocl.get("points").astype(np.float32))
+
+
+def test_intervals_bitexact(ctx, pair):
+    """projectIntervals radius image (pinholepointprojector.h:293-302)."""
+    proj = projector(pair["cam"], ctx)
+    d = (pair["d1"].astype(np.float32) * np.float32(0.001)).astype(np.float32)
+    d[pair["d1"] == 0] = 0
+    iv = proj.projectIntervals(d, 0.1)
+    K = proj.cameraMatrix()
+    inv = (np.float32(1.0) / d.astype(np.float32))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        a = (np.float32(K[0, 0]) * np.float32(0.1)) * inv
+        b = (np.float32(K[1, 1]) * np.float32(0.1)) * inv
+        m = np.where(a < b, b, a)
+        exp = np.where((d < 0.01) | (d > 6.0), -1, np.trunc(np.nan_to_num(m, posinf=0)).astype(np.int64))
+    assert np.array_equal(iv[..., 0], exp.astype(np.int32))
+
+
+def test_normals_curvature_vs_f64(ctx, pair):
+    """Normals and curvature within 1e-5 of the FP64 oracle.  Pixels whose
+    validity decision (min radius, min points, curvature threshold) sits on
+    a floating-point boundary may differ; they must stay below 0.2%.
+    Near-degenerate eigenvalues (lambda1 - lambda0 < 1e-3 lambda2) are
+    excluded from the angle check: there the smallest eigenvector is not
+    well defined in any precision."""
+    proj, conv = converter(pair["cam"], ctx, keep_stats=True)
+    cloud, idx = gpu_cloud(ctx, conv, pair["d1"])
+    g = cloud.download(stats=True)
+    pc, oc = cams(pair["cam"])
+    f, _ = O.build_cloud(O.F64, pair["d1"], oc)
+    r, _ = O.build_cloud(O.REF32, pair["d1"], oc)
+    fn, gn = f.get("normals")[:, :3], g["normals"][:, :3].astype(np.float64)
+    fhas = np.abs(fn).sum(1) > 0
+    ghas = np.abs(gn).sum(1) > 0
+    mismatch = np.mean(fhas != ghas)
+    assert mismatch < 2e-3, mismatch
+    both = fhas & ghas
+    lam = f.get("eigenvalues")
+    ok = both & ((lam[:, 1] - lam[:, 0]) > 1e-3 * lam[:, 2])
+    assert ok.sum() > 1000
+    ang = angle_between(fn[ok], gn[ok])
+    assert np.max(ang) < 1e-5, np.max(ang)
+    dk = np.abs(f.get("curvature") - g["curvature"].astype(np.float64))
+    assert np.max(dk[both]) < 1e-5, np.max(dk[both])
+    # information matrices (relative to their scale, 1000)
+    dop = np.abs(f.get("omega_p").reshape(-1, 3, 3) - g["omega_p"])[both]
+    assert np.max(dop) / 1000.0 < 1e-5
+    # REF32 (the reference's own float arithmetic) is reported, not gated
+    rn = r.get("normals")[:, :3]
+    rboth = both & (np.abs(rn).sum(1) > 0)
+    print("max normal angle GPU-F64 %.3g rad, REF32-F64 %.3g rad" %
+          (np.max(ang), np.max(angle_between(fn[rboth], rn[rboth]))))
+
+
+def test_project_bitexact(ctx, pair):
+    """z-buffer projection of identical clouds from a perturbed pose:
+    indices and depths equal the serial REF32 z-buffer (smallest depth,
+    lowest index on ties)."""
+    proj, conv = converter(pair["cam"], ctx)
+    cloud, idx = gpu_cloud(ctx, conv, pair["d1"])
+    g = cloud.download()
+    ocl = oracle_cloud_from_gpu(O.REF32, g)
+    pc, oc = cams(pair["cam"])
+    for k in range(3):
+        T = np.eye(4) if k == 0 else perturb(pair["seed"] * 10 + k, 1.5, 0.03)
+        proj.setTransform(T)
+        gi, gd = proj.project(cloud)
+        oi, od = O.project(O.REF32, ocl, oc, float_T(T))
+        assert np.array_equal(gi, oi), (k, np.sum(gi != oi))
+        assert np.array_equal(gd, od.astype(np.float32))
+
+
+def test_project_ties(ctx):
+    """Points with equal depth on one pixel: the lowest index wins."""
+    cam = dict(rows=8, cols=8, fx=4.0, fy=4.0, cx=3.5, cy=3.5)
+    pts = np.array([[0, 0, 2, 1], [0, 0, 2, 1], [0.001, 0, 2, 1], [0, 0, 1.5, 1], [0, 0, 1.5, 1]], np.float32)
+    c = api.Cloud(ctx)
+    c.upload(pts, np.zeros((5, 4), np.float32), np.zeros(5, np.float32))
+    proj = projector(cam, ctx)
+    gi, gd = proj.project(c)
+    pc, oc = cams(cam)
+    ocl = O.Cloud.from_arrays(O.REF32, pts.astype(float), np.zeros((5, 4)), np.zeros(5))
+    oi, od = O.project(O.REF32, ocl, oc, np.eye(4))
+    assert np.array_equal(gi, oi)
+    assert gi[4, 4] == 3
+
+
+def _pipeline_inputs(ctx, pair, T_off=None):
+    proj, conv = converter(pair["cam"], ctx)
+    ref, ri = gpu_cloud(ctx, conv, pair["d1"])
+    cur, ci = gpu_cloud(ctx, conv, pair["d2"])
+    T = pair["Tgt"] if T_off is None else T_off
+    proj.setTransform(np.eye(4))
+    cur_idx, _ = proj.project(cur)
+    proj.setTransform(T)
+    ref_idx, _ = proj.project(ref)
+    return proj, ref, cur, ref_idx, cur_idx, T
+
+
+@pytest.mark.parametrize("threads", [1, 4, 7])
+def test_correspond_bitexact(ctx, pair, threads):
+    """Correspondence list equals the REF32 oracle's on identical clouds,
+    index images and T, including the reference's OpenMP partition drops."""
+    proj, ref, cur, ri, ci, T = _pipeline_inputs(ctx, pair)
+    cf = api.CorrespondenceFinderProjective(ctx)
+    cf.parityThreads = threads
+    cf.setReferenceIndexImage(ri)
+    cf.setCurrentIndexImage(ci)
+    Tinv = np.linalg.inv(float_T(T)).astype(np.float32)
+    gp = cf.compute(ref, cur, Tinv)
+    oref = oracle_cloud_from_gpu(O.REF32, ref.download())
+    ocur = oracle_cloud_from_gpu(O.REF32, cur.download())
+    op = O.correspond(O.REF32, oref, ocur, ri, ci, Tinv.astype(np.float64), O.align_params(threads=threads))
+    assert len(gp) > 1000
+    assert np.array_equal(gp, op)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("threads", [1, 3])
+def test_linearize_vs_f64(ctx, pair, threads):
+    """H and b within 1e-5 relative of the FP64 oracle on identical inputs;
+    with threads > 1 the last K % T correspondences are dropped as the
+    reference drops them."""
+    proj, ref, cur, ri, ci, T = _pipeline_inputs(ctx, pair, perturb(pair["seed"], 1.0, 0.02))
+    cf = api.CorrespondenceFinderProjective(ctx)
+    cf.setReferenceIndexImage(ri)
+    cf.setCurrentIndexImage(ci)
+    Tinv = np.linalg.inv(float_T(T)).astype(np.float32)
+    pairs = cf.compute(ref, cur, Tinv)
+    lin = api.Linearizer(ctx)
+    lin.setT(Tinv)
+    lin.update(ref, cur, pairs, parity_threads=threads)
+    oref = oracle_cloud_from_gpu(O.F64, ref.download())
+    ocur = oracle_cloud_from_gpu(O.F64, cur.download())
+    Kk = (len(pairs) // threads) * threads
+    H, b, err, inl = O.linearize(O.F64, oref, ocur, pairs[:Kk], Tinv.astype(np.float64))
+    assert lin.inliers() == inl
+    assert _rel(lin.H(), H) < 1e-5, _rel(lin.H(), H)
+    assert _rel(lin.b(), b) < 1e-5, _rel(lin.b(), b)
+    assert abs(lin.error() - err) / max(err, 1e-300) < 1e-5
+
+
+def _align_gpu(ctx, pair, outer=10, inner=1, stats=True):
+    proj, conv = converter(pair["cam"], ctx)
+    ref, _ = gpu_cloud(ctx, conv, pair["d1"], keep_index=False)
+    cur, _ = gpu_cloud(ctx, conv, pair["d2"], keep_index=False)
+    cf = api.CorrespondenceFinderProjective(ctx)
+    lin = api.Linearizer(ctx)
+    al = api.AlignerProjective(proj, lin, cf, ctx)
+    al.setOuterIterations(outer)
+    al.setInnerIterations(inner)
+    al.computeStatistics = stats
+    al.setReferenceCloud(ref)
+    al.setCurrentCloud(cur)
+    al.align()
+    return al, ref, cur
+
+
+def test_align_vs_f64_pipeline(ctx, pair):
+    """Final pose of the whole GPU pipeline within 1e-5 rad / 0.05 mm of the
+    FP64 oracle pipeline (config: reference defaults, 10 outer x 1 inner)."""
+    al, ref, cur = _align_gpu(ctx, pair)
+    pc, oc = cams(pair["cam"])
+    fref, _ = O.build_cloud(O.F64, pair["d1"], oc)
+    fcur, _ = O.build_cloud(O.F64, pair["d2"], oc)
+    r = O.align(O.F64, fref, fcur, oc, statistics=True)
+    er, et = synth.pose_error(al.T(), r["T"])
+    print("GPU vs F64: %.3g rad %.3g m; F64 vs truth %s" % (er, et, synth.pose_error(r["T"], pair["Tgt"])))
+    assert er < 1e-5 and et < 5e-5, (er, et)
+    assert al.solutionValid() == bool(r["solution_valid"])
+
+
+def test_align_same_inputs_vs_f64(ctx, pair):
+    """Aligning the GPU's own clouds: the device loop (FP64 solve) tracks the
+    FP64 oracle loop run on the same float clouds."""
+    al, ref, cur = _align_gpu(ctx, pair)
+    pc, oc = cams(pair["cam"])
+    oref = oracle_cloud_from_gpu(O.F64, ref.download())
+    ocur = oracle_cloud_from_gpu(O.F64, cur.download())
+    r = O.align(O.F64, oref, ocur, oc)
+    er, et = synth.pose_error(al.T(), r["T"])
+    assert er < 1e-5 and et < 5e-5, (er, et)
+
+
+def test_inner_iterations_and_parity_threads(ctx, pair):
+    """2 inner iterations (ref index kept) and the list path with T = 4
+    both finish with a pose near the FP64 oracle run with the same options."""
+    pc, oc = cams(pair["cam"])
+    al, ref, cur = _align_gpu(ctx, pair, outer=6, inner=2, stats=False)
+    oref = oracle_cloud_from_gpu(O.F64, ref.download())
+    ocur = oracle_cloud_from_gpu(O.F64, cur.download())
+    r = O.align(O.F64, oref, ocur, oc, prm=O.align_params(outer_iterations=6, inner_iterations=2))
+    er, et = synth.pose_error(al.T(), r["T"])
+    assert er < 1e-5 and et < 5e-5, (er, et)
+
+
+def test_batch_equals_alone(ctx):
+    """Each pair's result is bitwise the same aligned alone and inside a
+    mixed-resolution batch (fixed tile -> partial order, no cross-pair
+    floating-point atomics)."""
+    specs = [(21, "320x240"), (22, "160x120"), (23, "640x480"), (24, "320x240")]
+    clouds, cam_list = [], []
+    for seed, name in specs:
+        d1, d2, Tgt, cam = synth.render_pair(seed, name, deg=2.0, meters=0.03)
+        proj, conv = converter(cam, ctx)
+        r, _ = gpu_cloud(ctx, conv, d1, keep_index=False)
+        c, _ = gpu_cloud(ctx, conv, d2, keep_index=False)
+        clouds.append((r, c))
+        cam_list.append(proj.camera())
+    corr = api.CorrespondenceFinderProjective(ctx).params()
+    lin = api.Linearizer(ctx).params()
+    prm = L.AlignParams()
+    ctx.lib.nicp_default_align_params(prm)
+    prm.compute_statistics = 0
+    prm.outer_iterations = 8
+    together = api.align_batch(ctx, [a for a, _ in clouds], [b for _, b in clouds], cam_list, None, corr, lin, prm)
+    for i in range(len(specs)):
+        alone = api.align_batch(ctx, [clouds[i][0]], [clouds[i][1]], [cam_list[i]], None, corr, lin, prm)
+        assert np.array_equal(np.array(alone[0].T), np.array(together[i].T)), i
+        assert alone[0].inliers == together[i].inliers
+    # the plain one-pair call runs the same kernels without the graph
+    proj = projector(synth.camera_dict(specs[0][1]), ctx)
+    aln = api.AlignerProjective(proj, api.Linearizer(ctx), api.CorrespondenceFinderProjective(ctx), ctx)
+    aln.computeStatistics = False
+    aln.setOuterIterations(8)
+    aln.setReferenceCloud(clouds[0][0])
+    aln.setCurrentCloud(clouds[0][1])
+    aln.align()
+    assert np.array_equal(aln.T(), np.array(together[0].T))
+
+
+def test_build_batch_equals_single(ctx):
+    """Clouds built in one batched pass equal clouds built one by one."""
+    frames, cam_list, singles = [], [], []
+    for seed, name in [(31, "320x240"), (32, "640x480"), (33, "160x120")]:
+        d1, _, _, cam = synth.render_pair(seed, name)
+        proj, conv = converter(cam, ctx)
+        frames.append(d1)
+        cam_list.append(proj.camera(cam["rows"], cam["cols"]))
+        singles.append(gpu_cloud(ctx, conv, d1, keep_index=False)[0].download())
+        prm = conv.params()
+    outs = [api.Cloud(ctx) for _ in frames]
+    api.build_batch(ctx, frames, cam_list, prm, outs)
+    for s, o in zip(singles, outs):
+        d = o.download()
+        for k in ("points", "normals", "curvature", "omega_p", "omega_n"):
+            assert np.array_equal(s[k], d[k]), k
+
+
+def test_sensor_offset(ctx, pair):
+    """A non-identity sensor offset transforms the built cloud
+    (Cloud::transformInPlace, cloud.cpp:191-204) like the REF32 oracle."""
+    S = perturb(5, 3.0, 0.1).astype(np.float32)
+    proj, conv = converter(pair["cam"], ctx)
+    c = api.Cloud(ctx)
+    conv.compute(c, pair["d1"], sensorOffset=S)
+    g = c.download()
+    plain, _ = gpu_cloud(ctx, conv, pair["d1"], keep_index=False)
+    p = plain.download()
+    exp = (S.astype(np.float64) @ p["points"].astype(np.float64).T).T
+    assert np.max(np.abs(g["points"] - exp)) < 1e-5
+    Rn = (S[:3, :3].astype(np.float64) @ p["normals"][:, :3].T.astype(np.float64)).T
+    assert np.max(np.abs(g["normals"][:, :3] - Rn)) < 1e-5
+
+
+def test_moments_precision_variants(ctx):
+    """FP32 / two-float / FP64 integral moments at 1280x720 far range: FP64
+    and two-float meet the 1e-5 normal gate; FP32 is reported only."""
+    d1, _, _, cam = synth.render_pair(41, "1280x720", kind=synth.FAR_ROOM)
+    pc, oc = cams(cam)
+    f, _ = O.build_cloud(O.F64, d1, oc)
+    fn = f.get("normals")[:, :3]
+    lam = f.get("eigenvalues")
+    res = {}
+    for prec in (L.NICP_MOMENTS_F64, L.NICP_MOMENTS_TWOFLOAT, L.NICP_MOMENTS_F32):
+        proj, conv = converter(cam, ctx, precision=prec)
+        c, _ = gpu_cloud(ctx, conv, d1, keep_index=False)
+        gn = c.download()["normals"][:, :3].astype(np.float64)
+        both = (np.abs(fn).sum(1) > 0) & (np.abs(gn).sum(1) > 0) & ((lam[:, 1] - lam[:, 0]) > 1e-3 * lam[:, 2])
+        res[prec] = float(np.max(angle_between(fn[both], gn[both]))) if both.any() else 0.0
+    print("max normal angle vs F64 oracle:", res)
+    assert res[L.NICP_MOMENTS_F64] < 1e-5
+    assert res[L.NICP_MOMENTS_TWOFLOAT] < 1e-5
