@@ -1,0 +1,430 @@
+"""NICP registration benchmark on B200 (one JSON line on stdout).
+
+Workload (default): 640x480 frame-to-frame odometry over a seeded 200-frame
+synthetic trajectory (fx = fy = 525, cx = 319.5, cy = 239.5; noise 0.0015 z^2,
+2% dropped pixels).  One step = build all 200 clouds
+(DepthImageConverterIntegralImage::compute) and align the 199 consecutive
+pairs (AlignerProjective::align, reference defaults, 10 outer x 1 inner) in
+one batched, graph-captured device loop.  Metric: 640x480 pairs/s.
+
+  value        inputs already resident in HBM, CUDA events on the library stream
+  e2e          through the public C ABI with pinned host frames: host->device
+               copies of every frame and device->host of every pose inside the
+               timed region
+  plain_*      the one-pair-per-call path (nicp_cloud_from_depth_u16 +
+               nicp_align per pair), for the batched/plain ratio
+  roofline     the kernel with the largest share of device time, algorithmic
+               bytes per launch / average launch time (CUDA events)
+  cpu_baseline the reference algorithm restated in C++ (oracle REF32, all host
+               threads) on a bounded sample of the same workload
+
+--impl reference runs only the CPU reference arm.  Multi-GPU (torchrun):
+replicas only -- every rank runs the same workload on its own GPU; value is
+the total over ranks divided by the slowest rank's time.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "640x480 NICP pairs/s (frame-to-frame, batched)"
+HBM_FALLBACK = 6650.0
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.reader = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.reader.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ workload
+def make_workload(seed, frames, cam_name="640x480"):
+    from nicp_b200 import synth
+    imgs, poses, cam = synth.render_sequence(seed, cam_name, n_frames=frames)
+    return np.stack(imgs), poses, cam
+
+
+def gpu_objects(ctx, cam):
+    from nicp_b200 import _lib as L
+    from nicp_b200 import api
+    proj = api.PinholePointProjector(ctx)
+    proj.setCameraMatrix([[cam["fx"], 0, cam["cx"]], [0, cam["fy"], cam["cy"]], [0, 0, 1]])
+    proj.setImageSize(cam["rows"], cam["cols"])
+    conv = api.DepthImageConverterIntegralImage(proj, api.StatsCalculatorIntegralImage(),
+                                                api.PointInformationMatrixCalculator(),
+                                                api.NormalInformationMatrixCalculator())
+    corr = api.CorrespondenceFinderProjective(ctx).params()
+    lin = api.Linearizer(ctx).params()
+    prm = L.AlignParams()
+    ctx.lib.nicp_default_align_params(prm)
+    prm.compute_statistics = 0  # the optional post-pass; not part of pairs/s
+    return proj, conv, corr, lin, prm
+
+
+def run_step(ctx, frames_ptrs, cam_c, prm_c, clouds, corr, lin, prm, on_device):
+    from nicp_b200 import api
+    n = len(clouds)
+    api.build_batch(ctx, frames_ptrs, [cam_c] * n, prm_c, clouds, on_device=on_device)
+    return api.align_batch(ctx, clouds[:-1], clouds[1:], [cam_c] * (n - 1), None, corr, lin, prm)
+
+
+# Algorithmic bytes per unit (the per-stage figures of the scope table):
+#   S1 unproject     2P + 4P + 12V          S2 moments   2P + 10 s P (+ the column pass reads and writes it)
+#   S3 stats + Omega 10 s P + 6P + 76V      S4 z-buffer  12V + 8V (+ 8P init, 8P resolve read, 4P write)
+#   S5 corr + lin    8P + 104 C             (s = 8 bytes per FP64 moment)
+def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
+    s = 8
+    if kernel == "unproject":
+        return (2 * P + 4 * P + 12 * V) * pairs
+    if kernel == "moments_rows":
+        return (2 * P + 10 * s * P) * pairs
+    if kernel == "moments_cols":
+        return (2 * 10 * s * P) * pairs
+    if kernel == "stats_omega":
+        return (10 * s * P + 6 * P + 76 * V) * pairs
+    if kernel == "zbuffer":
+        return (12 * V + 8 * V) * pairs
+    if kernel == "corr_lin":
+        return (8 * P + 104 * C) * pairs
+    if kernel == "resolve":
+        return (8 * P + 4 * P) * pairs
+    return 0
+
+
+def profile_step(ctx, run):
+    """Per-kernel device time of one step (CUDA events on the library stream)."""
+    from nicp_b200 import _lib as L
+    ctx.set_profiling(True)
+    ctx.synchronize()
+    res = run()
+    prof = {}
+    for k in L.KERNELS:
+        ms, n = ctx.read_profile(k)
+        if n:
+            prof[k] = (ms, n)
+    ctx.set_profiling(False)
+    return prof, res
+
+
+def cpu_baseline(frames, cam, seconds=15.0, threads=None):
+    """Oracle REF32 (the reference algorithm, float, reference order) on the
+    host cores: build + align per frame pair until `seconds` elapse."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    oc = O.camera(cam["rows"], cam["cols"], cam["fx"], cam["fy"], cam["cx"], cam["cy"])
+    prm = O.align_params(threads=threads)
+    t0 = time.perf_counter()
+    prev, _ = O.build_cloud(O.REF32, frames[0], oc)
+    pairs = 0
+    k = 1
+    while k < len(frames):
+        cur, _ = O.build_cloud(O.REF32, frames[k], oc)
+        O.align(O.REF32, prev, cur, oc, prm=prm)
+        prev = cur
+        pairs += 1
+        k += 1
+        if time.perf_counter() - t0 > seconds and pairs >= 2:
+            break
+    dt = time.perf_counter() - t0
+    # the first frame's build is included in dt: amortised over the sample
+    return pairs / dt, pairs, dt, threads
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    frames, poses, cam = make_workload(args.seed, min(args.frames, 40))
+    for _ in range(max(0, args.warmup)):
+        cpu_baseline(frames[:3], cam, seconds=0.0)
+    vals, total_pairs, total_t = [], 0, 0.0
+    per_step = min(args.cpu_seconds, 150.0 / max(1, args.steps))  # whole run stays within a few minutes
+    for _ in range(args.steps):
+        v, n, dt, threads = cpu_baseline(frames, cam, seconds=per_step)
+        vals.append(v)
+        total_pairs += n
+        total_t += dt
+    value = total_pairs / total_t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args),
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                             "sample": "%d frame pairs of the 640x480 sequence per step (build + align)" %
+                                       (total_pairs // max(1, args.steps))},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args):
+    return {"workload": "640x480 frame-to-frame sequence, %d frames (%d pairs), reference defaults, "
+                        "%d outer x 1 inner" % (args.frames, args.frames - 1, 10),
+            "resolution": "640x480", "frames": args.frames, "pairs_per_step": args.frames - 1,
+            "camera": "fx=fy=525 cx=319.5 cy=239.5", "moments": "fp64", "cross_block": "fp64",
+            "solve": "fp64 ldlt on device", "statistics": "not computed (optional post-pass)",
+            "l2": "inputs larger than L2 (clouds ~4.9 GB per step)", "parallelism": "replicas"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--frames", type=int, default=200)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-call leg")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+
+    if args.impl == "reference":
+        rc = reference_arm(args, rank, world)
+        if dist:
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+    from nicp_b200 import api
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream(device=local)
+    ctx = api.Context(local, stream.cuda_stream)
+    frames, poses, cam = make_workload(args.seed + 7919 * rank, args.frames)
+    F = len(frames)
+    npairs = F - 1
+    proj, conv, corr, lin, prm = gpu_objects(ctx, cam)
+    cam_c = proj.camera(cam["rows"], cam["cols"])
+    prm_c = conv.params()
+    clouds = [api.Cloud(ctx) for _ in range(F)]
+
+    # device-resident inputs
+    dev = torch.from_numpy(frames.astype(np.int16, copy=False).view(np.int16)).to(f"cuda:{local}")
+    P = cam["rows"] * cam["cols"]
+    dptrs = [(dev.data_ptr() + 2 * P * i, cam["rows"], cam["cols"]) for i in range(F)]
+    host = torch.from_numpy(frames.view(np.int16)).pin_memory()
+    hframes = [host[i].numpy().view(np.uint16) for i in range(F)]
+
+    def step_dev():
+        return run_step(ctx, dptrs, cam_c, prm_c, clouds, corr, lin, prm, True)
+
+    def step_host():
+        return run_step(ctx, hframes, cam_c, prm_c, clouds, corr, lin, prm, False)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step_dev()
+    torch.cuda.synchronize()
+
+    # ---- value: device-resident inputs
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ctx.kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            res = step_dev()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = ctx.kernel_launches() - l0
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ms = max_over_ranks(ms)
+    value = world * npairs * args.steps / (ms / 1e3)
+
+    # ---- e2e: pinned host frames through the C ABI, results back to the host
+    for _ in range(2):
+        step_host()
+    h0, d0 = ctx.transfer_bytes()
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e2.record(stream)
+        for _ in range(args.steps):
+            step_host()
+        e3.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    h1, d1 = ctx.transfer_bytes()
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3))
+    e2e = world * npairs * args.steps / (ms_e2e / 1e3)
+
+    # ---- accuracy against the synthetic ground truth (median over pairs)
+    from nicp_b200 import synth
+    errs = [synth.pose_error(np.array(r.T).reshape(4, 4), synth.rel(poses[i], poses[i + 1]))
+            for i, r in enumerate(res)]
+    rot_med = float(np.median([e[0] for e in errs]))
+    tr_med = float(np.median([e[1] for e in errs]))
+
+    # ---- per-kernel shares and the roofline of the top kernel
+    prof, res_p = profile_step(ctx, step_dev)
+    total = sum(v[0] for v in prof.values()) or 1.0
+    top = max(prof, key=lambda k: prof[k][0])
+    Vs = [c.size() for c in clouds[:4]]
+    V = float(np.mean(Vs))
+    C = float(np.mean([r.num_correspondences for r in res_p]))  # accepted; candidates are >= this
+    peak, peak_kind = measured_peak_gbs()
+    top_ms, top_n = prof[top]
+    launches_per_step = top_n
+    per_launch_bytes = {
+        "corr_lin": (8 * P + 104 * C) * npairs,
+        "zbuffer": (12 * V + 8 * V) * npairs,
+        "stats_omega": (10 * 8 * P + 6 * P + 76 * V) * F,
+        "moments_rows": (2 * P + 80 * P) * F,
+        "moments_cols": (160 * P) * F,
+        "unproject": (2 * P + 4 * P + 12 * V) * F / 2,  # two kernels per stage launch
+        "resolve": (12 * P) * npairs,
+    }.get(top, 0.0)
+    achieved = per_launch_bytes / (top_ms / top_n / 1e3) / 1e9
+    roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+            "bytes_per_launch": per_launch_bytes, "avg_launch_ms": top_ms / top_n,
+            "shares": {k: round(v[0] / total, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}}
+
+    # ---- plain one-pair-per-call path
+    plain = None
+    if not args.no_plain and rank == 0:
+        from nicp_b200 import _lib as L
+        import ctypes as Cc
+        pl = []
+        prm1 = L.AlignParams()
+        ctx.lib.nicp_default_align_params(prm1)
+        prm1.compute_statistics = 0
+        res1 = L.AlignResult()
+        nplain = min(npairs, 60)
+        for rep in range(2):
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            ctx.check(ctx.lib.nicp_cloud_from_depth_u16(ctx.h, Cc.c_void_p(dptrs[0][0]), cam["rows"], cam["cols"], 0,
+                                                        1, Cc.byref(cam_c), Cc.byref(prm_c), None, clouds[0].h, None))
+            for i in range(nplain):
+                ctx.check(ctx.lib.nicp_cloud_from_depth_u16(ctx.h, Cc.c_void_p(dptrs[i + 1][0]), cam["rows"],
+                                                            cam["cols"], 0, 1, Cc.byref(cam_c), Cc.byref(prm_c), None,
+                                                            clouds[i + 1].h, None))
+                ctx.check(ctx.lib.nicp_align(ctx.h, clouds[i].h, clouds[i + 1].h, Cc.byref(cam_c), None, None, None,
+                                             Cc.byref(corr), Cc.byref(lin), Cc.byref(prm1), Cc.byref(res1)))
+            ctx.synchronize()
+            pl.append(nplain / (time.perf_counter() - t0))
+        plain = max(pl)
+
+    cpu = None
+    if not args.no_cpu and rank == 0:
+        v, n, dt, threads = cpu_baseline(frames, cam, seconds=args.cpu_seconds)
+        cpu = {"value": v, "unit": "pairs/s", "cores": threads, "kind": "port",
+               "sample": "%d consecutive 640x480 frame pairs (build + align, oracle REF32, %d threads, %.1f s)"
+                         % (n, threads, dt)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(args),
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": (h1 - h0) // args.steps,
+                        "d2h_bytes_per_step": (d1 - d0) // args.steps},
+                "gpu_launches": int(launches), "clocks": clk,
+                "plain_pairs_per_s": plain, "batched_over_plain": (value / world / plain) if plain else None,
+                "pose_err_vs_truth_median": {"rad": rot_med, "m": tr_med},
+                "points_per_frame": V, "correspondences_per_pair": C}
+        print(json.dumps(line), flush=True)
+    del clouds
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

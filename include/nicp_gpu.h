@@ -171,6 +171,8 @@ enum {
 int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable);
 /* Kernels this context has launched so far (graph replays included). */
 unsigned long long nicp_ctx_kernel_launches(const nicp_ctx *ctx);
+/* Host->device and device->host bytes the context has copied so far. */
+int nicp_ctx_transfer_bytes(const nicp_ctx *ctx, unsigned long long *h2d, unsigned long long *d2h);
 int nicp_ctx_read_profile(nicp_ctx *ctx, int kernel, double *total_ms, int *launches);
 const char *nicp_kernel_name(int kernel);
 

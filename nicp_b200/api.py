@@ -59,6 +59,11 @@ class Context:
     def kernel_launches(self):
         return self.lib.nicp_ctx_kernel_launches(self.h)
 
+    def transfer_bytes(self):
+        h, d = C.c_ulonglong(0), C.c_ulonglong(0)
+        self.check(self.lib.nicp_ctx_transfer_bytes(self.h, C.byref(h), C.byref(d)))
+        return h.value, d.value
+
     def set_profiling(self, on):
         self.check(self.lib.nicp_ctx_set_profiling(self.h, 1 if on else 0))
 

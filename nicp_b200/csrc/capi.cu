@@ -58,6 +58,7 @@ struct nicp_ctx {
   size_t cloud_bytes = 0;
   std::vector<GraphEntry> graphs;
   nicp_cloud *scratch_cloud = nullptr;
+  unsigned long long h2d_bytes = 0, d2h_bytes = 0;  // host<->device traffic issued by the library
 };
 
 struct nicp_cloud {
@@ -349,6 +350,13 @@ extern "C" int nicp_ctx_read_profile(nicp_ctx *ctx, int kernel, double *total_ms
 
 extern "C" unsigned long long nicp_ctx_kernel_launches(const nicp_ctx *ctx) { return ctx ? ctx->prof.launches : 0; }
 
+extern "C" int nicp_ctx_transfer_bytes(const nicp_ctx *ctx, unsigned long long *h2d, unsigned long long *d2h) {
+  if (!ctx) return NICP_EINVAL;
+  if (h2d) *h2d = ctx->h2d_bytes;
+  if (d2h) *d2h = ctx->d2h_bytes;
+  return NICP_OK;
+}
+
 extern "C" const char *nicp_kernel_name(int k) {
   static const char *names[NICP_K_COUNT] = {"unproject", "moments_rows", "moments_cols", "stats_omega",
                                             "zbuffer",   "resolve",      "corr_lin",     "corr_list",
@@ -539,6 +547,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
         size_t pitch = f.pitch ? f.pitch : f.cols * esz;
         CK(ctx, cudaMemcpy2DAsync(dst, f.cols * esz, f.depth, pitch, f.cols * esz, f.rows,
                                   f.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        if (!f.on_device) ctx->h2d_bytes += (unsigned long long)f.cols * esz * f.rows;
         src = dst;
       }
       FrameDev &d = fd[k];
@@ -585,6 +594,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     }
     FrameDev *dfr = (FrameDev *)(ctx->ws + o_frames);
     CK(ctx, cudaMemcpyAsync(dfr, pin, sizeof(FrameDev) * nf, cudaMemcpyHostToDevice, s));
+    ctx->h2d_bytes += sizeof(FrameDev) * nf;
     CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
     launch_unproject(dfr, nf, tiles, s, &ctx->prof);
     if (!unproject_only) {
@@ -1028,7 +1038,11 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
   CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_guess, gs, 128 * (size_t)a.n, cudaMemcpyHostToDevice, s));
   CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_roff, ro, 128 * (size_t)a.n, cudaMemcpyHostToDevice, s));
   CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
-  if (a.graph) {
+  ctx->h2d_bytes += (sizeof(PairDev) + 48 + 256) * (unsigned long long)a.n;
+  // Events recorded while a stream is captured are capture-internal and
+  // cannot be timed after a replay, so a profiled call launches the same
+  // kernels directly.
+  if (a.graph && !ctx->prof.enabled) {
     std::string key = graph_key(ctx, pl, a);
     GraphEntry *ge = nullptr;
     for (auto &g : ctx->graphs)
@@ -1069,6 +1083,7 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
   char *res;
   if ((rc = pin_down(ctx, sizeof(PairState) * a.n, &res))) return rc;
   CK(ctx, cudaMemcpyAsync(res, ctx->ws + pl.o_states, sizeof(PairState) * a.n, cudaMemcpyDeviceToHost, s));
+  ctx->d2h_bytes += sizeof(PairState) * (unsigned long long)a.n;
   CK(ctx, cudaStreamSynchronize(s));
   const PairState *st = (const PairState *)res;
   for (int i = 0; i < a.n; i++) {

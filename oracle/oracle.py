@@ -204,7 +204,14 @@ def projector_matrices(mode, cam, T=None):
     return K.reshape(4, 4), iK.reshape(4, 4)
 
 
+def _same_mode(mode, *clouds):
+    for c in clouds:
+        if c.mode != mode:
+            raise ValueError("oracle cloud built in mode %d used in mode %d" % (c.mode, mode))
+
+
 def project(mode, cloud, cam, T=None):
+    _same_mode(mode, cloud)
     rows, cols = int(cam.rows * cam.scaling), int(cam.cols * cam.scaling)
     index = np.zeros((rows, cols), dtype=np.int32)
     depth = np.zeros((rows, cols), dtype=np.float64)
@@ -214,6 +221,7 @@ def project(mode, cloud, cam, T=None):
 
 def correspond(mode, ref, cur, ref_index, cur_index, T, prm=None):
     prm = prm or align_params()
+    _same_mode(mode, ref, cur)
     rows, cols = ref_index.shape
     pairs = np.zeros(2 * rows * cols, dtype=np.int32)
     ri = np.ascontiguousarray(ref_index, dtype=np.int32)
@@ -225,6 +233,7 @@ def correspond(mode, ref, cur, ref_index, cur_index, T, prm=None):
 
 def linearize(mode, ref, cur, pairs, T, prm=None):
     prm = prm or align_params()
+    _same_mode(mode, ref, cur)
     pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
     H, b, err = np.zeros(36), np.zeros(6), np.zeros(1)
     inl = C.c_int(0)
@@ -235,6 +244,7 @@ def linearize(mode, ref, cur, pairs, T, prm=None):
 
 def align(mode, ref, cur, cam, guess=None, ref_offset=None, cur_offset=None, prm=None, statistics=False):
     prm = prm or align_params()
+    _same_mode(mode, ref, cur)
     r = AlignResult()
     load().orc_align(mode, ref.h, cur.h, C.byref(cam), _d(guess), _d(ref_offset), _d(cur_offset), C.byref(prm),
                      1 if statistics else 0, C.byref(r))
@@ -274,6 +284,7 @@ def iso_inverse(mode, T):
 
 
 def integral_region(mode, cloud, index, xmin, xmax, ymin, ymax):
+    _same_mode(mode, cloud)
     index = np.ascontiguousarray(index, dtype=np.int32)
     rows, cols = index.shape
     out = np.zeros(10)

@@ -76,3 +76,52 @@ def angle_between(a, b):
 
 def deg(x):
     return math.degrees(x)
+
+
+def radius_image(depth_u16, cam, dtype, world_radius=0.1, depth_scale=0.001):
+    """Interval radius per pixel (pinholepointprojector.h:293-302) evaluated in
+    float32 (the reference and the CUDA path) or float64 (the FP64 oracle)."""
+    t = np.dtype(dtype).type
+    u = depth_u16.astype(np.int64)
+    d = t(np.float32(depth_scale)) * u.astype(dtype)
+    d = np.where(u == 0, t(0), d)
+    R = t(np.float32(world_radius))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = t(1) / d
+        a = (t(np.float32(cam["fx"])) * R) * inv
+        b = (t(np.float32(cam["fy"])) * R) * inv
+        m = np.where(a < b, b, a)
+        lo, hi = t(np.float32(cam.get("min_distance", 0.01))), t(np.float32(cam.get("max_distance", 6.0)))
+        r = np.where((d < lo) | (d > hi), -1, np.trunc(np.nan_to_num(m, posinf=0, neginf=0))).astype(np.int64)
+    return r
+
+
+def dilate(mask, r):
+    """Binary dilation by a (2r+1)^2 box (numpy only)."""
+    out = mask.copy()
+    if not mask.any():
+        return out
+    rows, cols = mask.shape
+    ys, xs = np.nonzero(mask)
+    for y, x in zip(ys, xs):
+        out[max(0, y - r):min(rows, y + r + 1), max(0, x - r):min(cols, x + r + 1)] = True
+    return out
+
+
+def decision_stable_pixels(depth_u16, cam, idx32, idx64, max_radius=30):
+    """Pixels whose normal computation takes the same discrete decisions in
+    float and in double: same interval radius, and no pixel of its window
+    (radius <= max_radius) changes validity between the two precisions."""
+    r32 = radius_image(depth_u16, cam, np.float32)
+    r64 = radius_image(depth_u16, cam, np.float64)
+    bad_valid = (idx32 >= 0) != (idx64 >= 0)
+    unstable = dilate(bad_valid, max_radius + 1) | (r32 != r64)
+    return ~unstable, float(np.mean(r32 != r64)), int(bad_valid.sum())
+
+
+def match_by_pixel(idx_a, idx_b, mask=None):
+    """Point index pairs (a, b) of pixels valid in both index images."""
+    m = (idx_a >= 0) & (idx_b >= 0)
+    if mask is not None:
+        m &= mask
+    return idx_a[m], idx_b[m]
