@@ -413,6 +413,7 @@ extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *c
   }
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   for (int i = 0; i < n; i++) {
+    if (p4) p4[4 * i + 3] = 1.0f;  // the device keeps a "has a normal" flag in w
     if (n4) { n4[4 * i] = nrm[i].x; n4[4 * i + 1] = nrm[i].y; n4[4 * i + 2] = nrm[i].z; n4[4 * i + 3] = 0.0f; }
     if (curv) curv[i] = nrm[i].w;
     const float *o = reinterpret_cast<const float *>(&omg[3 * (size_t)i]);
@@ -439,7 +440,8 @@ extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const fl
   if (rc) return rc;
   std::vector<float4> pts(n), nrm(n), omg(3 * (size_t)n);
   for (int i = 0; i < n; i++) {
-    pts[i] = make_float4(p4[4 * i], p4[4 * i + 1], p4[4 * i + 2], 1.0f);
+    bool has_normal = n4[4 * i] != 0.0f || n4[4 * i + 1] != 0.0f || n4[4 * i + 2] != 0.0f;
+    pts[i] = make_float4(p4[4 * i], p4[4 * i + 1], p4[4 * i + 2], has_normal ? 1.0f : kNoNormalW);
     nrm[i] = make_float4(n4[4 * i], n4[4 * i + 1], n4[4 * i + 2], curv[i]);
     float o[12] = {0};
     if (op9) { const float *s = op9 + 9 * (size_t)i; o[0] = s[0]; o[1] = s[1]; o[2] = s[2]; o[3] = s[4]; o[4] = s[5]; o[5] = s[8]; }
@@ -901,7 +903,7 @@ extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_c
   CK(ctx, cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s));
   const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
   launch_zbuffer(dpd, 1, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
-  launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ctx->ws + o_depth), s, &ctx->prof);
+  launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ctx->ws + o_depth), 0, s, &ctx->prof);
   CK(ctx, cudaGetLastError());
   if (index_out) CK(ctx, cudaMemcpyAsync(index_out, ctx->ws + pl.o_cur[0], 4 * P, cudaMemcpyDeviceToHost, s));
   if (depth_out) CK(ctx, cudaMemcpyAsync(depth_out, ctx->ws + o_depth, 4 * P, cudaMemcpyDeviceToHost, s));
@@ -940,11 +942,13 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
                     &ctx->prof);
   // current cloud, seen from its sensor offset, projected once (alignerprojective.cpp:36-39)
   launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
-  launch_resolve(dpd, pl.n, pl.total_tiles, 0, nullptr, s, &ctx->prof);
+  // outside list (parity) mode, current pixels whose point has no normal are
+  // dropped from the index image: the gates would reject them anyway
+  launch_resolve(dpd, pl.n, pl.total_tiles, 0, nullptr, (pl.list_mode || cp.demoted) ? 0 : 1, s, &ctx->prof);
   for (int i = 0; i < outer; i++) {
     launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 1, nullptr, s, &ctx->prof);
     if (pl.list_mode) {
-      launch_resolve(dpd, pl.n, pl.total_tiles, 1, nullptr, s, &ctx->prof);
+      launch_resolve(dpd, pl.n, pl.total_tiles, 1, nullptr, 0, s, &ctx->prof);
       launch_corr_list(dpd, pl.n, pl.total_tiles, cp, 1, nullptr, s, &ctx->prof);
       for (int k = 0; k < inner; k++) {
         launch_lin_list(dpd, pl.n, pl.total_tiles, lp, std::max(1, a.corr->parity_threads), 1, nullptr, s, &ctx->prof);

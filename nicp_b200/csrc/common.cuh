@@ -28,6 +28,14 @@ constexpr int kStatsThreads = 256;
 constexpr int kPartialWords = 32;       // doubles per CTA partial (21 H + 6 b + chi2 + inliers + C + K + pad)
 constexpr int kPointsPerCta = 256;      // z-buffer kernel: one point per thread
 
+// pts[i].w is 1 for a point with a non-zero normal and kNoNormalW otherwise
+// (the reference's Point has w = 1; downloads report 1).  The z-buffer key
+// carries this bit below the point index, (depth key << 32) | (i << 1) | bit,
+// which keeps the packed minimum ordered by (depth, index) exactly, and lets
+// the correspondence kernel reject a pixel whose point has no normal without
+// gathering it.
+constexpr float kNoNormalW = 0.5f;
+
 // ---- per-frame descriptor for the cloud-build kernels
 struct FrameDev {
   const uint16_t *depth_u16;  // packed rows*cols, or null when depth_f32 is used

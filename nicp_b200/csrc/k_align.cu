@@ -22,6 +22,8 @@
 //                72-100), early exit, and the float matrices of the next iteration.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.hpp"
 
@@ -58,14 +60,26 @@ __global__ void __launch_bounds__(kPointsPerCta)
   for (int k = 0; k < 12; k++) K[k] = src[k];
   int x, y;
   float d;
-  if (!project_pixel(K, pts[i], pd.rows, pd.cols, pd.min_d, pd.max_d, x, y, d)) return;
-  unsigned long long key = ((unsigned long long)float_key(d) << 32) | (unsigned)i;
+  float4 p = pts[i];
+  if (!project_pixel(K, p, pd.rows, pd.cols, pd.min_d, pd.max_d, x, y, d)) return;
+  unsigned long long key = ((unsigned long long)float_key(d) << 32) | ((unsigned)i << 1) | (p.w != 1.0f ? 1u : 0u);
   atomicMin(pd.zbuf + (size_t)y * pd.cols + x, key);
+}
+
+// Decodes a z-buffer word: the point index, or -1 when empty -- or, with
+// drop_no_normal, when the point has no normal (such a pixel can never pass
+// the correspondence gates unless they are demoted to GICP).
+__device__ __forceinline__ int zbuf_index(unsigned long long z, bool drop_no_normal) {
+  if (z == ~0ull) return -1;
+  unsigned lo = (unsigned)(z & 0xffffffffull);
+  if (drop_no_normal && (lo & 1u)) return -1;
+  return (int)(lo >> 1);
 }
 
 // z-buffer -> int index image (and optional depth image, FLT_MAX where empty);
 // the z-buffer is left all ones for its next use.
-__global__ void k_resolve(const PairDev *__restrict__ pairs, int npairs, int to_ref, float *depth_out) {
+__global__ void k_resolve(const PairDev *__restrict__ pairs, int npairs, int to_ref, float *depth_out,
+                          int drop_no_normal) {
   int pi = find_pair(pairs, npairs, blockIdx.x, false);
   const PairDev &pd = pairs[pi];
   int P = pd.rows * pd.cols;
@@ -77,7 +91,7 @@ __global__ void k_resolve(const PairDev *__restrict__ pairs, int npairs, int to_
     if (p >= P) break;
     unsigned long long z = pd.zbuf[p];
     pd.zbuf[p] = ~0ull;
-    dst[p] = (z == ~0ull) ? -1 : (int)(unsigned)(z & 0xffffffffull);
+    dst[p] = zbuf_index(z, drop_no_normal != 0);
     if (depth_out) depth_out[p] = (z == ~0ull) ? 3.402823466e+38f : key_float((uint32_t)(z >> 32));
   }
 }
@@ -114,10 +128,9 @@ __device__ __forceinline__ bool gate(const CorrParams &cp, const float *T12, flo
 
 // linearizer.cpp:59-100 for one correspondence, FP32.
 __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
-                                         float4 cn, const float4 *omg, Acc &acc) {
+                                         float4 cn, float4 o0, float4 o1, float4 o2, Acc &acc) {
   float3 rp = xform_point(T12, rp0);
   float3 rn = xform_normal(T12, rn0);
-  float4 o0 = omg[0], o1 = omg[1], o2 = omg[2];
   // symmetric 3x3 as (00 01 02 11 12 22)
   float Op[6] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y};
   float On[6] = {o1.z, o1.w, o2.x, o2.y, o2.z, o2.w};
@@ -217,53 +230,196 @@ __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) 
   }
 }
 
+// ---- fused correspondence + linearizer: persistent, cp.async-pipelined.
+// A pair image is cut into tiles of kCorrTilePixels; every tile yields one
+// FP64 partial, so results do not depend on the grid or the batch.  A CTA
+// walks its tiles (blockIdx.x, +gridDim.x, ...) in sub-tiles of 256 pixels
+// (one per thread).  For each pixel the thread reads the two indices, then
+// stages the 7 gathered float4 (reference point and normal, current point
+// and normal, 3 x Omega) into its own shared-memory slot with cp.async;
+// kCorrStages sub-tiles are in flight while the oldest one is gated and
+// linearized.  Each thread reads back only what it copied itself, so the
+// pipeline needs no barrier.
+constexpr int kSubPix = kCorrThreads;                    // pixels per sub-tile
+constexpr int kSubsPerTile = kCorrTilePixels / kSubPix;  // 4
+constexpr int kCorrStages = 3;
+
+// Structure-of-arrays stage: thread t owns element t of every array, so a
+// warp's accesses to one field are consecutive 16-byte words (no bank
+// conflicts).
+struct GatherStage {
+  float4 rp[kCorrThreads], rn[kCorrThreads], cp[kCorrThreads], cn[kCorrThreads];
+  float4 o0[kCorrThreads], o1[kCorrThreads], o2[kCorrThreads];
+  int ri[kCorrThreads], ci[kCorrThreads], valid[kCorrThreads];
+};
+constexpr int kCorrSmem = kCorrStages * (int)sizeof(GatherStage);
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // flags: bit0 read the reference index from the z-buffer (else ref_index),
 // bit1 reset the z-buffer after reading, bit2 keep the resolved reference
 // index image, bit3 statistics pass (gate with Tgate_used; ignores `done`).
-__global__ void __launch_bounds__(kCorrThreads)
-    k_corr_lin(const PairDev *__restrict__ pairs, int npairs, CorrParams cp, LinParams lp, int flags) {
-  int pi = find_pair(pairs, npairs, blockIdx.x, false);
-  const PairDev &pd = pairs[pi];
-  PairState *st = pd.state;
-  bool stats_pass = flags & 8;
-  if (st->done && !stats_pass) return;
-  int tile = blockIdx.x - pd.tile_base;
-  int cols = pd.cols, P = pd.rows * cols;
-  int rmax = pd.rows;
-  if (cp.row_limit_threads > 1) rmax = (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
-  float Tg[12], Tl[12];
-  const float *gsrc = stats_pass ? st->Tgate_used : st->Tgate;
-#pragma unroll
-  for (int k = 0; k < 12; k++) { Tg[k] = gsrc[k]; Tl[k] = st->Tlin[k]; }
-  const int nref = *pd.ref_count, ncur = *pd.cur_count;
+__global__ void __launch_bounds__(kCorrThreads, 2)
+    k_corr_lin(const PairDev *__restrict__ pairs, int npairs, int total_tiles, CorrParams cp, LinParams lp,
+               int flags) {
+  extern __shared__ __align__(16) unsigned char corr_smem[];
+  GatherStage *stages = reinterpret_cast<GatherStage *>(corr_smem);
+  const int t = threadIdx.x;
+  // per-tile constants for the two tiles the pipeline can span:
+  // [0..11] gating T, [12..23] linearizer T, then pair index and skip flag
+  __shared__ float sT[2][24];
+  __shared__ int sPair[2], sSkip[2];
+  const bool stats_pass = flags & 8;
+  if ((int)blockIdx.x >= total_tiles) return;
+  const int ntiles = (total_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int nsub = ntiles * kSubsPerTile;
+  const bool drop_no_normal = !cp.demoted;
+  auto tile_of = [&](int j) { return (int)blockIdx.x + (j / kSubsPerTile) * (int)gridDim.x; };
+  auto stage_of = [&](int j) -> GatherStage & { return stages[j % kCorrStages]; };
+
+  // Phase I (one iteration ahead, plain loads into registers): the two index
+  // words of sub-tile j.
+  unsigned long long zI = ~0ull;
+  int cI = -1;
+  auto load_indices = [&](int j) {
+    zI = ~0ull;
+    cI = -1;
+    if (j >= nsub) return;
+    int tile = tile_of(j);
+    const PairDev &pd = pairs[find_pair(pairs, npairs, tile, false)];
+    if (!stats_pass && pd.state->done) return;
+    int p = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + threadIdx.x;
+    if (p >= pd.rows * pd.cols) return;
+    if (flags & 1) zI = pd.zbuf[p];
+    else cI = pd.ref_index[p];  // stashed in cI until phase G1 reads the current index
+    if (flags & 1) cI = pd.cur_index[p];
+    else zI = (unsigned long long)(unsigned)pd.cur_index[p];
+  };
+
+  // Phase G1 (two sub-tiles ahead): decode the indices, reset the z-buffer,
+  // gather points and normals of both clouds.
+  auto issue_g1 = [&](int j) {
+    GatherStage &g = stage_of(j);
+    int ri = -1, ci = -1, valid = 0;
+    if (j < nsub) {
+      int tile = tile_of(j);
+      const PairDev &pd = pairs[find_pair(pairs, npairs, tile, false)];
+      if (stats_pass || !pd.state->done) {
+        int p = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + threadIdx.x;
+        if (p < pd.rows * pd.cols) {
+          if (flags & 1) {
+            ri = zbuf_index(zI, drop_no_normal);
+            ci = cI;
+            if (flags & 2) pd.zbuf[p] = ~0ull;
+            if (flags & 4) pd.ref_index[p] = ri;
+          } else {
+            ri = cI;
+            ci = (int)(unsigned)zI;
+          }
+          int rmax = pd.rows;
+          if (cp.row_limit_threads > 1) rmax = (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
+          valid = ri >= 0 && ci >= 0 && ri < *pd.ref_count && ci < *pd.cur_count && p / pd.cols < rmax;
+          if (valid) {
+            cp_async16(&g.rp[t], pd.ref_pts + ri);
+            cp_async16(&g.rn[t], pd.ref_nrm + ri);
+            cp_async16(&g.cp[t], pd.cur_pts + ci);
+            cp_async16(&g.cn[t], pd.cur_nrm + ci);
+          }
+        }
+      }
+    }
+    g.ri[t] = ri;
+    g.ci[t] = ci;
+    g.valid[t] = valid;
+    cp_async_commit();
+  };
+
+  // Per-tile constants, written when the tile's first sub-tile enters G1.
+  auto tile_constants = [&](int j) {
+    if (j >= nsub || j % kSubsPerTile) return;
+    int e = (j / kSubsPerTile) & 1;
+    int pi = find_pair(pairs, npairs, tile_of(j), false);
+    const PairState *st = pairs[pi].state;
+    if (threadIdx.x < 24)
+      sT[e][threadIdx.x] = threadIdx.x < 12 ? (stats_pass ? st->Tgate_used : st->Tgate)[threadIdx.x]
+                                            : st->Tlin[threadIdx.x - 12];
+    if (threadIdx.x == 0) {
+      sPair[e] = pi;
+      sSkip[e] = st->done && !stats_pass;
+    }
+  };
+
+  // Gate (one sub-tile ahead), then gather Omega only for accepted pairs.
+  auto gate_g2 = [&](int j) {
+    if (j < nsub) {
+      GatherStage &g = stage_of(j);
+      int e = (j / kSubsPerTile) & 1;
+      int acc_ok = 0;
+      if (g.valid[t] && !sSkip[e]) {
+        acc_ok = gate(cp, sT[e], g.rp[t], g.rn[t], g.cp[t], g.cn[t]) ? 2 : 1;
+        if (acc_ok == 2) {
+          const float4 *o = pairs[sPair[e]].cur_omg + 3 * (size_t)g.ci[t];
+          cp_async16(&g.o0[t], o);
+          cp_async16(&g.o1[t], o + 1);
+          cp_async16(&g.o2[t], o + 2);
+        }
+      }
+      g.valid[t] = acc_ok;  // 0 none, 1 candidate rejected, 2 accepted
+    }
+    cp_async_commit();
+  };
+
   Acc acc;
 #pragma unroll
   for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
-  int pix0 = tile * kCorrTilePixels + threadIdx.x * 4;
+  // prologue: sub-tile 0 through G1 and the gate, sub-tile 1 through G1
+  load_indices(0);
+  tile_constants(0);
+  issue_g1(0);
+  load_indices(1);
+  tile_constants(1);
+  issue_g1(1);
+  load_indices(2);
+  __syncthreads();
+  cp_async_wait<1>();
+  gate_g2(0);
+  for (int j = 0; j < nsub; j++) {
+    tile_constants(j + 2);
+    issue_g1(j + 2);          // uses the indices loaded in the previous iteration
+    load_indices(j + 3);
+    __syncthreads();          // tile constants visible; slots of j-1 fully consumed
+    cp_async_wait<2>();       // G1(j+1) complete (groups after it: G2(j), G1(j+2))
+    gate_g2(j + 1);
+    cp_async_wait<2>();       // G2(j) complete (groups after it: G1(j+2), G2(j+1))
+    const int e = (j / kSubsPerTile) & 1;
+    const int sub = j % kSubsPerTile;
+    if (sub == 0) {
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    int p = pix0 + k;
-    if (p >= P) break;
-    int ri;
-    if (flags & 1) {
-      unsigned long long z = pd.zbuf[p];
-      if (flags & 2) pd.zbuf[p] = ~0ull;
-      ri = (z == ~0ull) ? -1 : (int)(unsigned)(z & 0xffffffffull);
-      if (flags & 4) pd.ref_index[p] = ri;
-    } else {
-      ri = pd.ref_index[p];
+      for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
     }
-    int ci = pd.cur_index[p];
-    if (ri < 0 || ci < 0 || ri >= nref || ci >= ncur) continue;
-    if (p / cols >= rmax) continue;
-    acc.v[29] += 1.0f;
-    float4 rp = pd.ref_pts[ri], rn = pd.ref_nrm[ri];
-    float4 cpt = pd.cur_pts[ci], cn = pd.cur_nrm[ci];
-    if (!gate(cp, Tg, rp, rn, cpt, cn)) continue;
-    acc.v[30] += 1.0f;
-    lin_terms(lp, Tl, rp, rn, cpt, cn, pd.cur_omg + 3 * (size_t)ci, acc);
+    if (!sSkip[e]) {
+      const GatherStage &g = stage_of(j);
+      const int v = g.valid[t];
+      if (v) acc.v[29] += 1.0f;
+      if (v == 2) {
+        acc.v[30] += 1.0f;
+        lin_terms(lp, sT[e] + 12, g.rp[t], g.rn[t], g.cp[t], g.cn[t], g.o0[t], g.o1[t], g.o2[t], acc);
+      }
+      if (sub == kSubsPerTile - 1) {
+        const PairDev &pd = pairs[sPair[e]];
+        block_reduce_store(acc, pd.partials + (size_t)(tile_of(j) - pd.tile_base) * kPartialWords);
+      }
+    }
   }
-  block_reduce_store(acc, pd.partials + (size_t)tile * kPartialWords);
+  cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------ list mode
@@ -388,8 +544,8 @@ __global__ void __launch_bounds__(kCorrThreads) k_lin_list(const PairDev *__rest
     if (ri < 0 || ci < 0 || ri >= nref || ci >= ncur) continue;
     acc.v[29] += 1.0f;
     acc.v[30] += 1.0f;
-    lin_terms(lp, Tl, pd.ref_pts[ri], pd.ref_nrm[ri], pd.cur_pts[ci], pd.cur_nrm[ci], pd.cur_omg + 3 * (size_t)ci,
-              acc);
+    const float4 *o = pd.cur_omg + 3 * (size_t)ci;
+    lin_terms(lp, Tl, pd.ref_pts[ri], pd.ref_nrm[ri], pd.cur_pts[ci], pd.cur_nrm[ci], o[0], o[1], o[2], acc);
   }
   block_reduce_store(acc, pd.partials + (size_t)tile * kPartialWords);
 }
@@ -526,17 +682,34 @@ void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int 
   prof->end(NICP_K_ZBUFFER, s);
 }
 
-void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out, cudaStream_t s,
-                    Profiler *prof) {
+void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out,
+                    int drop_no_normal, cudaStream_t s, Profiler *prof) {
   prof->begin(NICP_K_RESOLVE, s);
-  k_resolve<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, to_ref, depth_out);
+  k_resolve<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, to_ref, depth_out, drop_no_normal);
   prof->end(NICP_K_RESOLVE, s);
+}
+
+// Persistent grid: as many CTAs as fit on the device at once, never more
+// than there are tiles.
+static int corr_lin_grid(int total_tiles) {
+  static int resident = 0;
+  if (!resident) {
+    cudaFuncSetAttribute(k_corr_lin, cudaFuncAttributeMaxDynamicSharedMemorySize, kCorrSmem);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lin, kCorrThreads, kCorrSmem);
+    resident = std::max(1, sms * std::max(1, per_sm));
+  }
+  return std::min(total_tiles, resident);
 }
 
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
                      int flags, cudaStream_t s, Profiler *prof) {
+  if (total_tiles <= 0) return;
+  int grid = corr_lin_grid(total_tiles);
   prof->begin(NICP_K_CORR_LIN, s);
-  k_corr_lin<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, cp, lp, flags);
+  k_corr_lin<<<grid, kCorrThreads, kCorrSmem, s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
   prof->end(NICP_K_CORR_LIN, s);
 }
 

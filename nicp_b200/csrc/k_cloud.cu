@@ -433,6 +433,9 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
     }
   }
   f.nrm[idx] = nout;
+  // the point's w carries "has a normal" for the z-buffer key (see kNoNormalW)
+  reinterpret_cast<float *>(f.pts + idx)[3] =
+      (nout.x != 0.0f || nout.y != 0.0f || nout.z != 0.0f) ? 1.0f : kNoNormalW;
   float4 *o = f.omg + 3 * (size_t)idx;
   o[0] = make_float4(om[0], om[1], om[2], om[3]);
   o[1] = make_float4(om[4], om[5], om[6], om[7]);
@@ -454,8 +457,9 @@ __global__ void k_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *
   float A[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) A[k] = m12[k];
-  float3 p = xform_point(A, pts[i]);
-  pts[i] = make_float4(p.x, p.y, p.z, 1.0f);
+  float4 p0 = pts[i];
+  float3 p = xform_point(A, p0);
+  pts[i] = make_float4(p.x, p.y, p.z, p0.w);
   float4 n0 = nrm[i];
   float3 n = xform_normal(A, n0);
   nrm[i] = make_float4(n.x, n.y, n.z, n0.w);

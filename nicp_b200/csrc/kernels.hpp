@@ -78,8 +78,8 @@ void solution_statistics(const double H36[36], const double T16[16], double *tra
 
 void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int mode, const float *explicit_KRt,
                     cudaStream_t s, Profiler *prof);
-void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out, cudaStream_t s,
-                    Profiler *prof);
+void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out,
+                    int drop_no_normal, cudaStream_t s, Profiler *prof);
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
                      int flags, cudaStream_t s, Profiler *prof);
 void launch_corr_list(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, int use_state_T,
