@@ -239,6 +239,33 @@ int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur,
                    const nicp_lin_params *prm, int parity_threads, double H36[36], double b6[6],
                    double *error, int *inliers);
 
+/* The linearizer without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: a real-time loop
+ * (an odometry thread with a frame deadline) that cannot afford the
+ * device-wide synchronisation and unbounded latency of an allocation, or a
+ * host framework that owns all device memory and forbids libraries from
+ * taking more.  Same result as nicp_linearize, but:
+ *   - pairs_dev (2 * num_pairs int32) and out_dev (44 doubles: H 6x6
+ *     row-major, b[6], error, inliers) are caller-owned DEVICE buffers;
+ *   - the per-tile partial sums live in a fixed array inside the library's
+ *     device image (256 KB; every GPU that loads the library holds it until
+ *     the process exits), which limits num_pairs to
+ *     NICP_LINEARIZE_NOALLOC_MAX_PAIRS -- larger lists return NICP_EINVAL;
+ *   - the call is asynchronous on the context's stream; read out_dev after
+ *     synchronising that stream;
+ *   - every call shares that array, so calls whose kernels overlap on the
+ *     GPU (two streams, two host threads on one device) race; serialise them;
+ *   - the first call on a device looks the array's address up (once per
+ *     device, with the context's device current); make that first call
+ *     before any stream capture.
+ * Returns NICP_EINVAL for null arguments or a list beyond the limit,
+ * NICP_ESTATE when the context's device is not current, NICP_ECUDA when a
+ * launch or the address lookup fails; it writes no error text. */
+#define NICP_LINEARIZE_NOALLOC_MAX_PAIRS 1048576
+int nicp_linearize_noalloc(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur,
+                           const int32_t *pairs_dev, int num_pairs, const float T16[16],
+                           const nicp_lin_params *prm, int parity_threads, double *out_dev);
+
 /* -------------------------------------------------------------- aligner */
 /* AlignerProjective::align for one pair (one call, one pair).  guess,
  * ref_offset, cur_offset may be NULL (identity). */

@@ -105,6 +105,7 @@ SIGNATURES = {
                                   C.POINTER(C.c_int)]),
     "nicp_linearize": (C.c_int, [P, P, P, i32p, C.c_int, f32p, C.POINTER(LinParams), C.c_int, f64p, f64p,
                                  f64p, C.POINTER(C.c_int)]),
+    "nicp_linearize_noalloc": (C.c_int, [P, P, P, P, C.c_int, f32p, C.POINTER(LinParams), C.c_int, P]),
     "nicp_align": (C.c_int, [P, P, P, C.POINTER(Camera), f32p, f32p, f32p, C.POINTER(CorrParams),
                              C.POINTER(LinParams), C.POINTER(AlignParams), C.POINTER(AlignResult)]),
     "nicp_build_batch": (C.c_int, [P, C.c_int, C.POINTER(P), i32p, i32p, C.c_int, C.POINTER(Camera),
@@ -162,3 +163,6 @@ def f16(T):
     if T is None:
         return None
     return np.ascontiguousarray(np.asarray(T, dtype=np.float32).reshape(4, 4))
+
+
+NICP_LINEARIZE_NOALLOC_MAX_PAIRS = 1048576  # include/nicp_gpu.h

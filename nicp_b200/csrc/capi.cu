@@ -879,6 +879,34 @@ extern "C" int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_c
   return NICP_OK;
 }
 
+// Scratch-free linearizer (see nicp_gpu.h): unpacks the cloud handles and
+// enqueues k_lin_noalloc; no allocation and no error text on this path.
+extern "C" int nicp_linearize_noalloc(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur,
+                                      const int32_t *pairs_dev, int num_pairs, const float T16[16],
+                                      const nicp_lin_params *prm, int parity_threads, double *out_dev) {
+  if (!ctx || !ref || !cur || !T16 || !prm || !out_dev || num_pairs < 0 || (num_pairs > 0 && !pairs_dev))
+    return NICP_EINVAL;
+  if (num_pairs > NICP_LINEARIZE_NOALLOC_MAX_PAIRS) return NICP_EINVAL;
+  if (!ref->mem || !cur->mem) return NICP_EINVAL;
+  int device = -1;
+  if (cudaGetDevice(&device) != cudaSuccess) return NICP_ECUDA;
+  if (device != ctx->device) return NICP_ESTATE;
+  NoAllocLinArgs a;
+  a.ref_pts = ref->pts;
+  a.ref_nrm = ref->nrm;
+  a.ref_count = ref->count;
+  a.cur_pts = cur->pts;
+  a.cur_nrm = cur->nrm;
+  a.cur_omg = cur->omg;
+  a.cur_count = cur->count;
+  a.pairs = pairs_dev;
+  a.num_pairs = num_pairs;
+  a.parity_threads = std::max(1, parity_threads);
+  rows12(HM4::from(T16), a.T);
+  a.lp = lin_params(*prm);
+  return lin_noalloc(a, out_dev, ctx->stream);
+}
+
 // ------------------------------------------------------------------ projection API
 extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_camera *cam, const float T16[16],
                             int32_t *index_out, float *depth_out) {

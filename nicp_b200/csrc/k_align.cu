@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.hpp"
@@ -740,6 +741,105 @@ void launch_solve(const PairDev *d_pairs, int npairs, float lambda, int mode, do
   prof->begin(NICP_K_SOLVE, s);
   k_solve<<<npairs, 128, 0, s>>>(d_pairs, npairs, lambda, mode, early_eps, ignore_done);
   prof->end(NICP_K_SOLVE, s);
+}
+
+// ------------------------------------------------------------ scratch-free linearizer
+// The linearizer of nicp_linearize, for callers that must not allocate
+// device memory: the per-tile FP64 partials go to this fixed array instead
+// of the context workspace.  The array is part of the library's device
+// image, so it exists on every GPU that loads the library, from the first
+// load until the process exits.  Every call uses the same array: calls whose
+// kernels overlap on the GPU (different streams, or different host threads
+// on one device) race on it.  Nothing in it needs clearing -- each call
+// writes every partial it later reads.
+constexpr int kNoAllocMaxTiles = NICP_LINEARIZE_NOALLOC_MAX_PAIRS / kCorrTilePixels;
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxTiles * kPartialWords];
+
+__global__ void __launch_bounds__(kCorrThreads) k_lin_noalloc(NoAllocLinArgs a, double *__restrict__ partials) {
+  const int tile = blockIdx.x;
+  int K = a.num_pairs;
+  if (a.parity_threads > 1) K = (K / a.parity_threads) * a.parity_threads;
+  const int nref = *a.ref_count, ncur = *a.cur_count;
+  Acc acc;
+#pragma unroll
+  for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
+  const int i0 = tile * kCorrTilePixels + threadIdx.x * 4;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int i = i0 + k;
+    if (i >= K) break;
+    const int ri = a.pairs[2 * i], ci = a.pairs[2 * i + 1];
+    if (ri < 0 || ci < 0 || ri >= nref || ci >= ncur) continue;
+    acc.v[29] += 1.0f;
+    acc.v[30] += 1.0f;
+    const float4 *o = a.cur_omg + 3 * (size_t)ci;
+    lin_terms(a.lp, a.T, a.ref_pts[ri], a.ref_nrm[ri], a.cur_pts[ci], a.cur_nrm[ci], o[0], o[1], o[2], acc);
+  }
+  block_reduce_store(acc, partials + (size_t)tile * kPartialWords);
+}
+
+// Sums the tile partials in the same fixed order as k_solve and writes
+// H (36, row-major), b (6), error, inliers to out.
+__global__ void __launch_bounds__(128) k_lin_noalloc_sum(int ntiles, const double *__restrict__ partials,
+                                                         double *__restrict__ out) {
+  __shared__ double part[4][32];
+  __shared__ double tot[32];
+  const int e = threadIdx.x & 31, g = threadIdx.x >> 5;
+  double s = 0.0;
+  for (int t = g; t < ntiles; t += 4) s += partials[(size_t)t * kPartialWords + e];
+  part[g][e] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) tot[e] = ((part[0][e] + part[1][e]) + part[2][e]) + part[3][e];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const int li[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
+  for (int q = 0; q < 6; q++) {
+    const int i = li[q][0], j = li[q][1];
+    out[i * 6 + j] = out[j * 6 + i] = tot[q];
+    out[(3 + i) * 6 + 3 + j] = out[(3 + j) * 6 + 3 + i] = tot[15 + q];
+  }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) out[i * 6 + 3 + j] = out[(3 + j) * 6 + i] = tot[6 + i * 3 + j];
+  for (int i = 0; i < 3; i++) {
+    out[36 + i] = tot[21 + i];
+    out[39 + i] = tot[24 + i];
+  }
+  out[42] = (double)(float)tot[27];  // Linearizer::error() is a float
+  out[43] = (double)(int)tot[28];
+}
+
+// Device address of g_noalloc_partials, looked up once per device with that
+// device current (host code must not use the symbol itself as an address).
+static double *noalloc_partials_on(int device, cudaError_t *err) {
+  constexpr int kMaxDevices = 64;
+  static double *addr[kMaxDevices] = {};
+  static std::mutex m;
+  *err = cudaSuccess;
+  if (device < 0 || device >= kMaxDevices) {
+    *err = cudaErrorInvalidDevice;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(m);
+  if (!addr[device]) {
+    double *p = nullptr;
+    *err = cudaGetSymbolAddress((void **)&p, g_noalloc_partials);
+    if (*err != cudaSuccess) return nullptr;
+    addr[device] = p;
+  }
+  return addr[device];
+}
+
+int lin_noalloc(const NoAllocLinArgs &args, double *out_dev, cudaStream_t s) {
+  if (args.num_pairs < 0 || args.num_pairs > NICP_LINEARIZE_NOALLOC_MAX_PAIRS) return NICP_EINVAL;
+  int device = -1;
+  if (cudaGetDevice(&device) != cudaSuccess) return NICP_ECUDA;
+  cudaError_t err;
+  double *partials = noalloc_partials_on(device, &err);
+  if (!partials) return NICP_ECUDA;
+  const int ntiles = std::max(1, (args.num_pairs + kCorrTilePixels - 1) / kCorrTilePixels);
+  k_lin_noalloc<<<ntiles, kCorrThreads, 0, s>>>(args, partials);
+  k_lin_noalloc_sum<<<1, 128, 0, s>>>(ntiles, partials, out_dev);
+  return cudaGetLastError() == cudaSuccess ? NICP_OK : NICP_ECUDA;
 }
 
 }  // namespace nicp

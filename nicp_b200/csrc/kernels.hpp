@@ -91,4 +91,19 @@ void launch_init_pairs(const PairDev *d_pairs, int npairs, const double *d_guess
 void launch_solve(const PairDev *d_pairs, int npairs, float lambda, int mode, double early_eps, int ignore_done,
                   cudaStream_t s, Profiler *prof);
 
+// Inputs of the scratch-free linearizer, passed by value to the kernel.
+struct NoAllocLinArgs {
+  const float4 *ref_pts, *ref_nrm;
+  const int *ref_count;
+  const float4 *cur_pts, *cur_nrm, *cur_omg;
+  const int *cur_count;
+  const int32_t *pairs;  // device, 2 * num_pairs
+  int num_pairs;
+  int parity_threads;
+  float T[12];
+  LinParams lp;
+};
+// Enqueues the scratch-free linearizer on s; allocates nothing.
+int lin_noalloc(const NoAllocLinArgs &args, double *out_dev, cudaStream_t s);
+
 }  // namespace nicp
