@@ -26,7 +26,9 @@ constexpr int kCorrThreads = 256;       // 4 pixels per thread
 constexpr int kUnprojTilePixels = 4096; // 16 pixels per thread, 256 threads
 constexpr int kStatsThreads = 256;
 constexpr int kPartialWords = 32;       // doubles per CTA partial (21 H + 6 b + chi2 + inliers + C + K + pad)
-constexpr int kPointsPerCta = 256;      // z-buffer kernel: one point per thread
+constexpr int kZbufThreads = 256;
+constexpr int kZbufPointsPerThread = 4;
+constexpr int kPointsPerCta = kZbufThreads * kZbufPointsPerThread;  // z-buffer kernel tile
 
 // pts[i].w is 1 for a point with a non-zero normal and kNoNormalW otherwise
 // (the reference's Point has w = 1; downloads report 1).  The z-buffer key
@@ -211,56 +213,62 @@ __device__ __forceinline__ float4 unproject_pixel(const float *iKRt, int c, int 
 // the trigonometric roots of the characteristic cubic (Smith 1961) with
 // eigenvectors from cross products / the orthogonal complement (Eberly
 // 2014); LDL^T with symmetric diagonal pivoting (Golub & Van Loan 4.2).
-__device__ __forceinline__ void d_cross(const double *a, const double *b, double *c) {
+template <typename T>
+__device__ __forceinline__ void t_cross(const T *a, const T *b, T *c) {
   c[0] = a[1] * b[2] - a[2] * b[1];
   c[1] = a[2] * b[0] - a[0] * b[2];
   c[2] = a[0] * b[1] - a[1] * b[0];
 }
-__device__ __forceinline__ double d_dot(const double *a, const double *b) {
+template <typename T>
+__device__ __forceinline__ T t_dot(const T *a, const T *b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
+__device__ __forceinline__ void d_cross(const double *a, const double *b, double *c) { t_cross(a, b, c); }
+__device__ __forceinline__ double d_dot(const double *a, const double *b) { return t_dot(a, b); }
 
-__device__ inline void d_null_vector(const double *B, double mu, double *v) {
-  double r0[3] = {B[0] - mu, B[1], B[2]};
-  double r1[3] = {B[1], B[3] - mu, B[4]};
-  double r2[3] = {B[2], B[4], B[5] - mu};
-  double c0[3], c1[3], c2[3];
-  d_cross(r0, r1, c0);
-  d_cross(r0, r2, c1);
-  d_cross(r1, r2, c2);
-  double d0 = d_dot(c0, c0), d1 = d_dot(c1, c1), d2 = d_dot(c2, c2);
-  const double *best = c0;
-  double db = d0;
+template <typename T>
+__device__ inline void t_null_vector(const T *B, T mu, T *v) {
+  T r0[3] = {B[0] - mu, B[1], B[2]};
+  T r1[3] = {B[1], B[3] - mu, B[4]};
+  T r2[3] = {B[2], B[4], B[5] - mu};
+  T c0[3], c1[3], c2[3];
+  t_cross(r0, r1, c0);
+  t_cross(r0, r2, c1);
+  t_cross(r1, r2, c2);
+  T d0 = t_dot(c0, c0), d1 = t_dot(c1, c1), d2 = t_dot(c2, c2);
+  const T *best = c0;
+  T db = d0;
   if (d1 > db) { best = c1; db = d1; }
   if (d2 > db) { best = c2; db = d2; }
-  if (!(db > 0.0)) { v[0] = 1; v[1] = 0; v[2] = 0; return; }
-  double inv = 1.0 / sqrt(db);
+  if (!(db > T(0))) { v[0] = 1; v[1] = 0; v[2] = 0; return; }
+  T inv = T(1) / sqrt(db);
   v[0] = best[0] * inv; v[1] = best[1] * inv; v[2] = best[2] * inv;
 }
 
-__device__ inline void d_plane_vector(const double *B, const double *e, double mu, double *v) {
-  double u[3];
+template <typename T>
+__device__ inline void t_plane_vector(const T *B, const T *e, T mu, T *v) {
+  T u[3];
   if (fabs(e[0]) > fabs(e[1])) {
-    double il = 1.0 / sqrt(e[0] * e[0] + e[2] * e[2]);
+    T il = T(1) / sqrt(e[0] * e[0] + e[2] * e[2]);
     u[0] = -e[2] * il; u[1] = 0; u[2] = e[0] * il;
   } else {
-    double il = 1.0 / sqrt(e[1] * e[1] + e[2] * e[2]);
+    T il = T(1) / sqrt(e[1] * e[1] + e[2] * e[2]);
     u[0] = 0; u[1] = e[2] * il; u[2] = -e[1] * il;
   }
-  double w[3];
-  d_cross(e, u, w);
-  double Bu[3] = {B[0] * u[0] + B[1] * u[1] + B[2] * u[2], B[1] * u[0] + B[3] * u[1] + B[4] * u[2],
-                  B[2] * u[0] + B[4] * u[1] + B[5] * u[2]};
-  double Bw[3] = {B[0] * w[0] + B[1] * w[1] + B[2] * w[2], B[1] * w[0] + B[3] * w[1] + B[4] * w[2],
-                  B[2] * w[0] + B[4] * w[1] + B[5] * w[2]};
-  double m00 = d_dot(u, Bu) - mu, m01 = d_dot(u, Bw), m11 = d_dot(w, Bw) - mu;
-  double n0 = m00 * m00 + m01 * m01, n1 = m01 * m01 + m11 * m11;
-  double a, b;
+  T w[3];
+  t_cross(e, u, w);
+  T Bu[3] = {B[0] * u[0] + B[1] * u[1] + B[2] * u[2], B[1] * u[0] + B[3] * u[1] + B[4] * u[2],
+             B[2] * u[0] + B[4] * u[1] + B[5] * u[2]};
+  T Bw[3] = {B[0] * w[0] + B[1] * w[1] + B[2] * w[2], B[1] * w[0] + B[3] * w[1] + B[4] * w[2],
+             B[2] * w[0] + B[4] * w[1] + B[5] * w[2]};
+  T m00 = t_dot(u, Bu) - mu, m01 = t_dot(u, Bw), m11 = t_dot(w, Bw) - mu;
+  T n0 = m00 * m00 + m01 * m01, n1 = m01 * m01 + m11 * m11;
+  T a, b;
   if (n0 >= n1) {
-    if (n0 > 0) { double il = 1.0 / sqrt(n0); a = -m01 * il; b = m00 * il; }
+    if (n0 > T(0)) { T il = T(1) / sqrt(n0); a = -m01 * il; b = m00 * il; }
     else { a = 1; b = 0; }
   } else {
-    double il = 1.0 / sqrt(n1); a = -m11 * il; b = m01 * il;
+    T il = T(1) / sqrt(n1); a = -m11 * il; b = m01 * il;
   }
   v[0] = a * u[0] + b * w[0];
   v[1] = a * u[1] + b * w[1];
@@ -268,54 +276,56 @@ __device__ inline void d_plane_vector(const double *B, const double *e, double m
 }
 
 // A = {a00 a01 a02 a11 a12 a22}; lam ascending; U row-major, column k <-> lam[k].
-__device__ inline void d_eig3(const double *A, double *lam, double *U) {
-  double amax = fabs(A[0]);
+template <typename T>
+__device__ inline void t_eig3(const T *A, T *lam, T *U) {
+  T amax = fabs(A[0]);
   for (int i = 1; i < 6; i++) amax = fmax(amax, fabs(A[i]));
-  if (!(amax > 0.0)) {
+  if (!(amax > T(0))) {
     lam[0] = lam[1] = lam[2] = 0;
-    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? T(1) : T(0);
     return;
   }
-  double is = 1.0 / amax;
-  double B[6];
+  T is = T(1) / amax;
+  T B[6];
   for (int i = 0; i < 6; i++) B[i] = A[i] * is;
-  double m = (B[0] + B[3] + B[5]) / 3.0;
-  double b00 = B[0] - m, b11 = B[3] - m, b22 = B[5] - m;
-  double off = B[1] * B[1] + B[2] * B[2] + B[4] * B[4];
-  double p2 = b00 * b00 + b11 * b11 + b22 * b22 + 2.0 * off;
-  if (!(p2 > 0.0)) {
+  T m = (B[0] + B[3] + B[5]) / T(3);
+  T b00 = B[0] - m, b11 = B[3] - m, b22 = B[5] - m;
+  T off = B[1] * B[1] + B[2] * B[2] + B[4] * B[4];
+  T p2 = b00 * b00 + b11 * b11 + b22 * b22 + T(2) * off;
+  if (!(p2 > T(0))) {
     lam[0] = lam[1] = lam[2] = m * amax;
-    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? T(1) : T(0);
     return;
   }
-  double p = sqrt(p2 / 6.0);
-  double ip = 1.0 / p;
-  double c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip, c01 = B[1] * ip, c02 = B[2] * ip, c12 = B[4] * ip;
-  double det = c00 * (c11 * c22 - c12 * c12) - c01 * (c01 * c22 - c12 * c02) + c02 * (c01 * c12 - c11 * c02);
-  double q = det / 2.0;
-  q = fmin(1.0, fmax(-1.0, q));
-  double phi = acos(q) / 3.0;
-  const double tpi3 = 2.0943951023931954923;
-  double l2 = m + 2.0 * p * cos(phi);
-  double l0 = m + 2.0 * p * cos(phi + tpi3);
-  double l1 = 3.0 * m - l0 - l2;
-  double t;
+  T p = sqrt(p2 / T(6));
+  T ip = T(1) / p;
+  T c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip, c01 = B[1] * ip, c02 = B[2] * ip, c12 = B[4] * ip;
+  T det = c00 * (c11 * c22 - c12 * c12) - c01 * (c01 * c22 - c12 * c02) + c02 * (c01 * c12 - c11 * c02);
+  T q = det / T(2);
+  q = fmin(T(1), fmax(T(-1), q));
+  T phi = acos(q) / T(3);
+  const T tpi3 = T(2.0943951023931954923);
+  T l2 = m + T(2) * p * cos(phi);
+  T l0 = m + T(2) * p * cos(phi + tpi3);
+  T l1 = T(3) * m - l0 - l2;
+  T t;
   if (l1 < l0) { t = l1; l1 = l0; l0 = t; }
   if (l2 < l1) { t = l2; l2 = l1; l1 = t; }
   if (l1 < l0) { t = l1; l1 = l0; l0 = t; }
-  double v0[3], v1[3], v2[3];
+  T v0[3], v1[3], v2[3];
   if (l1 - l0 >= l2 - l1) {
-    d_null_vector(B, l0, v0);
-    d_plane_vector(B, v0, l1, v1);
-    d_cross(v0, v1, v2);
+    t_null_vector(B, l0, v0);
+    t_plane_vector(B, v0, l1, v1);
+    t_cross(v0, v1, v2);
   } else {
-    d_null_vector(B, l2, v2);
-    d_plane_vector(B, v2, l1, v1);
-    d_cross(v1, v2, v0);
+    t_null_vector(B, l2, v2);
+    t_plane_vector(B, v2, l1, v1);
+    t_cross(v1, v2, v0);
   }
   lam[0] = l0 * amax; lam[1] = l1 * amax; lam[2] = l2 * amax;
   for (int r = 0; r < 3; r++) { U[r * 3 + 0] = v0[r]; U[r * 3 + 1] = v1[r]; U[r * 3 + 2] = v2[r]; }
 }
+__device__ inline void d_eig3(const double *A, double *lam, double *U) { t_eig3<double>(A, lam, U); }
 
 // Solve A x = b for a symmetric 6x6 A given by its lower triangle.
 __device__ inline void d_ldlt_solve6(const double *A, const double *b, double *x) {

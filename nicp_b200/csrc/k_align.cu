@@ -45,26 +45,37 @@ __device__ __forceinline__ int find_pair(const PairDev *pairs, int n, int key, b
 // mode 0: project the current cloud with pair.KRt_cur-equivalent `explicit_KRt`
 // (one matrix for all pairs, host-computed); mode 1: the reference cloud with
 // the pair state's KRt.
-__global__ void __launch_bounds__(kPointsPerCta)
+__global__ void __launch_bounds__(kZbufThreads)
     k_zbuffer(const PairDev *__restrict__ pairs, int npairs, int mode, const float *__restrict__ explicit_KRt) {
   int pi = find_pair(pairs, npairs, blockIdx.x, true);
   const PairDev &pd = pairs[pi];
   const PairState *st = pd.state;
   if (mode == 1 && st->done) return;
-  int i = (blockIdx.x - pd.pt_tile_base) * kPointsPerCta + threadIdx.x;
+  const int i0 = (blockIdx.x - pd.pt_tile_base) * kPointsPerCta + threadIdx.x;
   const float4 *pts = mode ? pd.ref_pts : pd.cur_pts;
-  int n = mode ? *pd.ref_count : *pd.cur_count;
-  if (i >= n) return;
+  const int n = mode ? *pd.ref_count : *pd.cur_count;
+  if (i0 >= n) return;
   float K[12];
   const float *src = mode ? st->KRt : explicit_KRt + 12 * pi;
 #pragma unroll
   for (int k = 0; k < 12; k++) K[k] = src[k];
-  int x, y;
-  float d;
-  float4 p = pts[i];
-  if (!project_pixel(K, p, pd.rows, pd.cols, pd.min_d, pd.max_d, x, y, d)) return;
-  unsigned long long key = ((unsigned long long)float_key(d) << 32) | ((unsigned)i << 1) | (p.w != 1.0f ? 1u : 0u);
-  atomicMin(pd.zbuf + (size_t)y * pd.cols + x, key);
+  // four independent points per thread: their loads and atomics overlap
+  float4 p[kZbufPointsPerThread];
+#pragma unroll
+  for (int k = 0; k < kZbufPointsPerThread; k++) {
+    int i = i0 + k * kZbufThreads;
+    p[k] = (i < n) ? pts[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+#pragma unroll
+  for (int k = 0; k < kZbufPointsPerThread; k++) {
+    int i = i0 + k * kZbufThreads;
+    int x, y;
+    float d;
+    if (i >= n || !project_pixel(K, p[k], pd.rows, pd.cols, pd.min_d, pd.max_d, x, y, d)) continue;
+    unsigned long long key =
+        ((unsigned long long)float_key(d) << 32) | ((unsigned)i << 1) | (p[k].w != 1.0f ? 1u : 0u);
+    atomicMin(pd.zbuf + (size_t)y * pd.cols + x, key);
+  }
 }
 
 // Decodes a z-buffer word: the point index, or -1 when empty -- or, with
@@ -286,6 +297,18 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
   auto tile_of = [&](int j) { return (int)blockIdx.x + (j / kSubsPerTile) * (int)gridDim.x; };
   auto stage_of = [&](int j) -> GatherStage & { return stages[j % kCorrStages]; };
 
+  // Tile -> pair lookups, cached per pipeline stage (a stage's tile changes
+  // once every kSubsPerTile sub-tiles).
+  int lt_tile = -1, lt_pi = 0, gt_tile = -1, gt_pi = 0;
+  bool lt_skip = false, gt_skip = false;
+  auto lookup = [&](int tile, int &ctile, int &cpi, bool &cskip) {
+    if (tile != ctile) {
+      ctile = tile;
+      cpi = find_pair(pairs, npairs, tile, false);
+      cskip = !stats_pass && pairs[cpi].state->done;
+    }
+  };
+
   // Phase I (one iteration ahead, plain loads into registers): the two index
   // words of sub-tile j.
   unsigned long long zI = ~0ull;
@@ -295,8 +318,9 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
     cI = -1;
     if (j >= nsub) return;
     int tile = tile_of(j);
-    const PairDev &pd = pairs[find_pair(pairs, npairs, tile, false)];
-    if (!stats_pass && pd.state->done) return;
+    lookup(tile, lt_tile, lt_pi, lt_skip);
+    if (lt_skip) return;
+    const PairDev &pd = pairs[lt_pi];
     int p = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + threadIdx.x;
     if (p >= pd.rows * pd.cols) return;
     if (flags & 1) zI = pd.zbuf[p];
@@ -312,8 +336,9 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
     int ri = -1, ci = -1, valid = 0;
     if (j < nsub) {
       int tile = tile_of(j);
-      const PairDev &pd = pairs[find_pair(pairs, npairs, tile, false)];
-      if (stats_pass || !pd.state->done) {
+      lookup(tile, gt_tile, gt_pi, gt_skip);
+      const PairDev &pd = pairs[gt_pi];
+      if (!gt_skip) {
         int p = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + threadIdx.x;
         if (p < pd.rows * pd.cols) {
           if (flags & 1) {
@@ -347,7 +372,8 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
   auto tile_constants = [&](int j) {
     if (j >= nsub || j % kSubsPerTile) return;
     int e = (j / kSubsPerTile) & 1;
-    int pi = find_pair(pairs, npairs, tile_of(j), false);
+    lookup(tile_of(j), gt_tile, gt_pi, gt_skip);
+    const int pi = gt_pi;
     const PairState *st = pairs[pi].state;
     if (threadIdx.x < 24)
       sT[e][threadIdx.x] = threadIdx.x < 12 ? (stats_pass ? st->Tgate_used : st->Tgate)[threadIdx.x]
@@ -679,7 +705,7 @@ void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int 
                     cudaStream_t s, Profiler *prof) {
   if (total_pt_tiles <= 0) return;
   prof->begin(NICP_K_ZBUFFER, s);
-  k_zbuffer<<<total_pt_tiles, kPointsPerCta, 0, s>>>(d_pairs, npairs, mode, explicit_KRt);
+  k_zbuffer<<<total_pt_tiles, kZbufThreads, 0, s>>>(d_pairs, npairs, mode, explicit_KRt);
   prof->end(NICP_K_ZBUFFER, s);
 }
 

@@ -14,8 +14,8 @@
 //       Columns: one CTA per (plane, 32-column strip); each warp scans a band
 //       of rows, band totals are combined through shared memory.
 //   k_stats
-//       one thread per pixel: interval radius, 4-corner box query, 3x3
-//       covariance, FP64 eigensolve, curvature, oriented normal, and both
+//       one thread per pixel: interval radius, 4-corner box query, FP64 3x3
+//       covariance and eigensolve, curvature, oriented normal, and both
 //       information matrices (statscalculatorintegralimage.cpp:20-82,
 //       informationmatrixcalculator.cpp:9-57).
 //   k_cloud_transform
@@ -398,6 +398,11 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
       double mu0 = S[1] * dn, mu1 = S[2] * dn, mu2 = S[3] * dn;
       double C[6] = {S[4] * dn - mu0 * mu0, S[5] * dn - mu0 * mu1, S[6] * dn - mu0 * mu2,
                      S[7] * dn - mu1 * mu1, S[8] * dn - mu1 * mu2, S[9] * dn - mu2 * mu2};
+      // FP64 solve.  (An FP32 trigonometric solve refined in FP64 was
+      // measured: no faster -- this kernel is bound by its 40 scattered FP64
+      // moment reads per pixel, not by the eigensolve -- and its refinement
+      // could still settle on the wrong root when the two smallest
+      // eigenvalues are close.)
       d_eig3(C, lam, U);
       if (lam[0] < 0) lam[0] = 0;
       reached = true;
