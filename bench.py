@@ -17,6 +17,9 @@ one batched, graph-captured device loop.  Metric: 640x480 pairs/s.
                bytes per launch / average launch time (CUDA events)
   cpu_baseline the reference algorithm restated in C++ (oracle REF32, all host
                threads) on a bounded sample of the same workload
+  serving      the request loop (nicp_server_*) under open-loop Poisson load:
+               64 camera streams, 30/60/10% 320x240/640x480/1280x720,
+               p50/p99 latency and throughput per arrival rate
 
 --impl reference runs only the CPU reference arm.  Multi-GPU (torchrun):
 replicas only -- every rank runs the same workload on its own GPU; value is
@@ -225,6 +228,112 @@ def reference_arm(args, rank, world):
     return 0
 
 
+# ------------------------------------------------------------------ serving leg
+SERVE_MIX = (("320x240", 0.3, 19), ("640x480", 0.6, 38), ("1280x720", 0.1, 7))  # (camera, request share, streams)
+
+
+def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=40000):
+    """Open-loop Poisson load on the serving loop (nicp_server_*): 64 camera
+    streams, requests 30/60/10% at 320x240 / 640x480 / 1280x720, each aligned
+    against its stream's device-resident keyframe (replaced when inliers fall
+    below 40% of its points), admission against a 60 GB budget.  A stream
+    replays a 16-frame stretch of a 200-frame loop back and forth, so
+    consecutive requests of a stream are one trajectory step apart.  Latency
+    is submit -> result published, measured inside the server."""
+    from concurrent.futures import ThreadPoolExecutor
+    from nicp_b200 import _lib as L
+    from nicp_b200 import api, synth
+
+    streams = []  # (camera name, frames, poses, Camera)
+    jobs = []
+    for name, _, count in SERVE_MIX:
+        for _ in range(count):
+            jobs.append((seed + 31 * len(jobs), name))
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        rendered = list(ex.map(lambda j: synth.render_sequence(j[0], j[1], n_frames=frames_per_stream, period=200),
+                               jobs))
+    for (sd, name), (frames, poses, cam) in zip(jobs, rendered):
+        c = L.Camera()
+        L.load().nicp_default_camera(c)
+        c.fx, c.fy, c.cx, c.cy = cam["fx"], cam["fy"], cam["cx"], cam["cy"]
+        c.rows, c.cols = cam["rows"], cam["cols"]
+        streams.append((name, [np.ascontiguousarray(f) for f in frames], poses, c))
+    by_cam, base = [], 0
+    for name, share, count in SERVE_MIX:
+        by_cam.append(list(range(base, base + count)))
+        base += count
+    shares = np.array([s for _, s, _ in SERVE_MIX])
+
+    def frame_of(k):  # back-and-forth replay: 0..15..1, 0..15..1, ...
+        p = 2 * (frames_per_stream - 1)
+        k %= p
+        return k if k < frames_per_stream else p - k
+
+    out = []
+    for rate in rates:
+        rng = np.random.default_rng(seed + int(rate))
+        n = int(min(max_requests, rate * seconds))
+        gaps = rng.exponential(1.0 / rate, size=n)
+        cams = rng.choice(len(SERVE_MIX), size=n, p=shares)
+        sid = [by_cam[c][rng.integers(len(by_cam[c]))] for c in cams]
+        srv = api.Server(device=device, hbm_budget_bytes=60 << 30, max_batch=64, workers=2)
+        seq = [0] * len(streams)
+        meta = {}
+        t_sub = {}
+        results = []
+        t0 = time.perf_counter()
+        due = t0
+        for i in range(n):
+            due += gaps[i]
+            while time.perf_counter() < due:
+                pass
+            s = sid[i]
+            k = seq[s]
+            seq[s] += 1
+            meta[i] = (s, frame_of(k), k)
+            name, frames, poses, c = streams[s]
+            t_sub[i] = time.perf_counter()
+            srv.submit(s, i, frames[frame_of(k)], c)
+            if i % 256 == 255:
+                results += srv.poll()
+        t_submitted = time.perf_counter()
+        results += srv.drain(n - len(results), timeout_s=300)
+        srv.close()
+        ok = [r for r in results if r["status"] == 0]
+        lat = np.array([r["latency_ms"] for r in ok])
+        q = np.array([r["queue_ms"] for r in ok])
+        end = max(t_sub[r["request_id"]] + r["latency_ms"] / 1e3 for r in ok) if ok else t_submitted
+        # pose error vs ground truth: replay each stream's results in order
+        errs, replaced = [], 0
+        per_stream = {}
+        for r in sorted(ok, key=lambda r: r["request_id"]):
+            per_stream.setdefault(r["stream_id"], []).append(r)
+        for s, rs in per_stream.items():
+            key = None
+            poses = streams[s][2]
+            for r in rs:
+                f = meta[r["request_id"]][1]
+                if key is not None:  # T maps the frame into the keyframe it was aligned against
+                    errs.append(synth.pose_error(r["T"], synth.rel(poses[key], poses[f])))
+                if r["keyframe_replaced"]:
+                    key = f
+                    replaced += 1
+        er = np.array([e[0] for e in errs]) if errs else np.zeros(1)
+        et = np.array([e[1] for e in errs]) if errs else np.zeros(1)
+        out.append({"offered_rps": rate, "submitted_rps": n / (t_submitted - t0), "requests": n,
+                    "completed": len(ok), "failed": len(results) - len(ok), "lost": n - len(results),
+                    "throughput_rps": len(ok) / (end - t0),
+                    "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+                    "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+                    "queue_p50_ms": float(np.percentile(q, 50)) if len(q) else None,
+                    "mean_batch": float(np.mean([r["batch_size"] for r in ok])) if ok else None,
+                    "keyframe_replacements": replaced,
+                    "pose_err_vs_truth": {"rad_p50": float(np.median(er)), "rad_p99": float(np.percentile(er, 99)),
+                                          "m_p50": float(np.median(et)), "m_p99": float(np.percentile(et, 99))}})
+    return {"streams": len(streams), "mix": {n: s for n, s, _ in SERVE_MIX}, "budget_gb": 60, "workers": 2,
+            "max_batch": 64, "arrivals": "poisson, open loop", "seconds_per_rate": seconds, "rates": out}
+
+
 def workload_config(args):
     return {"workload": "640x480 frame-to-frame sequence, %d frames (%d pairs), reference defaults, "
                         "%d outer x 1 inner" % (args.frames, args.frames - 1, 10),
@@ -245,6 +354,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-call leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
+    ap.add_argument("--serve-rates", default="500,2000,5000,10000,20000",
+                    help="Poisson arrival rates (requests/s) of the serving leg")
+    ap.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per rate")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -400,6 +513,10 @@ def main():
             pl.append(nplain / (time.perf_counter() - t0))
         plain = max(pl)
 
+    serving = None
+    if not args.no_serve and rank == 0:
+        serving = serve_leg(local, [float(r) for r in args.serve_rates.split(",")], args.serve_seconds, args.seed)
+
     cpu = None
     if not args.no_cpu and rank == 0:
         v, n, dt, threads = cpu_baseline(frames, cam, seconds=args.cpu_seconds)
@@ -417,7 +534,7 @@ def main():
                 "gpu_launches": int(launches), "clocks": clk,
                 "plain_pairs_per_s": plain, "batched_over_plain": (value / world / plain) if plain else None,
                 "pose_err_vs_truth_median": {"rad": rot_med, "m": tr_med},
-                "points_per_frame": V, "correspondences_per_pair": C}
+                "points_per_frame": V, "correspondences_per_pair": C, "serving": serving}
         print(json.dumps(line), flush=True)
     del clouds
     ctx.close()

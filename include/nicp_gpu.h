@@ -290,6 +290,57 @@ int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs,
                      const nicp_corr_params *corr, const nicp_lin_params *lin,
                      const nicp_align_params *prm, nicp_align_result *out);
 
+/* -------------------------------------------------------------- serving */
+/* A request loop (no counterpart in the reference; the closest caller is the
+ * frame-to-frame odometry of nicp_simple_aligner.cpp:129-184): every camera
+ * stream keeps its keyframe cloud resident on the device; each submitted
+ * frame is built into a cloud and aligned against its stream's keyframe.
+ * Requests are admitted while the device memory they need fits the budget,
+ * and batched as they arrive: whenever one of `workers` batch slots frees,
+ * it takes every admissible pending request (at most one in flight per
+ * stream, so a stream's frames stay in order).  Batches of different workers
+ * run on different CUDA streams and overlap on the device.  A stream's
+ * keyframe is replaced by the current frame when inliers fall below
+ * keyframe_min_inlier_ratio x the keyframe's points; the first frame of a
+ * stream becomes its keyframe (result T = identity). */
+typedef struct nicp_server nicp_server;
+
+typedef struct {
+  size_t hbm_budget_bytes;        /* device memory for in-flight work and keyframes */
+  int max_batch;                  /* requests per batch */
+  int workers;                    /* batches in flight */
+  float keyframe_min_inlier_ratio;
+  nicp_cloud_params cloud;
+  nicp_corr_params corr;
+  nicp_lin_params lin;
+  nicp_align_params align;        /* compute_statistics is ignored */
+} nicp_server_params;
+
+typedef struct {
+  uint64_t request_id;
+  int stream_id;
+  int status;             /* NICP_OK, or NICP_EBUDGET when the request can never fit */
+  double T[16];           /* current frame -> its stream's keyframe */
+  float error;
+  int inliers;
+  int keyframe_points;
+  int keyframe_replaced;  /* the frame became the stream's keyframe */
+  int batch_size;         /* requests in the batch that carried it */
+  double latency_ms;      /* submit -> result available */
+  double queue_ms;        /* submit -> batch start */
+} nicp_server_result;
+
+void nicp_default_server_params(nicp_server_params *p);
+int nicp_server_create(int device, const nicp_server_params *prm, nicp_server **out);
+/* Copies the u16 frame; returns immediately. */
+int nicp_server_submit(nicp_server *s, int stream_id, uint64_t request_id, const uint16_t *depth, int rows,
+                       int cols, const nicp_camera *cam);
+/* Up to max finished results; waits up to wait_ms for the first one. */
+int nicp_server_poll(nicp_server *s, nicp_server_result *out, int max, int *n, int wait_ms);
+/* pending = submitted but not finished; device_bytes = held by the server. */
+int nicp_server_status(nicp_server *s, int *pending, size_t *device_bytes);
+int nicp_server_destroy(nicp_server *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,19 @@ class AlignResult(C.Structure):
                 ("rotational_ratio", C.c_double), ("solution_valid", C.c_int), ("status", C.c_int)]
 
 
+class ServerParams(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_batch", C.c_int), ("workers", C.c_int),
+                ("keyframe_min_inlier_ratio", C.c_float), ("cloud", CloudParams), ("corr", CorrParams),
+                ("lin", LinParams), ("align", AlignParams)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("request_id", C.c_uint64), ("stream_id", C.c_int), ("status", C.c_int), ("T", D16),
+                ("error", C.c_float), ("inliers", C.c_int), ("keyframe_points", C.c_int),
+                ("keyframe_replaced", C.c_int), ("batch_size", C.c_int), ("latency_ms", C.c_double),
+                ("queue_ms", C.c_double)]
+
+
 P = C.c_void_p
 i32p = C.POINTER(C.c_int32)
 f32p = C.POINTER(C.c_float)
@@ -113,6 +126,12 @@ SIGNATURES = {
     "nicp_align_batch": (C.c_int, [P, C.c_int, C.POINTER(P), C.POINTER(P), C.POINTER(Camera), f32p,
                                    C.POINTER(CorrParams), C.POINTER(LinParams), C.POINTER(AlignParams),
                                    C.POINTER(AlignResult)]),
+    "nicp_default_server_params": (None, [C.POINTER(ServerParams)]),
+    "nicp_server_create": (C.c_int, [C.c_int, C.POINTER(ServerParams), C.POINTER(P)]),
+    "nicp_server_submit": (C.c_int, [P, C.c_int, C.c_uint64, P, C.c_int, C.c_int, C.POINTER(Camera)]),
+    "nicp_server_poll": (C.c_int, [P, C.POINTER(ServerResult), C.c_int, C.POINTER(C.c_int), C.c_int]),
+    "nicp_server_status": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
+    "nicp_server_destroy": (C.c_int, [P]),
 }
 
 _lib = None

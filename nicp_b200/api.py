@@ -685,3 +685,69 @@ def align_batch(ctx, refs, curs, cams, guesses, corr, lin, prm):
     ctx.check(ctx.lib.nicp_align_batch(ctx.h, n, r, c, camarr, L.fptr(g), C.byref(corr), C.byref(lin), C.byref(prm),
                                        res))
     return res
+
+
+# ------------------------------------------------------------------ serving (no reference counterpart)
+class Server:
+    """Continuous-batching request loop (nicp_server_* in include/nicp_gpu.h):
+    device-resident keyframe per camera stream, admission by HBM budget,
+    batches formed as requests arrive, several batches in flight."""
+
+    def __init__(self, device=0, hbm_budget_bytes=60 << 30, max_batch=64, workers=2, keyframe_min_inlier_ratio=0.4,
+                 params=None):
+        self.lib = L.load()
+        p = L.ServerParams()
+        self.lib.nicp_default_server_params(C.byref(p))
+        p.hbm_budget_bytes = int(hbm_budget_bytes)
+        p.max_batch, p.workers = int(max_batch), int(workers)
+        p.keyframe_min_inlier_ratio = float(keyframe_min_inlier_ratio)
+        if params:
+            params(p)
+        h = C.c_void_p()
+        rc = self.lib.nicp_server_create(device, C.byref(p), C.byref(h))
+        if rc != L.NICP_OK:
+            raise L.NicpError(rc, "cannot create the server")
+        self.h = h
+        self._buf = (L.ServerResult * 4096)()
+
+    def submit(self, stream_id, request_id, depth_u16, camera):
+        d = np.ascontiguousarray(depth_u16, np.uint16)
+        rows, cols = d.shape
+        rc = self.lib.nicp_server_submit(self.h, int(stream_id), int(request_id), d.ctypes.data_as(C.c_void_p),
+                                         rows, cols, C.byref(camera))
+        L.check(rc)
+
+    def poll(self, wait_ms=0):
+        n = C.c_int(0)
+        L.check(self.lib.nicp_server_poll(self.h, self._buf, len(self._buf), C.byref(n), int(wait_ms)))
+        out = []
+        for i in range(n.value):
+            r = self._buf[i]
+            out.append(dict(request_id=r.request_id, stream_id=r.stream_id, status=r.status,
+                            T=np.array(r.T).reshape(4, 4), error=r.error, inliers=r.inliers,
+                            keyframe_points=r.keyframe_points, keyframe_replaced=bool(r.keyframe_replaced),
+                            batch_size=r.batch_size, latency_ms=r.latency_ms, queue_ms=r.queue_ms))
+        return out
+
+    def status(self):
+        p, b = C.c_int(0), C.c_size_t(0)
+        L.check(self.lib.nicp_server_status(self.h, C.byref(p), C.byref(b)))
+        return p.value, b.value
+
+    def drain(self, expected, timeout_s=120.0):
+        import time
+        got, t0 = [], time.time()
+        while len(got) < expected and time.time() - t0 < timeout_s:
+            got += self.poll(wait_ms=50)
+        return got
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nicp_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -22,14 +22,14 @@ GPU_LIB = os.path.join(HERE, "libnicp_b200.so")
 SYNTH_LIB = os.path.join(HERE, "libnicp_synth.so")
 
 CUDA_SOURCES = ["k_cloud.cu", "k_align.cu", "capi.cu"]
-HOST_SOURCES = ["stats_host.cpp"]
+HOST_SOURCES = ["stats_host.cpp", "server.cpp"]
 HEADERS = ["common.cuh", "kernels.hpp", "host_math.hpp"]
 
 NVCC = os.environ.get("NVCC", "nvcc")
 # The image may export CXX pointing at a toolchain without libgomp.
 CXX = os.environ.get("NICP_CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-HOST_FLAGS = ["-O3", "-fPIC", "-std=c++17", "-ffp-contract=off"]
+HOST_FLAGS = ["-O3", "-fPIC", "-std=c++17", "-ffp-contract=off", "-pthread"]
 
 
 def _newer(target, deps):

@@ -149,7 +149,7 @@ static int cloud_reserve(nicp_cloud *c, int capacity, int rows, int cols, bool e
   size_t o_pts = L.take(16 * (size_t)capacity), o_nrm = L.take(16 * (size_t)capacity);
   size_t o_omg = L.take(48 * (size_t)capacity);
   size_t o_eig = eig ? L.take(48 * (size_t)capacity) : 0;
-  size_t o_cnt = L.take(sizeof(int));
+  size_t o_cnt = L.take(2 * sizeof(int));  // points, points with a normal
   size_t o_idx = L.take(4 * std::max<size_t>(P, 1));
   if (cudaMalloc(&c->mem, L.off) != cudaSuccess) {
     cudaGetLastError();
@@ -168,7 +168,7 @@ static int cloud_reserve(nicp_cloud *c, int capacity, int rows, int cols, bool e
   c->eig = eig ? (float *)(c->mem + o_eig) : nullptr;
   c->count = (int *)(c->mem + o_cnt);
   c->index = (int32_t *)(c->mem + o_idx);
-  CK(ctx, cudaMemsetAsync(c->count, 0, sizeof(int), ctx->stream));
+  CK(ctx, cudaMemsetAsync(c->count, 0, 2 * sizeof(int), ctx->stream));
   return NICP_OK;
 }
 
@@ -439,8 +439,10 @@ extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const fl
   int rc = cloud_reserve(c, n, c->rows, c->cols, false);
   if (rc) return rc;
   std::vector<float4> pts(n), nrm(n), omg(3 * (size_t)n);
+  int counts[2] = {n, 0};
   for (int i = 0; i < n; i++) {
     bool has_normal = n4[4 * i] != 0.0f || n4[4 * i + 1] != 0.0f || n4[4 * i + 2] != 0.0f;
+    counts[1] += has_normal;
     pts[i] = make_float4(p4[4 * i], p4[4 * i + 1], p4[4 * i + 2], has_normal ? 1.0f : kNoNormalW);
     nrm[i] = make_float4(n4[4 * i], n4[4 * i + 1], n4[4 * i + 2], curv[i]);
     float o[12] = {0};
@@ -453,7 +455,7 @@ extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const fl
     CK(ctx, cudaMemcpyAsync(c->nrm, nrm.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
     CK(ctx, cudaMemcpyAsync(c->omg, omg.data(), 48 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
   }
-  CK(ctx, cudaMemcpyAsync(c->count, &n, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CK(ctx, cudaMemcpyAsync(c->count, counts, sizeof(counts), cudaMemcpyHostToDevice, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return NICP_OK;
 }
@@ -953,6 +955,7 @@ struct AlignCall {
   const nicp_lin_params *lin;
   const nicp_align_params *prm;
   bool graph;
+  bool foreign_clouds = false;  // clouds of another context on the same device (the server's workers)
 };
 }  // namespace
 
@@ -1029,7 +1032,8 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
   for (int i = 0; i < a.n; i++) {
     if (!a.refs[i] || !a.curs[i] || !a.refs[i]->mem || !a.curs[i]->mem)
       return fail(ctx, NICP_EINVAL, "pair " + std::to_string(i) + " has an empty cloud");
-    if (a.refs[i]->ctx != ctx || a.curs[i]->ctx != ctx) return fail(ctx, NICP_EINVAL, "cloud of another context");
+    if (!a.foreign_clouds && (a.refs[i]->ctx != ctx || a.curs[i]->ctx != ctx))
+      return fail(ctx, NICP_EINVAL, "cloud of another context");
   }
   bool list_mode = a.corr->parity_threads > 1;
   bool keep_ref = p.inner_iterations > 1 || p.compute_statistics;
@@ -1151,3 +1155,43 @@ extern "C" int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *r
   AlignCall a{n, refs, curs, cams, guesses, nullptr, nullptr, corr, lin, prm, true};
   return align_impl(ctx, a, out);
 }
+
+// ------------------------------------------------------------------ internal hooks of the server
+namespace nicp {
+namespace internal {
+
+// Batch build into clouds that may belong to another context of this device.
+int build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *rows, const int *cols,
+                const nicp_camera *cams, const nicp_cloud_params *prm, nicp_cloud *const *out) {
+  if (!ctx || n < 0) return NICP_EINVAL;
+  std::vector<FrameIn> f(n);
+  for (int i = 0; i < n; i++) f[i] = FrameIn{depth[i], true, false, 0, rows[i], cols[i], nullptr};
+  return build_frames(ctx, n, f.data(), cams, prm, out, false);
+}
+
+// Batch align with direct launches (batch shapes vary from call to call).
+int align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs, const nicp_cloud *const *curs,
+                const nicp_camera *cams, const nicp_corr_params *corr, const nicp_lin_params *lin,
+                const nicp_align_params *prm, nicp_align_result *out) {
+  AlignCall a{n, refs, curs, cams, nullptr, nullptr, nullptr, corr, lin, prm, false, true};
+  return align_impl(ctx, a, out);
+}
+
+// Counts of points with a normal of n clouds, with one synchronisation.
+int cloud_normal_counts(nicp_ctx *ctx, int n, const nicp_cloud *const *c, int *out) {
+  char *pin;
+  int rc = pin_down(ctx, sizeof(int) * (size_t)std::max(n, 1), &pin);
+  if (rc) return rc;
+  for (int i = 0; i < n; i++) {
+    if (!c[i]->mem) { reinterpret_cast<int *>(pin)[i] = 0; continue; }
+    CK(ctx, cudaMemcpyAsync(pin + sizeof(int) * i, c[i]->count + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(out, pin, sizeof(int) * (size_t)n);
+  return NICP_OK;
+}
+
+size_t cloud_bytes(const nicp_cloud *c) { return c ? c->bytes : 0; }
+
+}  // namespace internal
+}  // namespace nicp

@@ -61,7 +61,7 @@ struct FrameDev {
   int32_t *index;             // rows*cols
   float4 *pts, *nrm, *omg;
   float *eig;
-  int *count;                 // device scalar: number of points
+  int *count;                 // device: [0] number of points, [1] points with a normal
   // scratch
   int *tile_counts;           // per unprojection tile
   void *moments;              // 10 planes of rows*cols values (double / float / float2)

@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(256) k_unproject_count(const FrameDev *__restr
   for (int k = 0; k < 16; k++) cnt += depth_valid(d[k], f.min_d, f.max_d) ? 1 : 0;
   int tot = block_sum_int(cnt, red);
   if (threadIdx.x == 0) f.tile_counts[tile] = tot;
+  if (tile == 0 && threadIdx.x == 0) f.count[1] = 0;  // points with a normal, counted by k_stats
 }
 
 __global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restrict__ frames, int nframes) {
@@ -438,6 +439,13 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
     }
   }
   f.nrm[idx] = nout;
+  {
+    // count the points that got a normal (one atomic per warp)
+    const bool has = nout.x != 0.0f || nout.y != 0.0f || nout.z != 0.0f;
+    const unsigned act = __activemask();
+    const unsigned m = __ballot_sync(act, has);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(act) - 1) && m) atomicAdd(f.count + 1, __popc(m));
+  }
   // the point's w carries "has a normal" for the z-buffer key (see kNoNormalW)
   reinterpret_cast<float *>(f.pts + idx)[3] =
       (nout.x != 0.0f || nout.y != 0.0f || nout.z != 0.0f) ? 1.0f : kNoNormalW;

@@ -131,15 +131,17 @@ def base_pose(rng, kind=ROOM):
                   [rng.uniform(-0.2, 0.2), rng.uniform(-0.15, 0.15), -1.8 + rng.uniform(-0.1, 0.1)])
 
 
-def trajectory(seed, n_frames=200, kind=ROOM):
-    """A smooth periodic camera path through the room: per-frame steps stay
-    below 1.5 degrees and 2 cm."""
+def trajectory(seed, n_frames=200, kind=ROOM, period=None):
+    """A smooth periodic camera path through the room, one loop every
+    `period` frames (default n_frames): with a period of 200 or more the
+    per-frame steps stay below 1.5 degrees and 2 cm."""
+    period = period or n_frames
     rng = np.random.default_rng(seed)
     P0 = base_pose(rng, kind)
     ph = rng.uniform(0, 2 * math.pi, size=6)
     poses = []
     for k in range(n_frames):
-        w = 2 * math.pi * k / n_frames
+        w = 2 * math.pi * k / period
         yaw = math.radians(15) * math.sin(w + ph[0])
         pitch = math.radians(6) * math.sin(2 * w + ph[1])
         roll = math.radians(4) * math.sin(w + ph[2])
@@ -171,10 +173,12 @@ def render_pair(seed, cam_name="320x240", deg=2.0, meters=0.03, deg_hi=None, m_h
     return d1, d2, rel(P1, P2), cam
 
 
-def render_sequence(seed, cam_name="640x480", n_frames=200, kind=ROOM, sigma_coef=SIGMA_COEF, drop_prob=DROP_PROB):
-    """Frames of the seeded smooth trajectory; returns (frames, poses, camera dict)."""
+def render_sequence(seed, cam_name="640x480", n_frames=200, kind=ROOM, sigma_coef=SIGMA_COEF, drop_prob=DROP_PROB,
+                    period=None):
+    """Frames of the seeded smooth trajectory (one loop every `period`
+    frames, default n_frames); returns (frames, poses, camera dict)."""
     scene = make_scene(seed, kind)
-    poses = trajectory(seed, n_frames, kind)
+    poses = trajectory(seed, n_frames, kind, period)
     cam = camera_dict(cam_name)
     args = (cam["fx"], cam["fy"], cam["cx"], cam["cy"], cam["rows"], cam["cols"])
     frames = [render(scene, P, *args, noise_seed=seed * 100003 + k, sigma_coef=sigma_coef, drop_prob=drop_prob)
