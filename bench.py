@@ -17,6 +17,8 @@ one batched, graph-captured device loop.  Metric: 640x480 pairs/s.
                bytes per launch / average launch time (CUDA events)
   cpu_baseline the reference algorithm restated in C++ (oracle REF32, all host
                threads) on a bounded sample of the same workload
+  mixed_batch  512 independent pairs of mixed resolution, <= 20 x 2 iterations
+               with early exit, batched vs the plain per-pair loop
   serving      the request loop (nicp_server_*) under open-loop Poisson load:
                64 camera streams, 30/60/10% 320x240/640x480/1280x720,
                p50/p99 latency and throughput per arrival rate
@@ -228,11 +230,120 @@ def reference_arm(args, rank, world):
     return 0
 
 
+# ------------------------------------------------------------------ mixed batch leg
+MIXED_CAMS = ("160x120", "320x240", "640x480")
+
+
+def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, plain_pairs=48):
+    """512 independent frame pairs, each its own seeded scene, resolutions
+    drawn uniformly from 160x120 / 320x240 / 640x480, the current frame
+    offset by 0.5-5 deg and 1-8 cm.  One step builds the 1024 clouds and
+    aligns the 512 pairs (up to 20 outer x 2 inner, a pair stops once its
+    pose change falls below 1e-6) in one graph-captured device loop.  The
+    plain leg runs the same pairs one call at a time (nicp_cloud_from_depth_u16
+    twice + nicp_align), with the same iteration controls."""
+    import ctypes as Cc
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from nicp_b200 import _lib as L
+    from nicp_b200 import api, synth
+
+    rng = np.random.default_rng(seed)
+    names = [MIXED_CAMS[i] for i in rng.integers(0, 3, size=npairs)]
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        pairs = list(ex.map(lambda i: synth.render_pair(seed + 1000 + i, names[i], deg=0.5, deg_hi=5.0, meters=0.01,
+                                                        m_hi=0.08), range(npairs)))
+    # device-resident frames: one buffer, 256-byte aligned slots
+    sizes = [2 * p[0].size for p in pairs for _ in range(2)]
+    offs = np.concatenate([[0], np.cumsum([(s + 255) // 256 * 256 for s in sizes])])
+    dev = torch.empty(int(offs[-1]), dtype=torch.uint8, device="cuda:%d" % device)
+    host = torch.empty(int(offs[-1]), dtype=torch.uint8).pin_memory()
+    hv = host.numpy()
+    for k, (p, j) in enumerate((p, j) for p in pairs for j in range(2)):
+        a = np.ascontiguousarray(p[j], np.uint16).view(np.uint8).ravel()
+        hv[offs[k]:offs[k] + a.size] = a
+    dev.copy_(host)
+    cams = []
+    for d1, d2, Tgt, cam in pairs:
+        proj = api.PinholePointProjector(ctx)
+        proj.setCameraMatrix([[cam["fx"], 0, cam["cx"]], [0, cam["fy"], cam["cy"]], [0, 0, 1]])
+        proj.setImageSize(cam["rows"], cam["cols"])
+        cams.append(proj.camera())
+    _, conv, corr, lin, prm = gpu_objects(ctx, pairs[0][3])
+    prm_c = conv.params()
+    prm.outer_iterations, prm.inner_iterations, prm.early_exit_eps = 20, 2, 1e-6
+    clouds = [api.Cloud(ctx) for _ in range(2 * npairs)]
+    dptrs = [(dev.data_ptr() + int(offs[k]), pairs[k // 2][3]["rows"], pairs[k // 2][3]["cols"])
+             for k in range(2 * npairs)]
+    fcams = [cams[k // 2] for k in range(2 * npairs)]
+
+    def step(p):
+        api.build_batch(ctx, dptrs, fcams, prm_c, clouds, on_device=True)
+        return api.align_batch(ctx, clouds[0::2], clouds[1::2], cams, None, corr, lin, p)
+
+    def timed(p):
+        for _ in range(warmup):
+            step(p)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(steps):
+                res = step(p)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, res
+
+    ms, res = timed(prm)
+    prm_fixed = L.AlignParams.from_buffer_copy(prm)
+    prm_fixed.early_exit_eps = 0.0
+    ms_fixed, res_fixed = timed(prm_fixed)
+    prof, _ = profile_step(ctx, lambda: step(prm))
+    total = sum(v[0] for v in prof.values()) or 1.0
+    shares = {k: [round(v[0] / total, 4), v[1]] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+    iters = [r.outer_iterations_run for r in res]
+    errs = [synth.pose_error(np.array(r.T).reshape(4, 4), p[2]) for r, p in zip(res, pairs)]
+    ok = [e for e in errs if e[0] < 0.01 and e[1] < 0.02]
+    # equal results with and without early exit, where a pair converged
+    dT = max(float(np.max(np.abs(np.array(a.T) - np.array(b.T)))) for a, b in zip(res, res_fixed))
+
+    # plain per-pair loop over a sample of the same pairs
+    res1 = L.AlignResult()
+    pl = []
+    for rep in range(2):
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for i in range(plain_pairs):
+            for j in range(2):
+                k = 2 * i + j
+                ctx.check(ctx.lib.nicp_cloud_from_depth_u16(ctx.h, Cc.c_void_p(dptrs[k][0]), dptrs[k][1], dptrs[k][2],
+                                                            0, 1, Cc.byref(cams[i]), Cc.byref(prm_c), None,
+                                                            clouds[k].h, None))
+            ctx.check(ctx.lib.nicp_align(ctx.h, clouds[2 * i].h, clouds[2 * i + 1].h, Cc.byref(cams[i]), None, None,
+                                         None, Cc.byref(corr), Cc.byref(lin), Cc.byref(prm), Cc.byref(res1)))
+        ctx.synchronize()
+        pl.append(plain_pairs / (time.perf_counter() - t0))
+    plain = max(pl)
+    value = npairs / (ms / 1e3)
+    del clouds
+    return {"workload": "%d independent pairs, resolutions uniform over %s, offsets 0.5-5 deg / 1-8 cm, "
+                        "<= 20 outer x 2 inner, early exit at pose change < 1e-6" % (npairs, "/".join(MIXED_CAMS)),
+            "pairs_per_s": value, "ms_per_step": ms, "pairs_per_s_no_early_exit": npairs / (ms_fixed / 1e3),
+            "plain_pairs_per_s": plain, "batched_over_plain": value / plain,
+            "outer_iterations_run": {"mean": float(np.mean(iters)), "max": int(max(iters)), "min": int(min(iters))},
+            "max_abs_T_diff_vs_no_early_exit": dT,
+            "converged_within_0.01rad_2cm": len(ok) / npairs,
+            "pose_err_vs_truth_median": {"rad": float(np.median([e[0] for e in errs])),
+                                         "m": float(np.median([e[1] for e in errs]))},
+            "resolution_counts": {n: names.count(n) for n in MIXED_CAMS},
+            "kernel_shares_and_launches": shares, "profiled_step_ms": total}
+
+
 # ------------------------------------------------------------------ serving leg
 SERVE_MIX = (("320x240", 0.3, 19), ("640x480", 0.6, 38), ("1280x720", 0.1, 7))  # (camera, request share, streams)
 
 
-def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=40000):
+def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=40000, workers=2, submitters=4):
     """Open-loop Poisson load on the serving loop (nicp_server_*): 64 camera
     streams, requests 30/60/10% at 320x240 / 640x480 / 1280x720, each aligned
     against its stream's device-resident keyframe (replaced when inliers fall
@@ -269,41 +380,73 @@ def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=4
         k %= p
         return k if k < frames_per_stream else p - k
 
+    srv = api.Server(device=device, hbm_budget_bytes=60 << 30, max_batch=64, workers=workers)
+    seq = [0] * len(streams)
+    rid = [0]
+
+    def submit(s, t_sub, meta):
+        k = seq[s]
+        seq[s] += 1
+        i = rid[0]
+        rid[0] += 1
+        meta[i] = (s, frame_of(k))
+        t_sub[i] = time.perf_counter()
+        srv.submit(s, i, streams[s][1][frame_of(k)], streams[s][3])
+
+    # warm-up: a burst of 3 requests per stream (sizes the pools and
+    # workspaces, sets every stream's keyframe), then a settle
+    wmeta, wt = {}, {}
+    for _ in range(3):
+        for s in range(len(streams)):
+            submit(s, wt, wmeta)
+    srv.drain(len(wmeta), timeout_s=300)
+
     out = []
     for rate in rates:
         rng = np.random.default_rng(seed + int(rate))
         n = int(min(max_requests, rate * seconds))
-        gaps = rng.exponential(1.0 / rate, size=n)
         cams = rng.choice(len(SERVE_MIX), size=n, p=shares)
-        sid = [by_cam[c][rng.integers(len(by_cam[c]))] for c in cams]
-        srv = api.Server(device=device, hbm_budget_bytes=60 << 30, max_batch=64, workers=2)
-        seq = [0] * len(streams)
-        meta = {}
-        t_sub = {}
+        sid = np.array([by_cam[c][rng.integers(len(by_cam[c]))] for c in cams])
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+        meta, t_sub = {}, {}
+        first = rid[0]
+        # submitters: streams are split between threads (a stream's requests
+        # stay in order); each follows the arrival times of its streams
+        lock = threading.Lock()
+
+        def run(t, t0):
+            mine = np.nonzero(sid % submitters == t)[0]
+            for i in mine:
+                due = t0 + arrivals[i]
+                while time.perf_counter() < due:
+                    pass
+                with lock:
+                    k = seq[sid[i]]
+                    seq[sid[i]] += 1
+                    j = first + int(i)
+                meta[j] = (int(sid[i]), frame_of(k))
+                t_sub[j] = time.perf_counter()
+                srv.submit(int(sid[i]), j, streams[sid[i]][1][frame_of(k)], streams[sid[i]][3])
+
+        t0 = time.perf_counter() + 0.01
+        th = [threading.Thread(target=run, args=(t, t0)) for t in range(submitters)]
+        for x in th:
+            x.start()
         results = []
-        t0 = time.perf_counter()
-        due = t0
-        for i in range(n):
-            due += gaps[i]
-            while time.perf_counter() < due:
-                pass
-            s = sid[i]
-            k = seq[s]
-            seq[s] += 1
-            meta[i] = (s, frame_of(k), k)
-            name, frames, poses, c = streams[s]
-            t_sub[i] = time.perf_counter()
-            srv.submit(s, i, frames[frame_of(k)], c)
-            if i % 256 == 255:
-                results += srv.poll()
-        t_submitted = time.perf_counter()
+        while any(x.is_alive() for x in th):
+            results += srv.poll(wait_ms=5)
+        for x in th:
+            x.join()
+        t_submitted = max(t_sub.values())
+        rid[0] = first + n
         results += srv.drain(n - len(results), timeout_s=300)
-        srv.close()
         ok = [r for r in results if r["status"] == 0]
         lat = np.array([r["latency_ms"] for r in ok])
         q = np.array([r["queue_ms"] for r in ok])
         end = max(t_sub[r["request_id"]] + r["latency_ms"] / 1e3 for r in ok) if ok else t_submitted
         # pose error vs ground truth: replay each stream's results in order
+        # (the keyframe of a stream's first request here is the one the
+        # previous load left: unknown frame, so that request is skipped)
         errs, replaced = [], 0
         per_stream = {}
         for r in sorted(ok, key=lambda r: r["request_id"]):
@@ -330,8 +473,13 @@ def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=4
                     "keyframe_replacements": replaced,
                     "pose_err_vs_truth": {"rad_p50": float(np.median(er)), "rad_p99": float(np.percentile(er, 99)),
                                           "m_p50": float(np.median(et)), "m_p99": float(np.percentile(et, 99))}})
-    return {"streams": len(streams), "mix": {n: s for n, s, _ in SERVE_MIX}, "budget_gb": 60, "workers": 2,
-            "max_batch": 64, "arrivals": "poisson, open loop", "seconds_per_rate": seconds, "rates": out}
+        # let the queue empty before the next rate
+        while srv.status()[0]:
+            time.sleep(0.01)
+    srv.close()
+    return {"streams": len(streams), "mix": {n: s for n, s, _ in SERVE_MIX}, "budget_gb": 60, "workers": workers,
+            "max_batch": 64, "submitter_threads": submitters, "arrivals": "poisson, open loop",
+            "seconds_per_rate": seconds, "warmup": "3 requests per stream, burst", "rates": out}
 
 
 def workload_config(args):
@@ -355,6 +503,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-call leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the 512-pair mixed-resolution batch leg")
     ap.add_argument("--serve-rates", default="500,2000,5000,10000,20000",
                     help="Poisson arrival rates (requests/s) of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per rate")
@@ -513,6 +662,10 @@ def main():
             pl.append(nplain / (time.perf_counter() - t0))
         plain = max(pl)
 
+    mixed = None
+    if not args.no_mixed and rank == 0:
+        mixed = mixed_batch_leg(ctx, stream, local, args.seed + 17)
+
     serving = None
     if not args.no_serve and rank == 0:
         serving = serve_leg(local, [float(r) for r in args.serve_rates.split(",")], args.serve_seconds, args.seed)
@@ -534,7 +687,8 @@ def main():
                 "gpu_launches": int(launches), "clocks": clk,
                 "plain_pairs_per_s": plain, "batched_over_plain": (value / world / plain) if plain else None,
                 "pose_err_vs_truth_median": {"rad": rot_med, "m": tr_med},
-                "points_per_frame": V, "correspondences_per_pair": C, "serving": serving}
+                "points_per_frame": V, "correspondences_per_pair": C, "mixed_batch": mixed,
+                "serving": serving}
         print(json.dumps(line), flush=True)
     del clouds
     ctx.close()

@@ -297,12 +297,16 @@ int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs,
  * frame is built into a cloud and aligned against its stream's keyframe.
  * Requests are admitted while the device memory they need fits the budget,
  * and batched as they arrive: whenever one of `workers` batch slots frees,
- * it takes every admissible pending request (at most one in flight per
- * stream, so a stream's frames stay in order).  Batches of different workers
+ * it takes the oldest admissible pending requests, up to max_batch and its
+ * share (1/workers) of the active streams (at most one request in flight
+ * per stream, so a stream's frames stay in order).  Batches of different workers
  * run on different CUDA streams and overlap on the device.  A stream's
  * keyframe is replaced by the current frame when inliers fall below
- * keyframe_min_inlier_ratio x the keyframe's points; the first frame of a
- * stream becomes its keyframe (result T = identity). */
+ * keyframe_min_inlier_ratio x the keyframe's points (points with a normal);
+ * the first frame of a stream becomes its keyframe (result T = identity).
+ * Each alignment starts from the stream's previous estimate against the
+ * same keyframe (identity right after a replacement), the constant-position
+ * guess of a tracker. */
 typedef struct nicp_server nicp_server;
 
 typedef struct {

@@ -1171,9 +1171,9 @@ int build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *r
 
 // Batch align with direct launches (batch shapes vary from call to call).
 int align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs, const nicp_cloud *const *curs,
-                const nicp_camera *cams, const nicp_corr_params *corr, const nicp_lin_params *lin,
-                const nicp_align_params *prm, nicp_align_result *out) {
-  AlignCall a{n, refs, curs, cams, nullptr, nullptr, nullptr, corr, lin, prm, false, true};
+                const nicp_camera *cams, const float *guesses, const nicp_corr_params *corr,
+                const nicp_lin_params *lin, const nicp_align_params *prm, nicp_align_result *out) {
+  AlignCall a{n, refs, curs, cams, guesses, nullptr, nullptr, corr, lin, prm, false, true};
   return align_impl(ctx, a, out);
 }
 

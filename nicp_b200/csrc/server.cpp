@@ -32,8 +32,8 @@ namespace internal {
 int build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *rows, const int *cols,
                 const nicp_camera *cams, const nicp_cloud_params *prm, nicp_cloud *const *out);
 int align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs, const nicp_cloud *const *curs,
-                const nicp_camera *cams, const nicp_corr_params *corr, const nicp_lin_params *lin,
-                const nicp_align_params *prm, nicp_align_result *out);
+                const nicp_camera *cams, const float *guesses, const nicp_corr_params *corr,
+                const nicp_lin_params *lin, const nicp_align_params *prm, nicp_align_result *out);
 int cloud_normal_counts(nicp_ctx *ctx, int n, const nicp_cloud *const *c, int *out);
 size_t cloud_bytes(const nicp_cloud *c);
 }  // namespace internal
@@ -65,6 +65,7 @@ struct StreamState {
   int key_rows = 0, key_cols = 0;
   nicp_camera key_cam{};
   int key_points = 0;  // keyframe points with a normal
+  float guess[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};  // last estimate against the keyframe
   bool busy = false;
 };
 
@@ -187,6 +188,7 @@ void nicp_server::worker(int w) {
     std::vector<int> pair_of(n, -1);
     std::vector<const nicp_cloud *> refs, curs;
     std::vector<nicp_camera> pcams;
+    std::vector<float> guesses;
     {
       std::lock_guard<std::mutex> lk(m);
       for (int i = 0; i < n; i++) {
@@ -196,6 +198,7 @@ void nicp_server::worker(int w) {
           refs.push_back(ss.keyframe);
           curs.push_back(cur_clouds[i]);
           pcams.push_back(cams[i]);
+          guesses.insert(guesses.end(), ss.guess, ss.guess + 16);
         }
       }
     }
@@ -204,8 +207,8 @@ void nicp_server::worker(int w) {
     if (rc == NICP_OK && !refs.empty()) {
       nicp_align_params ap = prm.align;
       ap.compute_statistics = 0;
-      rc = nicp::internal::align_batch(ctx, (int)refs.size(), refs.data(), curs.data(), pcams.data(), &prm.corr,
-                                       &prm.lin, &ap, res.data());
+      rc = nicp::internal::align_batch(ctx, (int)refs.size(), refs.data(), curs.data(), pcams.data(),
+                                       guesses.data(), &prm.corr, &prm.lin, &ap, res.data());
     }
     if (rc == NICP_OK) rc = nicp::internal::cloud_normal_counts(ctx, n, cur_clouds.data(), cur_counts.data());
     if (rc == NICP_OK) rc = nicp_ctx_synchronize(ctx);
@@ -229,6 +232,7 @@ void nicp_server::worker(int w) {
           r.inliers = a.inliers;
           r.keyframe_points = ss.key_points;
           replace = (double)a.inliers < (double)prm.keyframe_min_inlier_ratio * ss.key_points;
+          for (int k = 0; k < 16; k++) ss.guess[k] = (float)a.T[k];  // the next frame starts from here
         }
         size_t px = (size_t)rq.rows * rq.cols;
         if (rc == NICP_OK && replace) {
@@ -241,6 +245,7 @@ void nicp_server::worker(int w) {
           ss.key_cols = rq.cols;
           ss.key_cam = rq.cam;
           ss.key_points = cur_counts[i];
+          for (int k = 0; k < 16; k++) ss.guess[k] = (k % 5 == 0) ? 1.0f : 0.0f;
           keyframe_bytes += kKeyframeBytesPerPixel * px;
           r.keyframe_replaced = 1;
         } else if (cur_clouds[i]) {
@@ -296,6 +301,7 @@ extern "C" int nicp_server_submit(nicp_server *s, int stream_id, uint64_t reques
                                   int cols, const nicp_camera *cam) {
   if (!s || !depth || rows <= 0 || cols <= 0 || !cam) return NICP_EINVAL;
   Request r;
+  r.submitted = Clock::now();  // latency counts the copy of the frame below
   r.id = request_id;
   r.stream = stream_id;
   r.rows = rows;
@@ -304,7 +310,6 @@ extern "C" int nicp_server_submit(nicp_server *s, int stream_id, uint64_t reques
   r.cam.rows = rows;
   r.cam.cols = cols;
   r.depth.assign(depth, depth + (size_t)rows * cols);
-  r.submitted = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->m);
     s->queues[stream_id].push_back(std::move(r));
