@@ -144,7 +144,11 @@ def run_step(ctx, frames_ptrs, cam_c, prm_c, clouds, corr, lin, prm, on_device):
 # Algorithmic bytes per unit (the per-stage figures of the scope table):
 #   S1 unproject     2P + 4P + 12V          S2 moments   2P + 10 s P (+ the column pass reads and writes it)
 #   S3 stats + Omega 10 s P + 6P + 76V      S4 z-buffer  12V + 8V (+ 8P init, 8P resolve read, 4P write)
-#   S5 corr + lin    8P + 104 C             (s = 8 bytes per FP64 moment)
+#   S5 corr + lin    8P + 56 C: both index images, then per correspondence
+#                    point xyz, normal xyz and curvature of both clouds; the
+#                    information matrices are rebuilt from the current normal
+#                    (structured Omega), not read (the general path adds 48 C)
+#                    (s = 8 bytes per FP64 moment)
 def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     s = 8
     if kernel == "unproject":
@@ -158,7 +162,7 @@ def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     if kernel == "zbuffer":
         return (12 * V + 8 * V) * pairs
     if kernel == "corr_lin":
-        return (8 * P + 104 * C) * pairs
+        return (8 * P + 56 * C) * pairs
     if kernel == "resolve":
         return (8 * P + 4 * P) * pairs
     return 0
@@ -622,7 +626,7 @@ def main():
     top_ms, top_n = prof[top]
     launches_per_step = top_n
     per_launch_bytes = {
-        "corr_lin": (8 * P + 104 * C) * npairs,
+        "corr_lin": (8 * P + 56 * C) * npairs,
         "zbuffer": (12 * V + 8 * V) * npairs,
         "stats_omega": (10 * 8 * P + 6 * P + 76 * V) * F,
         "moments_rows": (2 * P + 80 * P) * F,

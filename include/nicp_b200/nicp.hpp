@@ -120,6 +120,14 @@ class Cloud {
   std::vector<float> points() const { return field(0); }
   std::vector<float> normals() const { return field(1); }
   std::vector<float> curvature() const { return field(2); }
+  // gaussians() (cloud.h:107): means n x 3 and covariances n x 9 (row-major);
+  // needs a converter with setKeepGaussians(true)
+  void gaussians(std::vector<float> &means, std::vector<float> &covariances) const {
+    size_t n = size();
+    means.resize(3 * n);
+    covariances.resize(9 * n);
+    check(ctx_->handle(), nicp_cloud_download_gaussians(h_, means.data(), covariances.data()));
+  }
   void transformInPlace(const Isometry3f &T) { check(ctx_->handle(), nicp_cloud_transform(h_, T.data())); }
 
  private:
@@ -260,6 +268,8 @@ class DepthImageConverterIntegralImage {
                                    PointInformationMatrixCalculator *pim, NormalInformationMatrixCalculator *nim)
       : proj_(projector), stats_(stats), pim_(pim), nim_(nim) {}
   void setDepthScale(float s) { depth_scale_ = s; }
+  // Also fill Cloud::gaussians() (the reference always does; opt-in here).
+  void setKeepGaussians(bool v) { keep_gaussians_ = v; }
   // compute(cloud, depthImage, sensorOffset): u16 depth in depthScale units.
   void compute(Cloud &cloud, const uint16_t *depth, int rows, int cols,
                const Isometry3f &sensorOffset = Isometry3f::Identity()) {
@@ -291,6 +301,7 @@ class DepthImageConverterIntegralImage {
     std::memcpy(p.nim_flat, nim_->flat(), sizeof(p.nim_flat));
     std::memcpy(p.nim_nonflat, nim_->nonflat(), sizeof(p.nim_nonflat));
     p.nim_curvature_threshold = nim_->curvatureThreshold();
+    p.keep_gaussians = keep_gaussians_ ? 1 : 0;
     return p;
   }
   PinholePointProjector *proj_;
@@ -298,6 +309,7 @@ class DepthImageConverterIntegralImage {
   PointInformationMatrixCalculator *pim_;
   NormalInformationMatrixCalculator *nim_;
   float depth_scale_ = 0.001f;
+  bool keep_gaussians_ = false;
 };
 
 // correspondencefinder{,projective}.{h,cpp}.

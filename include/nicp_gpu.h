@@ -96,6 +96,11 @@ typedef struct {
   float nim_curvature_threshold;
   int moments_precision; /* NICP_MOMENTS_*; F64 is the default */
   int keep_stats;        /* also store eigenvalues/eigenvectors per point */
+  /* also store the per-point sensor-noise Gaussian3f (mean + covariance) of
+   * PinholePointProjector::unProject(points, gaussians, ...)
+   * (pinholepointprojector.cpp:93-134).  The reference always computes it;
+   * only the Merger consumes it, so here it is opt-in (0 = off). */
+  int keep_gaussians;
 } nicp_cloud_params;
 
 /* CorrespondenceFinder(Projective) (correspondencefinder.cpp:9-18). */
@@ -118,6 +123,10 @@ typedef struct {
   int z_scaling;
   float scale;
   int demoted_to_gicp;
+  /* Precision study: sum the per-tile FP64 partials in FP32 instead of FP64
+   * (the reference sums its per-thread float partials in float,
+   * linearizer.cpp:119-127).  0 (default) = FP64. */
+  int cross_block_f32;
 } nicp_lin_params;
 
 /* Aligner (aligner.cpp:21-41) plus the device-loop controls. */
@@ -181,6 +190,14 @@ int nicp_cloud_create(nicp_ctx *ctx, nicp_cloud **out);
 int nicp_cloud_destroy(nicp_cloud *c);
 /* Number of points (synchronizes). */
 int nicp_cloud_size(nicp_cloud *c, int *n);
+
+/* Cloud::gaussians() (cloud.h:107; filled by unProject,
+ * pinholepointprojector.cpp:93-134, moved by Gaussian3fVector::
+ * transformInPlace, gaussian3.h:66-73): per point the mean (3 floats) and
+ * the 3x3 covariance (9 floats, row-major).  Either pointer may be null.
+ * NICP_ESTATE when the cloud was not built with keep_gaussians. */
+int nicp_cloud_download_gaussians(nicp_cloud *cloud, float *mean3, float *cov9);
+
 /* Any output may be NULL.  points4/normals4: n*4 floats (w = 1 / 0);
  * curvature: n; omega_p9/omega_n9: n*9 (3x3 blocks); eigval3: n*3;
  * eigvec9: n*9 (columns are eigenvectors; needs keep_stats). */

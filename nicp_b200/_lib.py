@@ -36,7 +36,7 @@ class CloudParams(C.Structure):
                 ("curvature_threshold", C.c_float),
                 ("pim_flat", F3), ("pim_nonflat", F3), ("pim_curvature_threshold", C.c_float),
                 ("nim_flat", F3), ("nim_nonflat", F3), ("nim_curvature_threshold", C.c_float),
-                ("moments_precision", C.c_int), ("keep_stats", C.c_int)]
+                ("moments_precision", C.c_int), ("keep_stats", C.c_int), ("keep_gaussians", C.c_int)]
 
 
 class CorrParams(C.Structure):
@@ -47,7 +47,7 @@ class CorrParams(C.Structure):
 
 class LinParams(C.Structure):
     _fields_ = [("inlier_max_chi2", C.c_float), ("robust_kernel", C.c_int), ("z_scaling", C.c_int),
-                ("scale", C.c_float), ("demoted_to_gicp", C.c_int)]
+                ("scale", C.c_float), ("demoted_to_gicp", C.c_int), ("cross_block_f32", C.c_int)]
 
 
 class AlignParams(C.Structure):
@@ -103,6 +103,7 @@ SIGNATURES = {
     "nicp_cloud_destroy": (C.c_int, [P]),
     "nicp_cloud_size": (C.c_int, [P, C.POINTER(C.c_int)]),
     "nicp_cloud_download": (C.c_int, [P, f32p, f32p, f32p, f32p, f32p, f32p, f32p]),
+    "nicp_cloud_download_gaussians": (C.c_int, [P, f32p, f32p]),
     "nicp_cloud_upload": (C.c_int, [P, C.c_int, f32p, f32p, f32p, f32p, f32p]),
     "nicp_cloud_transform": (C.c_int, [P, f32p]),
     "nicp_cloud_from_depth_u16": (C.c_int, [P, P, C.c_int, C.c_int, C.c_size_t, C.c_int, C.POINTER(Camera),

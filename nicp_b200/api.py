@@ -125,6 +125,15 @@ class Cloud:
             out["eigenvectors"] = U.reshape(n, 3, 3)
         return out
 
+    def gaussians(self):
+        """Cloud::gaussians() (cloud.h:107): (means n x 3, covariances n x 3 x 3);
+        the cloud must have been built with keepGaussians."""
+        n = self.size()
+        m = np.zeros((n, 3), np.float32)
+        c = np.zeros((n, 9), np.float32)
+        self.ctx.check(self.ctx.lib.nicp_cloud_download_gaussians(self.h, L.fptr(m), L.fptr(c)))
+        return m, c.reshape(n, 3, 3)
+
     def points(self):
         return self.download()["points"]
 
@@ -344,6 +353,9 @@ class DepthImageConverterIntegralImage:
         self._nim = normalInformationMatrixCalculator
         self.depthScale = 0.001
         self.keepStats = False
+        # unProject's per-point Gaussian3f (mean + covariance); the reference
+        # always fills Cloud::gaussians(), here it is opt-in
+        self.keepGaussians = False
         self._indexImage = None
 
     def projector(self): return self._projector
@@ -369,6 +381,7 @@ class DepthImageConverterIntegralImage:
         prm.nim_curvature_threshold = n._curvatureThreshold
         prm.moments_precision = s.momentsPrecision
         prm.keep_stats = 1 if self.keepStats else 0
+        prm.keep_gaussians = 1 if self.keepGaussians else 0
         return prm
 
     def compute(self, cloud, depthImage, sensorOffset=None, keep_index=False):
@@ -471,6 +484,8 @@ class Linearizer:
         self._inlierMaxChi2 = 9e3
         self._robustKernel = True
         self._demotedToGeneralizedICP = False
+        # precision study: sum the per-tile partials in FP32 (default FP64)
+        self.crossBlockF32 = False
         self._zScaling = False
         self._scale = 1.0
         self._H = np.zeros((6, 6))
@@ -506,6 +521,7 @@ class Linearizer:
         p.z_scaling = 1 if self._zScaling else 0
         p.scale = self._scale
         p.demoted_to_gicp = 1 if self._demotedToGeneralizedICP else 0
+        p.cross_block_f32 = 1 if self.crossBlockF32 else 0
         return p
 
     def update(self, referenceCloud=None, currentCloud=None, correspondences=None, parity_threads=None):

@@ -67,9 +67,16 @@ struct nicp_cloud {
   size_t bytes = 0;
   int capacity = 0;  // points
   int rows = 0, cols = 0;
-  bool has_eig = false;
+  bool has_eig = false, has_gauss = false;      // storage reserved
+  bool eig_valid = false, gauss_valid = false;  // written by the last build
+  // information matrices Omega = d1 I + (d0 - d1) n n^T with (d0, d1) per
+  // class in omd (point flat / non-flat, normal flat / non-flat): true for
+  // clouds built with such parameters, false for uploaded ones
+  bool omega_structured = false;
+  float omd[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   float4 *pts = nullptr, *nrm = nullptr, *omg = nullptr;
   float *eig = nullptr;
+  float4 *gauss = nullptr;  // 3 float4 per point: mean, then the 9 covariance entries row-major
   int *count = nullptr;
   int32_t *index = nullptr;
 };
@@ -130,11 +137,11 @@ static int pin_down(nicp_ctx *ctx, size_t bytes, char **out) {
   return NICP_OK;
 }
 
-static int cloud_reserve(nicp_cloud *c, int capacity, int rows, int cols, bool eig) {
+static int cloud_reserve(nicp_cloud *c, int capacity, int rows, int cols, bool eig, bool gauss = false) {
   nicp_ctx *ctx = c->ctx;
   size_t P = (size_t)rows * cols;
   if (capacity < 1) capacity = 1;
-  if (capacity <= c->capacity && P <= (size_t)c->rows * c->cols && (!eig || c->has_eig)) {
+  if (capacity <= c->capacity && P <= (size_t)c->rows * c->cols && (!eig || c->has_eig) && (!gauss || c->has_gauss)) {
     c->rows = rows;
     c->cols = cols;
     return NICP_OK;
@@ -149,6 +156,7 @@ static int cloud_reserve(nicp_cloud *c, int capacity, int rows, int cols, bool e
   size_t o_pts = L.take(16 * (size_t)capacity), o_nrm = L.take(16 * (size_t)capacity);
   size_t o_omg = L.take(48 * (size_t)capacity);
   size_t o_eig = eig ? L.take(48 * (size_t)capacity) : 0;
+  size_t o_gauss = gauss ? L.take(48 * (size_t)capacity) : 0;
   size_t o_cnt = L.take(2 * sizeof(int));  // points, points with a normal
   size_t o_idx = L.take(4 * std::max<size_t>(P, 1));
   if (cudaMalloc(&c->mem, L.off) != cudaSuccess) {
@@ -162,10 +170,13 @@ static int cloud_reserve(nicp_cloud *c, int capacity, int rows, int cols, bool e
   c->rows = rows;
   c->cols = cols;
   c->has_eig = eig;
+  c->has_gauss = gauss;
+  c->eig_valid = c->gauss_valid = false;
   c->pts = (float4 *)(c->mem + o_pts);
   c->nrm = (float4 *)(c->mem + o_nrm);
   c->omg = (float4 *)(c->mem + o_omg);
   c->eig = eig ? (float *)(c->mem + o_eig) : nullptr;
+  c->gauss = gauss ? (float4 *)(c->mem + o_gauss) : nullptr;
   c->count = (int *)(c->mem + o_cnt);
   c->index = (int32_t *)(c->mem + o_idx);
   CK(ctx, cudaMemsetAsync(c->count, 0, 2 * sizeof(int), ctx->stream));
@@ -227,6 +238,7 @@ extern "C" void nicp_default_cloud_params(nicp_cloud_params *p) {
   p->pim_curvature_threshold = 0.02f;
   p->nim_curvature_threshold = 0.02f;
   p->moments_precision = NICP_MOMENTS_F64;
+  p->keep_gaussians = 0;
   p->keep_stats = 0;
 }
 
@@ -245,6 +257,7 @@ extern "C" void nicp_default_lin_params(nicp_lin_params *p) {
   p->z_scaling = 0;
   p->scale = 1.0f;
   p->demoted_to_gicp = 0;
+  p->cross_block_f32 = 0;
 }
 
 extern "C" void nicp_default_align_params(nicp_align_params *p) {
@@ -401,7 +414,7 @@ extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *c
   int rc = nicp_cloud_size(c, &n);
   if (rc) return rc;
   if (n == 0) return NICP_OK;
-  if ((ev3 || U9) && !c->has_eig) return fail(ctx, NICP_ESTATE, "cloud was built without keep_stats");
+  if ((ev3 || U9) && !c->eig_valid) return fail(ctx, NICP_ESTATE, "cloud was built without keep_stats");
   std::vector<float4> nrm(n), omg(3 * (size_t)n);
   std::vector<float> eig;
   if (p4) CK(ctx, cudaMemcpyAsync(p4, c->pts, 16 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -432,12 +445,33 @@ extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *c
   return NICP_OK;
 }
 
+extern "C" int nicp_cloud_download_gaussians(nicp_cloud *c, float *mean3, float *cov9) {
+  if (!c) return NICP_EINVAL;
+  nicp_ctx *ctx = c->ctx;
+  int n = 0;
+  int rc = nicp_cloud_size(c, &n);
+  if (rc) return rc;
+  if (n == 0) return NICP_OK;
+  if (!c->gauss_valid) return fail(ctx, NICP_ESTATE, "cloud was built without keep_gaussians");
+  std::vector<float4> g(3 * (size_t)n);
+  CK(ctx, cudaMemcpyAsync(g.data(), c->gauss, 48 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < n; i++) {
+    const float *o = reinterpret_cast<const float *>(&g[3 * (size_t)i]);
+    if (mean3) for (int k = 0; k < 3; k++) mean3[3 * (size_t)i + k] = o[k];
+    if (cov9) for (int k = 0; k < 9; k++) cov9[9 * (size_t)i + k] = o[3 + k];
+  }
+  return NICP_OK;
+}
+
 extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const float *n4, const float *curv,
                                  const float *op9, const float *on9) {
   if (!c || n < 0 || (n > 0 && (!p4 || !n4 || !curv))) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int rc = cloud_reserve(c, n, c->rows, c->cols, false);
   if (rc) return rc;
+  c->eig_valid = c->gauss_valid = false;
+  c->omega_structured = false;
   std::vector<float4> pts(n), nrm(n), omg(3 * (size_t)n);
   int counts[2] = {n, 0};
   for (int i = 0; i < n; i++) {
@@ -478,8 +512,8 @@ extern "C" int nicp_cloud_transform(nicp_cloud *c, const float T16[16]) {
   if ((rc = ensure_ws(ctx, L.off))) return rc;
   CK(ctx, cudaMemcpyAsync(ctx->ws + o, pin, 48, cudaMemcpyHostToDevice, ctx->stream));
   CK(ctx, cudaEventRecord(ctx->pin_up_ev, ctx->stream));
-  launch_cloud_transform(c->pts, c->nrm, c->omg, c->has_eig ? c->eig : nullptr, c->count, c->capacity,
-                         (const float *)(ctx->ws + o), ctx->stream, &ctx->prof);
+  launch_cloud_transform(c->pts, c->nrm, c->omg, c->eig_valid ? c->eig : nullptr, c->gauss_valid ? c->gauss : nullptr,
+                         c->count, c->capacity, (const float *)(ctx->ws + o), ctx->stream, &ctx->prof);
   CK(ctx, cudaGetLastError());
   return NICP_OK;
 }
@@ -507,7 +541,8 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     if (!fin[i].depth || fin[i].rows <= 0 || fin[i].cols <= 0 || !clouds[i] || !valid_camera(&cams[i]))
       return fail(ctx, NICP_EINVAL, "bad frame " + std::to_string(i));
     if ((long long)fin[i].rows * fin[i].cols > (1ll << 30)) return fail(ctx, NICP_EINVAL, "frame too large");
-    if ((rc = cloud_reserve(clouds[i], fin[i].rows * fin[i].cols, fin[i].rows, fin[i].cols, prm->keep_stats != 0)))
+    if ((rc = cloud_reserve(clouds[i], fin[i].rows * fin[i].cols, fin[i].rows, fin[i].cols, prm->keep_stats != 0,
+                            prm->keep_gaussians != 0)))
       return rc;
   }
   int i0 = 0;
@@ -587,6 +622,23 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.pim_thr = prm->pim_curvature_threshold;
       d.nim_thr = prm->nim_curvature_threshold;
       d.keep_stats = prm->keep_stats && cl->has_eig;
+      cl->eig_valid = d.keep_stats != 0;
+      {
+        float K[9];
+        cam_K(cam, K);
+        hm_inv3(K, d.iK);
+        d.fB = cam.baseline * K[0];
+        d.alpha = cam.alpha;
+      }
+      d.gauss = (prm->keep_gaussians && cl->has_gauss) ? cl->gauss : nullptr;
+      cl->gauss_valid = d.gauss != nullptr;
+      cl->omega_structured = prm->pim_flat[1] == prm->pim_flat[2] && prm->pim_nonflat[1] == prm->pim_nonflat[2] &&
+                             prm->nim_flat[1] == prm->nim_flat[2] && prm->nim_nonflat[1] == prm->nim_nonflat[2];
+      {
+        const float od[8] = {prm->pim_flat[0], prm->pim_flat[1], prm->pim_nonflat[0], prm->pim_nonflat[1],
+                             prm->nim_flat[0], prm->nim_flat[1], prm->nim_nonflat[0], prm->nim_nonflat[1]};
+        std::memcpy(cl->omd, od, sizeof(od));
+      }
       d.index = cl->index;
       d.pts = cl->pts;
       d.nrm = cl->nrm;
@@ -708,6 +760,7 @@ struct PairPlan {
   int n = 0;
   size_t o_extra = 0;
   bool keep_ref = false, list_mode = false;
+  bool structured = false;  // every current cloud has structured Omegas (k_corr_lin<true>)
   int total_tiles = 0, total_pt_tiles = 0;
   size_t o_pairs = 0, o_states = 0, o_krt = 0, o_guess = 0, o_roff = 0, o_zbuf = 0, zbuf_bytes = 0;
   std::vector<size_t> o_cur, o_ref, o_part, o_list, o_ltc, o_np;
@@ -777,6 +830,8 @@ static void fill_pairs(nicp_ctx *ctx, const PairPlan &pl, const nicp_camera *cam
     d.cur_nrm = c ? c->nrm : nullptr;
     d.cur_omg = c ? c->omg : nullptr;
     d.cur_count = c ? c->count : nullptr;
+    d.cur_structured = (c && c->omega_structured) ? 1 : 0;
+    if (c) std::memcpy(d.cur_omd, c->omd, sizeof(d.cur_omd));
     d.rows = cam_rows(cams[i]);
     d.cols = cam_cols(cams[i]);
     d.tile_base = tb;
@@ -867,7 +922,7 @@ extern "C" int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_c
   const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
   launch_lin_list(dpd, 1, pl.total_tiles, lin_params(*prm), std::max(1, parity_threads), 0,
                   (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
-  launch_solve(dpd, 1, 0.0f, 2, 0.0, 1, s, &ctx->prof);
+  launch_solve(dpd, 1, 0.0f, 2 | (prm->cross_block_f32 ? kSolveCrossF32 : 0), 0.0, 1, s, &ctx->prof);
   CK(ctx, cudaGetLastError());
   char *pd_host;
   if ((rc = pin_down(ctx, sizeof(PairState), &pd_host))) return rc;
@@ -968,6 +1023,7 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
   const nicp_align_params &p = *a.prm;
   int outer = p.outer_iterations, inner = p.inner_iterations;
   bool stats = p.compute_statistics != 0;
+  const int xb = a.lin->cross_block_f32 ? kSolveCrossF32 : 0;
   cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s);
   launch_init_pairs(dpd, pl.n, (const double *)(ctx->ws + pl.o_guess), (const double *)(ctx->ws + pl.o_roff), s,
                     &ctx->prof);
@@ -983,13 +1039,13 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
       launch_corr_list(dpd, pl.n, pl.total_tiles, cp, 1, nullptr, s, &ctx->prof);
       for (int k = 0; k < inner; k++) {
         launch_lin_list(dpd, pl.n, pl.total_tiles, lp, std::max(1, a.corr->parity_threads), 1, nullptr, s, &ctx->prof);
-        launch_solve(dpd, pl.n, p.lambda, (k == inner - 1) ? 1 : 0, p.early_exit_eps, 0, s, &ctx->prof);
+        launch_solve(dpd, pl.n, p.lambda, ((k == inner - 1) ? 1 : 0) | xb, p.early_exit_eps, 0, s, &ctx->prof);
       }
     } else {
       for (int k = 0; k < inner; k++) {
         int flags = (k == 0) ? (1 | 2 | (pl.keep_ref ? 4 : 0)) : 0;
-        launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, flags, s, &ctx->prof);
-        launch_solve(dpd, pl.n, p.lambda, (k == inner - 1) ? 1 : 0, p.early_exit_eps, 0, s, &ctx->prof);
+        launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, flags, pl.structured, s, &ctx->prof);
+        launch_solve(dpd, pl.n, p.lambda, ((k == inner - 1) ? 1 : 0) | xb, p.early_exit_eps, 0, s, &ctx->prof);
       }
     }
   }
@@ -999,8 +1055,8 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
     if (pl.list_mode)
       launch_lin_list(dpd, pl.n, pl.total_tiles, lp, std::max(1, a.corr->parity_threads), 2, nullptr, s, &ctx->prof);
     else
-      launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, 8, s, &ctx->prof);
-    launch_solve(dpd, pl.n, 0.0f, 4, 0.0, 1, s, &ctx->prof);
+      launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, 8, pl.structured, s, &ctx->prof);
+    launch_solve(dpd, pl.n, 0.0f, 4 | xb, 0.0, 1, s, &ctx->prof);
   }
 }
 
@@ -1011,6 +1067,7 @@ static std::string graph_key(nicp_ctx *ctx, const PairPlan &pl, const AlignCall 
   put(&pl.n, sizeof(int));
   put(&pl.keep_ref, 1);
   put(&pl.list_mode, 1);
+  put(&pl.structured, 1);
   put(&pl.total_tiles, sizeof(int));
   put(&pl.total_pt_tiles, sizeof(int));
   put(&pl.zbuf_bytes, sizeof(size_t));
@@ -1044,6 +1101,8 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
   PairPlan pl;
   int rc;
   if ((rc = plan_pairs(ctx, a.n, a.cams, big.data(), keep_ref, list_mode, pl))) return rc;
+  pl.structured = !list_mode;
+  for (int i = 0; i < a.n && pl.structured; i++) pl.structured = a.curs[i] && a.curs[i]->omega_structured;
   size_t up = sizeof(PairDev) * a.n + 48 * (size_t)a.n + 256 * (size_t)a.n;
   char *pin;
   if ((rc = pin_up(ctx, up, &pin))) return rc;

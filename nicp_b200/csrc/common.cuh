@@ -26,17 +26,21 @@ constexpr int kCorrThreads = 256;       // 4 pixels per thread
 constexpr int kUnprojTilePixels = 4096; // 16 pixels per thread, 256 threads
 constexpr int kStatsThreads = 256;
 constexpr int kPartialWords = 32;       // doubles per CTA partial (21 H + 6 b + chi2 + inliers + C + K + pad)
+constexpr int kSolveCrossF32 = 32;      // k_solve mode bit: FP32 sum of the tile partials
 constexpr int kZbufThreads = 256;
 constexpr int kZbufPointsPerThread = 4;
 constexpr int kPointsPerCta = kZbufThreads * kZbufPointsPerThread;  // z-buffer kernel tile
 
-// pts[i].w is 1 for a point with a non-zero normal and kNoNormalW otherwise
-// (the reference's Point has w = 1; downloads report 1).  The z-buffer key
-// carries this bit below the point index, (depth key << 32) | (i << 1) | bit,
+// pts[i].w is kNoNormalW for a point without a normal, and 1 + class for a
+// point with one, class = (point information matrix non-flat) + 2 (normal
+// information matrix non-flat) as the converter chose them (the reference's
+// Point has w = 1; downloads report 1).  The z-buffer key carries the
+// no-normal bit below the point index, (depth key << 32) | (i << 1) | bit,
 // which keeps the packed minimum ordered by (depth, index) exactly, and lets
 // the correspondence kernel reject a pixel whose point has no normal without
 // gathering it.
 constexpr float kNoNormalW = 0.5f;
+__host__ __device__ __forceinline__ bool point_has_normal(float w) { return w >= 1.0f; }
 
 // ---- per-frame descriptor for the cloud-build kernels
 struct FrameDev {
@@ -57,9 +61,12 @@ struct FrameDev {
   float pim_flat[3], pim_nonflat[3], pim_thr;
   float nim_flat[3], nim_nonflat[3], nim_thr;
   int keep_stats;
+  float iK[9];                // K^-1 (Gaussian Jacobian)
+  float fB, alpha;            // baseline * fx, depth noise coefficient
   // outputs
   int32_t *index;             // rows*cols
   float4 *pts, *nrm, *omg;
+  float4 *gauss;              // 3 float4 per point (mean xyz, 9 covariance entries) or null
   float *eig;
   int *count;                 // device: [0] number of points, [1] points with a normal
   // scratch
@@ -94,6 +101,13 @@ struct PairDev {
   const int *ref_count;
   const float4 *cur_pts, *cur_nrm, *cur_omg;
   const int *cur_count;
+  // The current cloud's information matrices have the converter's structure
+  // Omega = d1 I + (d0 - d1) n n^T (n its normal): the fused kernel rebuilds
+  // them from the normal and the class code in the point's w instead of
+  // gathering them.  cur_omd: (d0, d1) of point-flat, point-non-flat,
+  // normal-flat, normal-non-flat.
+  int cur_structured;
+  float cur_omd[8];
   int rows, cols;       // projection image (scaled)
   int tile_base;        // first pixel tile of this pair in the grid
   int pt_tile_base;     // first point tile (reference cloud) in the grid

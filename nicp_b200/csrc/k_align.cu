@@ -22,6 +22,8 @@
 //                72-100), early exit, and the float matrices of the next iteration.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include <algorithm>
 #include <mutex>
 
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(kZbufThreads)
     float d;
     if (i >= n || !project_pixel(K, p[k], pd.rows, pd.cols, pd.min_d, pd.max_d, x, y, d)) continue;
     unsigned long long key =
-        ((unsigned long long)float_key(d) << 32) | ((unsigned)i << 1) | (p[k].w != 1.0f ? 1u : 0u);
+        ((unsigned long long)float_key(d) << 32) | ((unsigned)i << 1) | (point_has_normal(p[k].w) ? 0u : 1u);
     atomicMin(pd.zbuf + (size_t)y * pd.cols + x, key);
   }
 }
@@ -213,6 +215,74 @@ __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12,
   acc.v[24] += ks * (u0 + w0); acc.v[25] += ks * (u1 + w1); acc.v[26] += ks * (u2 + w2);
 }
 
+// lin_terms for a current point whose information matrices have the
+// converter's structure Omega = d1 I + (d0 - d1) u u^T, u its normal (the
+// smallest-eigenvalue eigenvector; Omega = U diag(d0, d1, d1) U^T,
+// informationmatrixcalculator.cpp:9-57).  With S = skew(2 v) (S x = x cross 2v)
+// and w = S^T u:  Omega e = a e + b (u.e) u,  Omega S = a S + b u w^T,
+// S^T Omega S = a (|2v|^2 I - (2v)(2v)^T) + b w w^T.  The class code in the
+// point's w selects (d0, d1); omd holds them for the four classes.
+__device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const float *T12, const float *omd,
+                                                    float4 rp0, float4 rn0, float4 cpt, float4 cn, Acc &acc) {
+  float3 rp = xform_point(T12, rp0);
+  float3 rn = xform_normal(T12, rn0);
+  float alp = 0.0f, bep = 0.0f, aln = 0.0f, ben = 0.0f;
+  if (point_has_normal(cpt.w)) {
+    const int cls = (int)cpt.w - 1;
+    const float *dp = omd + 2 * (cls & 1), *dn = omd + 4 + 2 * ((cls >> 1) & 1);
+    alp = dp[1];
+    bep = dp[0] - dp[1];
+    aln = lp.scale * dn[1];
+    ben = lp.scale * dn[0] - aln;
+  }
+  if (lp.z_scaling) {
+    float f = 1.0f / fabsf(cpt.z);
+    alp *= f; bep *= f; aln *= f; ben *= f;
+  }
+  if (lp.demoted) { aln = 0.0f; ben = 0.0f; }
+  const float ux = cn.x, uy = cn.y, uz = cn.z;
+  float pe[3] = {rp.x - cpt.x, rp.y - cpt.y, rp.z - cpt.z};
+  float ne[3] = {rn.x - cn.x, rn.y - cn.y, rn.z - cn.z};
+  float up = ux * pe[0] + uy * pe[1] + uz * pe[2];
+  float un = ux * ne[0] + uy * ne[1] + uz * ne[2];
+  float ep[3] = {alp * pe[0] + bep * up * ux, alp * pe[1] + bep * up * uy, alp * pe[2] + bep * up * uz};
+  float en[3] = {aln * ne[0] + ben * un * ux, aln * ne[1] + ben * un * uy, aln * ne[2] + ben * un * uz};
+  float le = (pe[0] * ep[0] + pe[1] * ep[1] + pe[2] * ep[2]) + (ne[0] * en[0] + ne[1] * en[1] + ne[2] * en[2]);
+  float ks = 1.0f;
+  if (le > lp.max_chi2) {
+    if (lp.robust) ks = lp.max_chi2 / le;
+    else return;
+  }
+  acc.v[27] += ks * le;
+  acc.v[28] += 1.0f;
+  const float a = 2.0f * rp.x, b = 2.0f * rp.y, c = 2.0f * rp.z;
+  const float an = 2.0f * rn.x, bn = 2.0f * rn.y, cn2 = 2.0f * rn.z;
+  const float ka = ks * alp, kb = ks * bep, kan = ks * aln, kbn = ks * ben;
+  // Htt += ks Omega_p
+  const float t0 = kb * ux, t1 = kb * uy, t2 = kb * uz;
+  acc.v[0] += ka + t0 * ux; acc.v[1] += t0 * uy; acc.v[2] += ka + t1 * uy;
+  acc.v[3] += t0 * uz; acc.v[4] += t1 * uz; acc.v[5] += ka + t2 * uz;
+  // Htr += ks Omega_p S, S = [[0, c, -b], [-c, 0, a], [b, -a, 0]]
+  const float wp0 = -c * uy + b * uz, wp1 = c * ux - a * uz, wp2 = -b * ux + a * uy;
+  const float wn0 = -cn2 * uy + bn * uz, wn1 = cn2 * ux - an * uz, wn2 = -bn * ux + an * uy;
+  acc.v[6] += t0 * wp0;          acc.v[7] += ka * c + t0 * wp1;  acc.v[8] += -ka * b + t0 * wp2;
+  acc.v[9] += -ka * c + t1 * wp0; acc.v[10] += t1 * wp1;         acc.v[11] += ka * a + t1 * wp2;
+  acc.v[12] += ka * b + t2 * wp0; acc.v[13] += -ka * a + t2 * wp1; acc.v[14] += t2 * wp2;
+  // Hrr += ks (S^T Omega_p S + Sn^T Omega_n Sn)
+  const float ss = a * a + b * b + c * c, sn = an * an + bn * bn + cn2 * cn2;
+  acc.v[15] += ka * (ss - a * a) + kb * wp0 * wp0 + kan * (sn - an * an) + kbn * wn0 * wn0;
+  acc.v[16] += -ka * (b * a) + kb * wp1 * wp0 - kan * (bn * an) + kbn * wn1 * wn0;
+  acc.v[17] += ka * (ss - b * b) + kb * wp1 * wp1 + kan * (sn - bn * bn) + kbn * wn1 * wn1;
+  acc.v[18] += -ka * (c * a) + kb * wp2 * wp0 - kan * (cn2 * an) + kbn * wn2 * wn0;
+  acc.v[19] += -ka * (c * b) + kb * wp2 * wp1 - kan * (cn2 * bn) + kbn * wn2 * wn1;
+  acc.v[20] += ka * (ss - c * c) + kb * wp2 * wp2 + kan * (sn - cn2 * cn2) + kbn * wn2 * wn2;
+  // bt += ks ep; br += ks (S^T ep + Sn^T en)
+  acc.v[21] += ks * ep[0]; acc.v[22] += ks * ep[1]; acc.v[23] += ks * ep[2];
+  float u0 = b * ep[2] - c * ep[1], u1 = c * ep[0] - a * ep[2], u2 = a * ep[1] - b * ep[0];
+  float w0 = bn * en[2] - cn2 * en[1], w1 = cn2 * en[0] - an * en[2], w2 = an * en[1] - bn * en[0];
+  acc.v[24] += ks * (u0 + w0); acc.v[25] += ks * (u1 + w1); acc.v[26] += ks * (u2 + w2);
+}
+
 // Reduces every thread's Acc to one FP64 partial of the CTA (fixed order).
 __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) {
   __shared__ double wsum[kCorrThreads / 32][32];
@@ -259,12 +329,21 @@ constexpr int kCorrStages = 3;
 // Structure-of-arrays stage: thread t owns element t of every array, so a
 // warp's accesses to one field are consecutive 16-byte words (no bank
 // conflicts).
-struct GatherStage {
+struct GatherStageS {  // structured Omega: rebuilt from the current normal
   float4 rp[kCorrThreads], rn[kCorrThreads], cp[kCorrThreads], cn[kCorrThreads];
-  float4 o0[kCorrThreads], o1[kCorrThreads], o2[kCorrThreads];
-  int ri[kCorrThreads], ci[kCorrThreads], valid[kCorrThreads];
+  int valid[kCorrThreads];
 };
-constexpr int kCorrSmem = kCorrStages * (int)sizeof(GatherStage);
+struct GatherStageG : GatherStageS {  // general Omega: gathered for accepted pixels
+  float4 o0[kCorrThreads], o1[kCorrThreads], o2[kCorrThreads];
+  int ci[kCorrThreads];
+};
+#ifndef NICP_CORR_S_CTAS
+#define NICP_CORR_S_CTAS 3
+#endif
+template <bool kStructured>
+using GatherStage = typename std::conditional<kStructured, GatherStageS, GatherStageG>::type;
+template <bool kStructured>
+constexpr int corr_smem() { return kCorrStages * (int)sizeof(GatherStage<kStructured>); }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -279,27 +358,32 @@ __device__ __forceinline__ void cp_async_wait() {
 // flags: bit0 read the reference index from the z-buffer (else ref_index),
 // bit1 reset the z-buffer after reading, bit2 keep the resolved reference
 // index image, bit3 statistics pass (gate with Tgate_used; ignores `done`).
-__global__ void __launch_bounds__(kCorrThreads, 2)
+// kStructured: every pair's current cloud has structured information
+// matrices (no Omega gathers, smaller stages).
+template <bool kStructured>
+__global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS : 2)
     k_corr_lin(const PairDev *__restrict__ pairs, int npairs, int total_tiles, CorrParams cp, LinParams lp,
                int flags) {
-  extern __shared__ __align__(16) unsigned char corr_smem[];
-  GatherStage *stages = reinterpret_cast<GatherStage *>(corr_smem);
+  extern __shared__ __align__(16) unsigned char corr_smem_raw[];
+  using Stage = GatherStage<kStructured>;
+  Stage *stages = reinterpret_cast<Stage *>(corr_smem_raw);
   const int t = threadIdx.x;
   // per-tile constants for the two tiles the pipeline can span:
-  // [0..11] gating T, [12..23] linearizer T, then pair index and skip flag
-  __shared__ float sT[2][24];
-  __shared__ int sPair[2], sSkip[2];
+  // [0..11] gating T, [12..23] linearizer T, [24..31] the current cloud's
+  // Omega parameters, then pair index, skip flag and structured-Omega flag
+  __shared__ float sT[2][32];
+  __shared__ int sPair[2], sSkip[2], sStruct[2];
   const bool stats_pass = flags & 8;
   if ((int)blockIdx.x >= total_tiles) return;
   const int ntiles = (total_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   const int nsub = ntiles * kSubsPerTile;
   const bool drop_no_normal = !cp.demoted;
   auto tile_of = [&](int j) { return (int)blockIdx.x + (j / kSubsPerTile) * (int)gridDim.x; };
-  auto stage_of = [&](int j) -> GatherStage & { return stages[j % kCorrStages]; };
+  auto stage_of = [&](int j) -> Stage & { return stages[j % kCorrStages]; };
 
   // Tile -> pair lookups, cached per pipeline stage (a stage's tile changes
   // once every kSubsPerTile sub-tiles).
-  int lt_tile = -1, lt_pi = 0, gt_tile = -1, gt_pi = 0;
+  int lt_tile = -1, lt_pi = 0, gt_tile = -1, gt_pi = 0, gt_ctile = -1, gt_rc = 0, gt_cc = 0;
   bool lt_skip = false, gt_skip = false;
   auto lookup = [&](int tile, int &ctile, int &cpi, bool &cskip) {
     if (tile != ctile) {
@@ -332,7 +416,7 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
   // Phase G1 (two sub-tiles ahead): decode the indices, reset the z-buffer,
   // gather points and normals of both clouds.
   auto issue_g1 = [&](int j) {
-    GatherStage &g = stage_of(j);
+    Stage &g = stage_of(j);
     int ri = -1, ci = -1, valid = 0;
     if (j < nsub) {
       int tile = tile_of(j);
@@ -350,9 +434,14 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
             ri = cI;
             ci = (int)(unsigned)zI;
           }
-          int rmax = pd.rows;
-          if (cp.row_limit_threads > 1) rmax = (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
-          valid = ri >= 0 && ci >= 0 && ri < *pd.ref_count && ci < *pd.cur_count && p / pd.cols < rmax;
+          if (gt_ctile != tile) {  // point counts, read once per tile
+            gt_ctile = tile;
+            gt_rc = *pd.ref_count;
+            gt_cc = *pd.cur_count;
+          }
+          valid = ri >= 0 && ci >= 0 && ri < gt_rc && ci < gt_cc;
+          if (valid && cp.row_limit_threads > 1)
+            valid = p / pd.cols < (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
           if (valid) {
             cp_async16(&g.rp[t], pd.ref_pts + ri);
             cp_async16(&g.rn[t], pd.ref_nrm + ri);
@@ -362,8 +451,7 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
         }
       }
     }
-    g.ri[t] = ri;
-    g.ci[t] = ci;
+    if constexpr (!kStructured) g.ci[t] = ci;
     g.valid[t] = valid;
     cp_async_commit();
   };
@@ -378,25 +466,30 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
     if (threadIdx.x < 24)
       sT[e][threadIdx.x] = threadIdx.x < 12 ? (stats_pass ? st->Tgate_used : st->Tgate)[threadIdx.x]
                                             : st->Tlin[threadIdx.x - 12];
+    else if (threadIdx.x < 32)
+      sT[e][threadIdx.x] = pairs[pi].cur_omd[threadIdx.x - 24];
     if (threadIdx.x == 0) {
       sPair[e] = pi;
       sSkip[e] = st->done && !stats_pass;
+      sStruct[e] = pairs[pi].cur_structured;
     }
   };
 
   // Gate (one sub-tile ahead), then gather Omega only for accepted pairs.
   auto gate_g2 = [&](int j) {
     if (j < nsub) {
-      GatherStage &g = stage_of(j);
+      Stage &g = stage_of(j);
       int e = (j / kSubsPerTile) & 1;
       int acc_ok = 0;
       if (g.valid[t] && !sSkip[e]) {
         acc_ok = gate(cp, sT[e], g.rp[t], g.rn[t], g.cp[t], g.cn[t]) ? 2 : 1;
-        if (acc_ok == 2) {
-          const float4 *o = pairs[sPair[e]].cur_omg + 3 * (size_t)g.ci[t];
-          cp_async16(&g.o0[t], o);
-          cp_async16(&g.o1[t], o + 1);
-          cp_async16(&g.o2[t], o + 2);
+        if constexpr (!kStructured) {
+          if (acc_ok == 2 && !sStruct[e]) {
+            const float4 *o = pairs[sPair[e]].cur_omg + 3 * (size_t)g.ci[t];
+            cp_async16(&g.o0[t], o);
+            cp_async16(&g.o1[t], o + 1);
+            cp_async16(&g.o2[t], o + 2);
+          }
         }
       }
       g.valid[t] = acc_ok;  // 0 none, 1 candidate rejected, 2 accepted
@@ -433,12 +526,19 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
       for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
     }
     if (!sSkip[e]) {
-      const GatherStage &g = stage_of(j);
+      const Stage &g = stage_of(j);
       const int v = g.valid[t];
       if (v) acc.v[29] += 1.0f;
       if (v == 2) {
         acc.v[30] += 1.0f;
-        lin_terms(lp, sT[e] + 12, g.rp[t], g.rn[t], g.cp[t], g.cn[t], g.o0[t], g.o1[t], g.o2[t], acc);
+        if constexpr (kStructured) {
+          lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, g.rp[t], g.rn[t], g.cp[t], g.cn[t], acc);
+        } else {
+          if (sStruct[e])
+            lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, g.rp[t], g.rn[t], g.cp[t], g.cn[t], acc);
+          else
+            lin_terms(lp, sT[e] + 12, g.rp[t], g.rn[t], g.cp[t], g.cn[t], g.o0[t], g.o1[t], g.o2[t], acc);
+        }
       }
       if (sub == kSubsPerTile - 1) {
         const PairDev &pd = pairs[sPair[e]];
@@ -627,7 +727,7 @@ __global__ void k_init_pairs(const PairDev *__restrict__ pairs, int npairs, cons
 
 // mode: bit0 last inner iteration of the outer loop, bit1 reduce only (no
 // pose update: Linearizer results of a list pass), bit2 statistics pass
-// (reduce into Hstat only).
+// (reduce into Hstat only), kSolveCrossF32 sum the tile partials in FP32.
 __global__ void __launch_bounds__(128) k_solve(const PairDev *__restrict__ pairs, int npairs, float lambda, int mode,
                                               double early_eps, int ignore_done) {
   __shared__ double part[4][32];
@@ -638,11 +738,21 @@ __global__ void __launch_bounds__(128) k_solve(const PairDev *__restrict__ pairs
   int P = pd.rows * pd.cols;
   int nt = (P + kCorrTilePixels - 1) / kCorrTilePixels;
   int e = threadIdx.x & 31, g = threadIdx.x >> 5;
-  double s = 0.0;
-  for (int t = g; t < nt; t += 4) s += pd.partials[(size_t)t * kPartialWords + e];
-  part[g][e] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) tot[e] = ((part[0][e] + part[1][e]) + part[2][e]) + part[3][e];
+  if (mode & kSolveCrossF32) {
+    // precision study: the same fixed order, in FP32
+    float s = 0.0f;
+    for (int t = g; t < nt; t += 4) s += (float)pd.partials[(size_t)t * kPartialWords + e];
+    part[g][e] = (double)s;
+    __syncthreads();
+    if (threadIdx.x < 32)
+      tot[e] = (double)((((float)part[0][e] + (float)part[1][e]) + (float)part[2][e]) + (float)part[3][e]);
+  } else {
+    double s = 0.0;
+    for (int t = g; t < nt; t += 4) s += pd.partials[(size_t)t * kPartialWords + e];
+    part[g][e] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) tot[e] = ((part[0][e] + part[1][e]) + part[2][e]) + part[3][e];
+  }
   __syncthreads();
   if (threadIdx.x != 0) return;
   const int li[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
@@ -718,25 +828,33 @@ void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_
 
 // Persistent grid: as many CTAs as fit on the device at once, never more
 // than there are tiles.
+template <bool kStructured>
 static int corr_lin_grid(int total_tiles) {
   static int resident = 0;
   if (!resident) {
-    cudaFuncSetAttribute(k_corr_lin, cudaFuncAttributeMaxDynamicSharedMemorySize, kCorrSmem);
+    cudaFuncSetAttribute(k_corr_lin<kStructured>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         corr_smem<kStructured>());
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lin, kCorrThreads, kCorrSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lin<kStructured>, kCorrThreads,
+                                                  corr_smem<kStructured>());
     resident = std::max(1, sms * std::max(1, per_sm));
   }
   return std::min(total_tiles, resident);
 }
 
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
-                     int flags, cudaStream_t s, Profiler *prof) {
+                     int flags, bool structured, cudaStream_t s, Profiler *prof) {
   if (total_tiles <= 0) return;
-  int grid = corr_lin_grid(total_tiles);
   prof->begin(NICP_K_CORR_LIN, s);
-  k_corr_lin<<<grid, kCorrThreads, kCorrSmem, s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
+  if (structured) {
+    int grid = corr_lin_grid<true>(total_tiles);
+    k_corr_lin<true><<<grid, kCorrThreads, corr_smem<true>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
+  } else {
+    int grid = corr_lin_grid<false>(total_tiles);
+    k_corr_lin<false><<<grid, kCorrThreads, corr_smem<false>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
+  }
   prof->end(NICP_K_CORR_LIN, s);
 }
 

@@ -118,6 +118,41 @@ __global__ void __launch_bounds__(256) k_unproject_count(const FrameDev *__restr
   if (tile == 0 && threadIdx.x == 0) f.count[1] = 0;  // points with a normal, counted by k_stats
 }
 
+// Gaussian3f of an unprojected pixel (pinholepointprojector.cpp:93-134):
+// zVariation = (alpha z z) / (fB + z alpha), J = K^-1 [[z,0,c],[0,z,r],[0,0,1]],
+// covariance = J diag(3, 3, zVariation) J^T, every product and sum in the
+// order written, single rounding each.  All nine entries are kept: entry
+// (i, j) is sum_k (J_ik D_k) J_jk, which differs from (j, i) in the last bit,
+// as in the reference's product.  Stored as (mean, c00), (c01, c02, c10,
+// c11), (c12, c20, c21, c22).
+__device__ __forceinline__ void write_gaussian(const FrameDev &f, float4 *g, float4 pt, int c, int r, float z) {
+  float zv = __fdiv_rn(fm(fm(f.alpha, z), z), fa(f.fB, fm(z, f.alpha)));
+  const float J[9] = {z, 0.0f, (float)c, 0.0f, z, (float)r, 0.0f, 0.0f, 1.0f};
+  float IJ[9];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      IJ[i * 3 + j] = fa(fa(fm(f.iK[i * 3 + 0], J[0 * 3 + j]), fm(f.iK[i * 3 + 1], J[1 * 3 + j])),
+                         fm(f.iK[i * 3 + 2], J[2 * 3 + j]));
+  const float D[3] = {3.0f, 3.0f, zv};
+  float UD[9];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) UD[i * 3 + k] = fm(IJ[i * 3 + k], D[k]);
+  float C[9];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      C[i * 3 + j] = fa(fa(fm(UD[i * 3 + 0], IJ[j * 3 + 0]), fm(UD[i * 3 + 1], IJ[j * 3 + 1])),
+                        fm(UD[i * 3 + 2], IJ[j * 3 + 2]));
+  g[0] = make_float4(pt.x, pt.y, pt.z, C[0]);
+  g[1] = make_float4(C[1], C[2], C[3], C[4]);
+  g[2] = make_float4(C[5], C[6], C[7], C[8]);
+}
+
 __global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restrict__ frames, int nframes) {
   __shared__ int red[32];
   __shared__ int wsum[8];
@@ -159,7 +194,9 @@ __global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restr
     if (mask & (1u << k)) {
       int p = pix0 + k;
       int r = p / f.cols, c = p - r * f.cols;
-      f.pts[idx] = unproject_pixel(f.iKRt, c, r, d[k]);
+      float4 pt = unproject_pixel(f.iKRt, c, r, d[k]);
+      f.pts[idx] = pt;
+      if (f.gauss) write_gaussian(f, f.gauss + 3 * (size_t)idx, pt, c, r, d[k]);
       out[k] = idx++;
     }
   }
@@ -376,6 +413,7 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
   double lam[3] = {0, 0, 0};
   double U[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   bool reached = false;
+  int omega_class = 0;
   int rad = interval_radius(f.K, d, f.min_d, f.max_d, f.world_radius);
   if (rad >= 0 && rad >= f.min_radius) {
     if (rad > f.max_radius) rad = f.max_radius;
@@ -421,6 +459,7 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
           Dp[k] = (kappa < (double)f.pim_thr) ? f.pim_flat[k] : f.pim_nonflat[k];
           Dn[k] = (kappa < (double)f.nim_thr) ? f.nim_flat[k] : f.nim_nonflat[k];
         }
+        omega_class = (kappa < (double)f.pim_thr ? 0 : 1) + (kappa < (double)f.nim_thr ? 0 : 2);
         const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
         for (int e = 0; e < 6; e++) {
@@ -446,9 +485,10 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
     const unsigned m = __ballot_sync(act, has);
     if ((threadIdx.x & 31) == (unsigned)(__ffs(act) - 1) && m) atomicAdd(f.count + 1, __popc(m));
   }
-  // the point's w carries "has a normal" for the z-buffer key (see kNoNormalW)
+  // the point's w carries "has a normal" and the information-matrix class
+  // (see kNoNormalW)
   reinterpret_cast<float *>(f.pts + idx)[3] =
-      (nout.x != 0.0f || nout.y != 0.0f || nout.z != 0.0f) ? 1.0f : kNoNormalW;
+      (nout.x != 0.0f || nout.y != 0.0f || nout.z != 0.0f) ? 1.0f + (float)omega_class : kNoNormalW;
   float4 *o = f.omg + 3 * (size_t)idx;
   o[0] = make_float4(om[0], om[1], om[2], om[3]);
   o[1] = make_float4(om[4], om[5], om[6], om[7]);
@@ -463,8 +503,8 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
 }
 
 // ------------------------------------------------------------ transform
-__global__ void k_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, const int *count, int capacity,
-                                  const float *__restrict__ m12) {
+__global__ void k_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,
+                                  int capacity, const float *__restrict__ m12) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= capacity || i >= *count) return;
   float A[12];
@@ -497,6 +537,26 @@ __global__ void k_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *
   omg[3 * i] = make_float4(res[0][0], res[0][1], res[0][2], res[0][3]);
   omg[3 * i + 1] = make_float4(res[0][4], res[0][5], res[1][0], res[1][1]);
   omg[3 * i + 2] = make_float4(res[1][2], res[1][3], res[1][4], res[1][5]);
+  if (gauss) {
+    // Gaussian3fVector::transformInPlace (gaussian3.h:66-73): mean' = R mean + t,
+    // covariance' = (R C) R^T
+    float4 g0 = gauss[3 * i], g1 = gauss[3 * i + 1], g2 = gauss[3 * i + 2];
+    float C[9] = {g0.w, g1.x, g1.y, g1.z, g1.w, g2.x, g2.y, g2.z, g2.w};
+    float m[3] = {g0.x, g0.y, g0.z}, mo[3];
+    for (int a = 0; a < 3; a++)
+      mo[a] = fa(fa(fa(fm(R[a * 3 + 0], m[0]), fm(R[a * 3 + 1], m[1])), fm(R[a * 3 + 2], m[2])), A[a * 4 + 3]);
+    float RC[9], Co[9];
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++)
+        RC[a * 3 + b] = fa(fa(fm(R[a * 3 + 0], C[0 * 3 + b]), fm(R[a * 3 + 1], C[1 * 3 + b])), fm(R[a * 3 + 2], C[2 * 3 + b]));
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++)
+        Co[a * 3 + b] =
+            fa(fa(fm(RC[a * 3 + 0], R[b * 3 + 0]), fm(RC[a * 3 + 1], R[b * 3 + 1])), fm(RC[a * 3 + 2], R[b * 3 + 2]));
+    gauss[3 * i] = make_float4(mo[0], mo[1], mo[2], Co[0]);
+    gauss[3 * i + 1] = make_float4(Co[1], Co[2], Co[3], Co[4]);
+    gauss[3 * i + 2] = make_float4(Co[5], Co[6], Co[7], Co[8]);
+  }
   if (eig) {
     float *e = eig + 12 * (size_t)i;
     float U[9];
@@ -555,11 +615,11 @@ void launch_stats(int precision, const FrameDev *d_frames, int nframes, int tota
   prof->end(NICP_K_STATS, s);
 }
 
-void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, const int *count, int capacity,
-                            const float *d_m12, cudaStream_t s, Profiler *prof) {
+void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,
+                            int capacity, const float *d_m12, cudaStream_t s, Profiler *prof) {
   prof->begin(NICP_K_TRANSFORM, s);
   int blocks = (capacity + 255) / 256;
-  if (blocks > 0) k_cloud_transform<<<blocks, 256, 0, s>>>(pts, nrm, omg, eig, count, capacity, d_m12);
+  if (blocks > 0) k_cloud_transform<<<blocks, 256, 0, s>>>(pts, nrm, omg, eig, gauss, count, capacity, d_m12);
   prof->end(NICP_K_TRANSFORM, s);
 }
 

@@ -65,8 +65,8 @@ void launch_moments(int precision, const FrameDev *d_frames, int nframes, int to
                     cudaStream_t s, Profiler *prof);
 void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s,
                   Profiler *prof);
-void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, const int *count, int capacity,
-                            const float *d_m12, cudaStream_t s, Profiler *prof);
+void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,
+                            int capacity, const float *d_m12, cudaStream_t s, Profiler *prof);
 size_t moment_bytes(int precision);
 void launch_intervals(const float *d_depth, int P, const float *d_K9, float min_d, float max_d, float R, int32_t *d_out,
                       cudaStream_t s, Profiler *prof);
@@ -81,7 +81,7 @@ void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int 
 void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out,
                     int drop_no_normal, cudaStream_t s, Profiler *prof);
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
-                     int flags, cudaStream_t s, Profiler *prof);
+                     int flags, bool structured, cudaStream_t s, Profiler *prof);
 void launch_corr_list(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, int use_state_T,
                       const float *explicit_T, cudaStream_t s, Profiler *prof);
 void launch_lin_list(const PairDev *d_pairs, int npairs, int total_tiles, const LinParams &lp, int parity_threads,

@@ -367,13 +367,14 @@ template <class S> struct Cloud {
   std::vector<S> eigval, eigvec;   // Stats eigenvalues (3) / eigenvectors (9)
   std::vector<S> omega_p, omega_n; // 3x3 blocks of the InformationMatrix
   std::vector<S> gauss_cov;        // Gaussian3f covariance (9)
+  std::vector<S> gauss_mean;       // Gaussian3f mean (3)
   std::vector<int> stats_n;
   void resize(int k) {
     n = k;
     points.resize(k); normals.resize(k); curvature.assign(k, S(0));
     eigval.assign(3 * k, S(0)); eigvec.assign(9 * k, S(0));
     omega_p.assign(9 * k, S(0)); omega_n.assign(9 * k, S(0));
-    gauss_cov.assign(9 * k, S(0)); stats_n.assign(k, 0);
+    gauss_cov.assign(9 * k, S(0)); gauss_mean.assign(3 * k, S(0)); stats_n.assign(k, 0);
   }
 };
 
@@ -584,6 +585,9 @@ static Cloud<S> *build_cloud(const uint16_t *depth, int rows, int cols, const or
   cl->resize(count);
   cl->points = pts;
   cl->gauss_cov = gcov;
+  cl->gauss_mean.resize(3 * (size_t)count);
+  for (int i = 0; i < count; i++)
+    for (int k = 0; k < 3; k++) cl->gauss_mean[3 * (size_t)i + k] = pts[i][k];
   // default Stats: identity eigenvectors, zero eigenvalues, curvature 0
   for (int i = 0; i < count; i++) {
     cl->normals[i] = V4<S>{{S(0), S(0), S(0), S(0)}};
@@ -666,6 +670,31 @@ static Cloud<S> *build_cloud(const uint16_t *depth, int rows, int cols, const or
         M4<S> RU = mm(m, U);
         for (int a = 0; a < 3; a++)
           for (int b = 0; b < 3; b++) cl->eigvec[9 * i + a * 3 + b] = RU(a, b);
+        // Gaussian3fVector::transformInPlace (gaussian3.h:66-73):
+        // mean' = R mean + t, covariance' = (R C) R^T
+        {
+          S *gm = &cl->gauss_mean[3 * (size_t)i], *gc = &cl->gauss_cov[9 * (size_t)i];
+          S mo[3], RC[9];
+          for (int a = 0; a < 3; a++) {
+            S v = m(a, 0) * gm[0];
+            v = v + m(a, 1) * gm[1];
+            v = v + m(a, 2) * gm[2];
+            mo[a] = v + m(a, 3);
+          }
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+              S v = m(a, 0) * gc[0 * 3 + b];
+              v = v + m(a, 1) * gc[1 * 3 + b];
+              RC[a * 3 + b] = v + m(a, 2) * gc[2 * 3 + b];
+            }
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+              S v = RC[a * 3 + 0] * m(b, 0);
+              v = v + RC[a * 3 + 1] * m(b, 1);
+              gc[a * 3 + b] = v + RC[a * 3 + 2] * m(b, 2);
+            }
+          for (int k = 0; k < 3; k++) gm[k] = mo[k];
+        }
         for (int which = 0; which < 2; which++) {
           S *om = which ? &cl->omega_n[9 * i] : &cl->omega_p[9 * i];
           M4<S> O = M4<S>::zero();
@@ -1148,6 +1177,7 @@ template <class S> static int cloud_get(const Cloud<S> &c, int field, double *ou
     case 6: for (int i = 0; i < 9 * n; i++) out[i] = c.eigvec[i]; return 9 * n;
     case 7: for (int i = 0; i < n; i++) out[i] = c.stats_n[i]; return n;
     case 8: for (int i = 0; i < 9 * n && i < (int)c.gauss_cov.size(); i++) out[i] = c.gauss_cov[i]; return 9 * n;
+    case 9: for (int i = 0; i < 3 * n && i < (int)c.gauss_mean.size(); i++) out[i] = c.gauss_mean[i]; return 3 * n;
   }
   return -1;
 }

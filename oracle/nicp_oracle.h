@@ -94,7 +94,7 @@ void orc_cloud_free(orc_cloud *c);
 int orc_cloud_size(const orc_cloud *c);
 /* field: 0 points(4n) 1 normals(4n) 2 curvature(n) 3 omega_p(9n) 4 omega_n(9n)
  *        5 eigenvalues(3n) 6 eigenvectors(9n, row-major 3x3, columns = vectors)
- *        7 stats_n(n) 8 gaussian covariance (9n) */
+ *        7 stats_n(n) 8 gaussian covariance (9n) 9 gaussian mean (3n) */
 int orc_cloud_get(const orc_cloud *c, int field, double *out);
 
 /* PinholePointProjector::_updateMatrices outputs for transform T. */

@@ -154,7 +154,8 @@ def align_params(**kw):
 
 class Cloud:
     FIELDS = {"points": (0, 4), "normals": (1, 4), "curvature": (2, 1), "omega_p": (3, 9), "omega_n": (4, 9),
-              "eigenvalues": (5, 3), "eigenvectors": (6, 9), "stats_n": (7, 1), "gaussian_cov": (8, 9)}
+              "eigenvalues": (5, 3), "eigenvectors": (6, 9), "stats_n": (7, 1), "gaussian_cov": (8, 9),
+              "gaussian_mean": (9, 3)}
 
     def __init__(self, handle, mode):
         self.h = handle

@@ -310,6 +310,37 @@ def test_build_batch_equals_single(ctx):
             assert np.array_equal(s[k], d[k]), k
 
 
+@pytest.mark.parametrize("offset", [False, True], ids=["identity", "sensor_offset"])
+def test_gaussians(ctx, pair, offset):
+    """unProject's Gaussian3f per point (pinholepointprojector.cpp:93-134),
+    moved by a sensor offset like Gaussian3fVector::transformInPlace
+    (gaussian3.h:66-73): bit-exact against the REF32 oracle (same operation
+    order, single rounding per operation) and within 1e-5 relative of the FP64
+    oracle."""
+    S = perturb(9, 3.0, 0.1).astype(np.float32) if offset else None
+    proj, conv = converter(pair["cam"], ctx)
+    conv.keepGaussians = True
+    c = api.Cloud(ctx)
+    conv.compute(c, pair["d1"], sensorOffset=S)
+    mean, cov = c.gaussians()
+    pc, oc = cams(pair["cam"])
+    So = None if S is None else S.astype(np.float64)
+    ref32, _ = O.build_cloud(O.REF32, pair["d1"], oc, sensor_offset=So)
+    n = len(ref32)
+    assert mean.shape == (n, 3)
+    assert np.array_equal(mean, ref32.get("gaussian_mean").reshape(n, 3).astype(np.float32))
+    assert np.array_equal(cov.reshape(n, 9), ref32.get("gaussian_cov").reshape(n, 9).astype(np.float32))
+    f64, _ = O.build_cloud(O.F64, pair["d1"], oc, sensor_offset=So)
+    gc = f64.get("gaussian_cov").reshape(n, 9)
+    scale = np.max(np.abs(gc), axis=1, keepdims=True)
+    assert np.max(np.abs(cov.reshape(n, 9) - gc) / scale) < 1e-5
+    assert np.max(np.abs(mean - f64.get("gaussian_mean").reshape(n, 3))) < 1e-5
+    # the plain build keeps no Gaussians and says so
+    plain, _ = gpu_cloud(ctx, converter(pair["cam"], ctx)[1], pair["d1"], keep_index=False)
+    with pytest.raises(L.NicpError):
+        plain.gaussians()
+
+
 def test_sensor_offset(ctx, pair):
     """A non-identity sensor offset transforms the built cloud
     (Cloud::transformInPlace, cloud.cpp:191-204) like the REF32 oracle."""

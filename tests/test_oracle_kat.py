@@ -266,3 +266,25 @@ def test_thread_partition_drops(pair640):
         rel = np.linalg.norm(H - Hf) / np.linalg.norm(Hf)
         rel1 = np.linalg.norm(Hd - Hf) / np.linalg.norm(Hf)
         assert rel < 1e-2 and rel1 < 1e-2, (rel, rel1)
+
+
+def test_unprojection_gaussian_analytic():
+    """Gaussian3f of unProject (pinholepointprojector.cpp:93-134): with
+    K^-1 [[z,0,c],[0,z,r],[0,0,1]] = [[z/f,0,(c-cx)/f],[0,z/f,(r-cy)/f],[0,0,1]]
+    the covariance is that matrix times diag(3, 3, a z^2/(f B + a z)) times
+    its transpose; the mean is the point."""
+    cam = synth.camera_dict("160x120")
+    d = np.full((cam["rows"], cam["cols"]), 2500, np.uint16)
+    oc = O.camera(cam["rows"], cam["cols"], cam["fx"], cam["fy"], cam["cx"], cam["cy"])
+    cl, idx = O.build_cloud(O.F64, d, oc)
+    cov = cl.get("gaussian_cov").reshape(-1, 3, 3)
+    mean = cl.get("gaussian_mean").reshape(-1, 3)
+    z = np.float64(np.float32(0.001)) * 2500
+    f, B, a = cam["fx"], 0.075, np.float64(np.float32(0.1))
+    for r, c in [(0, 0), (37, 101), (119, 159)]:
+        k = idx[r, c]
+        J = np.array([[z / f, 0, (c - cam["cx"]) / f], [0, z / f, (r - cam["cy"]) / f], [0, 0, 1.0]])
+        zv = a * z * z / (f * np.float64(np.float32(B)) + z * a)
+        exp = J @ np.diag([3.0, 3.0, zv]) @ J.T
+        assert np.allclose(cov[k], exp, rtol=1e-9, atol=1e-15), (r, c)
+        assert np.array_equal(mean[k], cl.get("points").reshape(-1, 4)[k, :3])
