@@ -53,6 +53,23 @@ def measured_peak_gbs():
         return HBM_FALLBACK, "fallback"
 
 
+def max_over_ranks_of(dist, x):
+    """The slowest rank's time: every rank gets the maximum of x (gloo
+    all-reduce over host tensors; `dist` is torch.distributed or None)."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, units_per_rank, steps, ms_max):
+    """Whole-job throughput of `world` replicas: the units every rank
+    processed, divided by the slowest rank's time."""
+    return world * units_per_rank * steps / (ms_max / 1e3)
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """Samples nvidia-smi clocks and throttle reasons during the timed region."""
@@ -560,11 +577,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(dist, x)
 
     for _ in range(args.warmup):
         step_dev()
@@ -588,7 +601,7 @@ def main():
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     ms = max_over_ranks(ms)
-    value = world * npairs * args.steps / (ms / 1e3)
+    value = replica_value(world, npairs, args.steps, ms)
 
     # ---- e2e: pinned host frames through the C ABI, results back to the host
     for _ in range(2):
@@ -606,7 +619,7 @@ def main():
     barrier()
     h1, d1 = ctx.transfer_bytes()
     ms_e2e = max_over_ranks(e2.elapsed_time(e3))
-    e2e = world * npairs * args.steps / (ms_e2e / 1e3)
+    e2e = replica_value(world, npairs, args.steps, ms_e2e)
 
     # ---- accuracy against the synthetic ground truth (median over pairs)
     from nicp_b200 import synth
