@@ -128,9 +128,9 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ workload
-def make_workload(seed, frames, cam_name="640x480"):
+def make_workload(seed, frames, cam_name="640x480", period=None):
     from nicp_b200 import synth
-    imgs, poses, cam = synth.render_sequence(seed, cam_name, n_frames=frames)
+    imgs, poses, cam = synth.render_sequence(seed, cam_name, n_frames=frames, period=period)
     return np.stack(imgs), poses, cam
 
 
@@ -185,6 +185,21 @@ def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     return 0
 
 
+def measured_traffic(kernel, units):
+    """DRAM bytes of one launch of `kernel` processing `units` pairs or
+    frames, from the committed ncu summary (None if it has no entry)."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_640x480_seq.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 3 and not line.startswith("#") and parts[0] == kernel:
+                    return float(parts[2]) * units[parts[1]]
+    except OSError:
+        pass
+    return None
+
+
 def profile_step(ctx, run):
     """Per-kernel device time of one step (CUDA events on the library stream)."""
     from nicp_b200 import _lib as L
@@ -228,7 +243,8 @@ def cpu_baseline(frames, cam, seconds=15.0, threads=None):
 def reference_arm(args, rank, world):
     if rank != 0:
         return 0
-    frames, poses, cam = make_workload(args.seed, min(args.frames, 40))
+    # the first 40 frames of the same trajectory (same per-frame motion)
+    frames, poses, cam = make_workload(args.seed, min(args.frames, 40), period=args.period or args.frames)
     for _ in range(max(0, args.warmup)):
         cpu_baseline(frames[:3], cam, seconds=0.0)
     vals, total_pairs, total_t = [], 0, 0.0
@@ -519,6 +535,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--frames", type=int, default=200)
+    ap.add_argument("--period", type=int, default=None,
+                    help="trajectory loop length in frames (default: --frames); a short run with --period 200 "
+                         "has the per-frame motion of the 200-frame workload (small profiling cases)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -551,7 +570,7 @@ def main():
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream(device=local)
     ctx = api.Context(local, stream.cuda_stream)
-    frames, poses, cam = make_workload(args.seed + 7919 * rank, args.frames)
+    frames, poses, cam = make_workload(args.seed + 7919 * rank, args.frames, period=args.period)
     F = len(frames)
     npairs = F - 1
     proj, conv, corr, lin, prm = gpu_objects(ctx, cam)
@@ -649,7 +668,9 @@ def main():
     }.get(top, 0.0)
     achieved = per_launch_bytes / (top_ms / top_n / 1e3) / 1e9
     roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": measured_traffic(top, {"pair": npairs, "frame": F}),
+            "traffic_source": "profiles/dram_traffic_640x480_seq.txt (ncu, 19-pair case scaled per pair/frame)",
             "bytes_per_launch": per_launch_bytes, "avg_launch_ms": top_ms / top_n,
             "shares": {k: round(v[0] / total, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}}
 
