@@ -318,6 +318,10 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
         api.build_batch(ctx, dptrs, fcams, prm_c, clouds, on_device=True)
         return api.align_batch(ctx, clouds[0::2], clouds[1::2], cams, None, corr, lin, p)
 
+    # the autotuner picks launch shapes for this resolution mix on the first
+    # (warm-up) call; results do not depend on them
+    ctx.set_autotune(True)
+
     def timed(p):
         for _ in range(warmup):
             step(p)
@@ -332,6 +336,7 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
         return e0.elapsed_time(e1) / steps, res
 
     ms, res = timed(prm)
+    shape = ctx.launch_shape()
     prm_fixed = L.AlignParams.from_buffer_copy(prm)
     prm_fixed.early_exit_eps = 0.0
     ms_fixed, res_fixed = timed(prm_fixed)
@@ -362,6 +367,7 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
         pl.append(plain_pairs / (time.perf_counter() - t0))
     plain = max(pl)
     value = npairs / (ms / 1e3)
+    ctx.set_autotune(False)
     del clouds
     return {"workload": "%d independent pairs, resolutions uniform over %s, offsets 0.5-5 deg / 1-8 cm, "
                         "<= 20 outer x 2 inner, early exit at pose change < 1e-6" % (npairs, "/".join(MIXED_CAMS)),
@@ -373,7 +379,9 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
             "pose_err_vs_truth_median": {"rad": float(np.median([e[0] for e in errs])),
                                          "m": float(np.median([e[1] for e in errs]))},
             "resolution_counts": {n: names.count(n) for n in MIXED_CAMS},
-            "kernel_shares_and_launches": shares, "profiled_step_ms": total}
+            "kernel_shares_and_launches": shares, "profiled_step_ms": total,
+            "autotuned_launch_shape": {"zbuffer_points_per_thread": shape[0],
+                                       "corr_lin_ctas_per_sm": shape[1] or "all that fit"}}
 
 
 # ------------------------------------------------------------------ serving leg

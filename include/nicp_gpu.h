@@ -178,6 +178,19 @@ enum {
   NICP_K_SOLVE, NICP_K_TRANSFORM, NICP_K_COUNT
 };
 int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable);
+
+/* Autotuner (no reference counterpart).  When enabled, the first alignment
+ * call with a new resolution mix (the multiset of pair image sizes, with the
+ * iteration counts) times the Gauss-Newton loop with each candidate launch
+ * shape -- z-buffer points per thread 1/2/4/8, fused correspondence +
+ * linearizer CTAs per SM 1/2/as many as fit -- and keeps the fastest for
+ * that mix.  Results do not depend on the launch shape (bitwise).  The
+ * trials run on the context stream before the call's own loop. */
+int nicp_ctx_set_autotune(nicp_ctx *ctx, int enable);
+/* Launch shape used by the last alignment call (corr_ctas_per_sm 0 = as many
+ * as fit) and the number of resolution mixes tuned so far. */
+int nicp_ctx_launch_shape(const nicp_ctx *ctx, int *zbuffer_points_per_thread, int *corr_ctas_per_sm,
+                          int *tuned_mixes);
 /* Kernels this context has launched so far (graph replays included). */
 unsigned long long nicp_ctx_kernel_launches(const nicp_ctx *ctx);
 /* Host->device and device->host bytes the context has copied so far. */

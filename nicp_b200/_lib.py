@@ -96,6 +96,8 @@ SIGNATURES = {
     "nicp_ctx_device_bytes": (C.c_size_t, [P]),
     "nicp_ctx_set_profiling": (C.c_int, [P, C.c_int]),
     "nicp_ctx_kernel_launches": (C.c_ulonglong, [P]),
+    "nicp_ctx_set_autotune": (C.c_int, [P, C.c_int]),
+    "nicp_ctx_launch_shape": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "nicp_ctx_transfer_bytes": (C.c_int, [P, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
     "nicp_ctx_read_profile": (C.c_int, [P, C.c_int, f64p, C.POINTER(C.c_int)]),
     "nicp_kernel_name": (C.c_char_p, [C.c_int]),

@@ -67,6 +67,17 @@ class Context:
     def set_profiling(self, on):
         self.check(self.lib.nicp_ctx_set_profiling(self.h, 1 if on else 0))
 
+    def set_autotune(self, on):
+        """Per resolution mix, pick the fastest launch shapes on first use."""
+        self.check(self.lib.nicp_ctx_set_autotune(self.h, 1 if on else 0))
+
+    def launch_shape(self):
+        """(z-buffer points per thread, fused-kernel CTAs per SM (0 = all that
+        fit), resolution mixes tuned) of the last alignment call."""
+        a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        self.check(self.lib.nicp_ctx_launch_shape(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def read_profile(self, kernel):
         ms = C.c_double(0)
         n = C.c_int(0)

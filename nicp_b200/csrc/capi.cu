@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -59,6 +60,16 @@ struct nicp_ctx {
   std::vector<GraphEntry> graphs;
   nicp_cloud *scratch_cloud = nullptr;
   unsigned long long h2d_bytes = 0, d2h_bytes = 0;  // host<->device traffic issued by the library
+  // launch shapes of the alignment loop; the autotuner picks them per
+  // resolution mix (results do not depend on them)
+  struct Launch {
+    int zb_ppt = kZbufDefaultPPT;  // z-buffer points per thread
+    int corr_ctas = 0;             // fused kernel CTAs per SM (0: as many as fit)
+  };
+  Launch launch;
+  bool autotune = false;
+  std::map<std::string, Launch> tuned;
+  std::map<std::string, std::vector<float>> tune_ms;  // trial times per resolution mix
 };
 
 struct nicp_cloud {
@@ -335,6 +346,21 @@ extern "C" int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable) {
   ctx->prof.enabled = enable != 0;
   ctx->prof.recs.clear();
   ctx->prof.next = 0;
+  return NICP_OK;
+}
+
+extern "C" int nicp_ctx_set_autotune(nicp_ctx *ctx, int enable) {
+  if (!ctx) return NICP_EINVAL;
+  ctx->autotune = enable != 0;
+  return NICP_OK;
+}
+
+extern "C" int nicp_ctx_launch_shape(const nicp_ctx *ctx, int *zbuffer_points_per_thread, int *corr_ctas_per_sm,
+                                     int *tuned_mixes) {
+  if (!ctx) return NICP_EINVAL;
+  if (zbuffer_points_per_thread) *zbuffer_points_per_thread = ctx->launch.zb_ppt;
+  if (corr_ctas_per_sm) *corr_ctas_per_sm = ctx->launch.corr_ctas;
+  if (tuned_mixes) *tuned_mixes = (int)ctx->tuned.size();
   return NICP_OK;
 }
 
@@ -987,7 +1013,7 @@ extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_c
   CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
   CK(ctx, cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s));
   const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
-  launch_zbuffer(dpd, 1, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
+  launch_zbuffer(dpd, 1, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), kZbufDefaultPPT, s, &ctx->prof);
   launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ctx->ws + o_depth), 0, s, &ctx->prof);
   CK(ctx, cudaGetLastError());
   if (index_out) CK(ctx, cudaMemcpyAsync(index_out, ctx->ws + pl.o_cur[0], 4 * P, cudaMemcpyDeviceToHost, s));
@@ -1028,12 +1054,13 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
   launch_init_pairs(dpd, pl.n, (const double *)(ctx->ws + pl.o_guess), (const double *)(ctx->ws + pl.o_roff), s,
                     &ctx->prof);
   // current cloud, seen from its sensor offset, projected once (alignerprojective.cpp:36-39)
-  launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), s, &ctx->prof);
+  const nicp_ctx::Launch &L = ctx->launch;
+  launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), L.zb_ppt, s, &ctx->prof);
   // outside list (parity) mode, current pixels whose point has no normal are
   // dropped from the index image: the gates would reject them anyway
   launch_resolve(dpd, pl.n, pl.total_tiles, 0, nullptr, (pl.list_mode || cp.demoted) ? 0 : 1, s, &ctx->prof);
   for (int i = 0; i < outer; i++) {
-    launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 1, nullptr, s, &ctx->prof);
+    launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 1, nullptr, L.zb_ppt, s, &ctx->prof);
     if (pl.list_mode) {
       launch_resolve(dpd, pl.n, pl.total_tiles, 1, nullptr, 0, s, &ctx->prof);
       launch_corr_list(dpd, pl.n, pl.total_tiles, cp, 1, nullptr, s, &ctx->prof);
@@ -1044,7 +1071,7 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
     } else {
       for (int k = 0; k < inner; k++) {
         int flags = (k == 0) ? (1 | 2 | (pl.keep_ref ? 4 : 0)) : 0;
-        launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, flags, pl.structured, s, &ctx->prof);
+        launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, flags, pl.structured, L.corr_ctas, s, &ctx->prof);
         launch_solve(dpd, pl.n, p.lambda, ((k == inner - 1) ? 1 : 0) | xb, p.early_exit_eps, 0, s, &ctx->prof);
       }
     }
@@ -1055,7 +1082,7 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
     if (pl.list_mode)
       launch_lin_list(dpd, pl.n, pl.total_tiles, lp, std::max(1, a.corr->parity_threads), 2, nullptr, s, &ctx->prof);
     else
-      launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, 8, pl.structured, s, &ctx->prof);
+      launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, 8, pl.structured, L.corr_ctas, s, &ctx->prof);
     launch_solve(dpd, pl.n, 0.0f, 4 | xb, 0.0, 1, s, &ctx->prof);
   }
 }
@@ -1076,7 +1103,67 @@ static std::string graph_key(nicp_ctx *ctx, const PairPlan &pl, const AlignCall 
   put(a.prm, sizeof(*a.prm));
   bool pe = ctx->prof.enabled;
   put(&pe, 1);
+  put(&ctx->launch, sizeof(ctx->launch));
   return k;
+}
+
+// The resolution mix of a batch: sorted (rows, cols, count) plus the loop
+// shape; the autotuner keeps one choice per key.
+static std::string tune_key(const PairPlan &pl, const AlignCall &a) {
+  std::map<std::pair<int, int>, int> hist;
+  for (int i = 0; i < a.n; i++) hist[{cam_rows(a.cams[i]), cam_cols(a.cams[i])}]++;
+  std::string k;
+  for (auto &h : hist) k += std::to_string(h.first.first) + "x" + std::to_string(h.first.second) + ":" +
+                           std::to_string(h.second) + " ";
+  k += "o" + std::to_string(a.prm->outer_iterations) + "i" + std::to_string(a.prm->inner_iterations) +
+       (pl.structured ? "s" : "g") + (a.prm->compute_statistics ? "t" : "");
+  return k;
+}
+
+// Times the loop with each candidate launch shape (direct launches, CUDA
+// events on the context stream) and keeps the fastest: z-buffer points per
+// thread first, then the fused kernel's CTAs per SM.  The loop re-initialises
+// every pair from its guess, so trials leave no trace in the results.
+static int autotune_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a, nicp_ctx::Launch *best) {
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t e0, e1;
+  CK(ctx, cudaEventCreate(&e0));
+  CK(ctx, cudaEventCreate(&e1));
+  bool prof = ctx->prof.enabled;
+  ctx->prof.enabled = false;
+  std::vector<float> times;
+  auto trial = [&](const nicp_ctx::Launch &c, float *ms) -> int {
+    ctx->launch = c;
+    CK(ctx, cudaEventRecord(e0, s));
+    enqueue_loop(ctx, pl, a);
+    CK(ctx, cudaEventRecord(e1, s));
+    CK(ctx, cudaEventSynchronize(e1));
+    CK(ctx, cudaEventElapsedTime(ms, e0, e1));
+    times.push_back(*ms);
+    return NICP_OK;
+  };
+  nicp_ctx::Launch cur;
+  float ms = 0, best_ms = 0;
+  int rc = trial(cur, &ms);  // warm-up (module load, caches)
+  if (!rc) rc = trial(cur, &best_ms);
+  *best = cur;
+  const int ppts[] = {1, 2, 8};
+  for (int i = 0; i < 3 && !rc; i++) {
+    nicp_ctx::Launch c = *best;
+    c.zb_ppt = ppts[i];
+    if (!(rc = trial(c, &ms)) && ms < best_ms) { best_ms = ms; *best = c; }
+  }
+  const int ctas[] = {1, 2};
+  for (int i = 0; i < 2 && !rc; i++) {
+    nicp_ctx::Launch c = *best;
+    c.corr_ctas = ctas[i];
+    if (!(rc = trial(c, &ms)) && ms < best_ms) { best_ms = ms; *best = c; }
+  }
+  ctx->prof.enabled = prof;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->tune_ms[tune_key(pl, a)] = times;
+  return rc;
 }
 
 static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out) {
@@ -1134,6 +1221,17 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
   CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_roff, ro, 128 * (size_t)a.n, cudaMemcpyHostToDevice, s));
   CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
   ctx->h2d_bytes += (sizeof(PairDev) + 48 + 256) * (unsigned long long)a.n;
+  ctx->launch = nicp_ctx::Launch();
+  if (ctx->autotune && !list_mode) {
+    std::string tk = tune_key(pl, a);
+    auto it = ctx->tuned.find(tk);
+    if (it == ctx->tuned.end()) {
+      nicp_ctx::Launch best;
+      if ((rc = autotune_loop(ctx, pl, a, &best))) return rc;
+      it = ctx->tuned.emplace(tk, best).first;
+    }
+    ctx->launch = it->second;
+  }
   // Events recorded while a stream is captured are capture-internal and
   // cannot be timed after a replay, so a profiled call launches the same
   // kernels directly.

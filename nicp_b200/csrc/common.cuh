@@ -27,9 +27,8 @@ constexpr int kUnprojTilePixels = 4096; // 16 pixels per thread, 256 threads
 constexpr int kStatsThreads = 256;
 constexpr int kPartialWords = 32;       // doubles per CTA partial (21 H + 6 b + chi2 + inliers + C + K + pad)
 constexpr int kSolveCrossF32 = 32;      // k_solve mode bit: FP32 sum of the tile partials
-constexpr int kZbufThreads = 256;
-constexpr int kZbufPointsPerThread = 4;
-constexpr int kPointsPerCta = kZbufThreads * kZbufPointsPerThread;  // z-buffer kernel tile
+constexpr int kPointsPerCta = 1024;     // z-buffer kernel tile (points per CTA; threads = 1024 / points per thread)
+constexpr int kZbufDefaultPPT = 4;      // points per thread unless the autotuner picked another
 
 // pts[i].w is kNoNormalW for a point without a normal, and 1 + class for a
 // point with one, class = (point information matrix non-flat) + 2 (normal

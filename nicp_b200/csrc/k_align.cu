@@ -47,8 +47,13 @@ __device__ __forceinline__ int find_pair(const PairDev *pairs, int n, int key, b
 // mode 0: project the current cloud with pair.KRt_cur-equivalent `explicit_KRt`
 // (one matrix for all pairs, host-computed); mode 1: the reference cloud with
 // the pair state's KRt.
-__global__ void __launch_bounds__(kZbufThreads)
+// A CTA covers kPointsPerCta points with kPointsPerCta / PPT threads, PPT
+// independent points per thread (their loads and atomics overlap); the
+// result does not depend on PPT (atomicMin is order-free).
+template <int PPT>
+__global__ void __launch_bounds__(kPointsPerCta / PPT)
     k_zbuffer(const PairDev *__restrict__ pairs, int npairs, int mode, const float *__restrict__ explicit_KRt) {
+  constexpr int kThreads = kPointsPerCta / PPT;
   int pi = find_pair(pairs, npairs, blockIdx.x, true);
   const PairDev &pd = pairs[pi];
   const PairState *st = pd.state;
@@ -61,16 +66,15 @@ __global__ void __launch_bounds__(kZbufThreads)
   const float *src = mode ? st->KRt : explicit_KRt + 12 * pi;
 #pragma unroll
   for (int k = 0; k < 12; k++) K[k] = src[k];
-  // four independent points per thread: their loads and atomics overlap
-  float4 p[kZbufPointsPerThread];
+  float4 p[PPT];
 #pragma unroll
-  for (int k = 0; k < kZbufPointsPerThread; k++) {
-    int i = i0 + k * kZbufThreads;
+  for (int k = 0; k < PPT; k++) {
+    int i = i0 + k * kThreads;
     p[k] = (i < n) ? pts[i] : make_float4(0.f, 0.f, 0.f, 0.f);
   }
 #pragma unroll
-  for (int k = 0; k < kZbufPointsPerThread; k++) {
-    int i = i0 + k * kZbufThreads;
+  for (int k = 0; k < PPT; k++) {
+    int i = i0 + k * kThreads;
     int x, y;
     float d;
     if (i >= n || !project_pixel(K, p[k], pd.rows, pd.cols, pd.min_d, pd.max_d, x, y, d)) continue;
@@ -812,10 +816,15 @@ __global__ void __launch_bounds__(128) k_solve(const PairDev *__restrict__ pairs
 
 // ------------------------------------------------------------ launchers
 void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int mode, const float *explicit_KRt,
-                    cudaStream_t s, Profiler *prof) {
+                    int ppt, cudaStream_t s, Profiler *prof) {
   if (total_pt_tiles <= 0) return;
   prof->begin(NICP_K_ZBUFFER, s);
-  k_zbuffer<<<total_pt_tiles, kZbufThreads, 0, s>>>(d_pairs, npairs, mode, explicit_KRt);
+  switch (ppt) {
+    case 1: k_zbuffer<1><<<total_pt_tiles, kPointsPerCta, 0, s>>>(d_pairs, npairs, mode, explicit_KRt); break;
+    case 2: k_zbuffer<2><<<total_pt_tiles, kPointsPerCta / 2, 0, s>>>(d_pairs, npairs, mode, explicit_KRt); break;
+    case 8: k_zbuffer<8><<<total_pt_tiles, kPointsPerCta / 8, 0, s>>>(d_pairs, npairs, mode, explicit_KRt); break;
+    default: k_zbuffer<4><<<total_pt_tiles, kPointsPerCta / 4, 0, s>>>(d_pairs, npairs, mode, explicit_KRt); break;
+  }
   prof->end(NICP_K_ZBUFFER, s);
 }
 
@@ -829,8 +838,8 @@ void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_
 // Persistent grid: as many CTAs as fit on the device at once, never more
 // than there are tiles.
 template <bool kStructured>
-static int corr_lin_grid(int total_tiles) {
-  static int resident = 0;
+static int corr_lin_grid(int total_tiles, int ctas_per_sm) {
+  static int resident = 0, sm_count = 0, per_sm_max = 0;
   if (!resident) {
     cudaFuncSetAttribute(k_corr_lin<kStructured>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          corr_smem<kStructured>());
@@ -839,20 +848,23 @@ static int corr_lin_grid(int total_tiles) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lin<kStructured>, kCorrThreads,
                                                   corr_smem<kStructured>());
-    resident = std::max(1, sms * std::max(1, per_sm));
+    per_sm_max = std::max(1, per_sm);
+    sm_count = std::max(1, sms);
+    resident = sm_count * per_sm_max;
   }
-  return std::min(total_tiles, resident);
+  int grid = (ctas_per_sm > 0 && ctas_per_sm < per_sm_max) ? sm_count * ctas_per_sm : resident;
+  return std::min(total_tiles, grid);
 }
 
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
-                     int flags, bool structured, cudaStream_t s, Profiler *prof) {
+                     int flags, bool structured, int ctas_per_sm, cudaStream_t s, Profiler *prof) {
   if (total_tiles <= 0) return;
   prof->begin(NICP_K_CORR_LIN, s);
   if (structured) {
-    int grid = corr_lin_grid<true>(total_tiles);
+    int grid = corr_lin_grid<true>(total_tiles, ctas_per_sm);
     k_corr_lin<true><<<grid, kCorrThreads, corr_smem<true>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
   } else {
-    int grid = corr_lin_grid<false>(total_tiles);
+    int grid = corr_lin_grid<false>(total_tiles, ctas_per_sm);
     k_corr_lin<false><<<grid, kCorrThreads, corr_smem<false>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
   }
   prof->end(NICP_K_CORR_LIN, s);

@@ -77,11 +77,11 @@ void solution_statistics(const double H36[36], const double T16[16], double *tra
                          double *rotational_ratio);
 
 void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int mode, const float *explicit_KRt,
-                    cudaStream_t s, Profiler *prof);
+                    int ppt, cudaStream_t s, Profiler *prof);
 void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out,
                     int drop_no_normal, cudaStream_t s, Profiler *prof);
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
-                     int flags, bool structured, cudaStream_t s, Profiler *prof);
+                     int flags, bool structured, int ctas_per_sm, cudaStream_t s, Profiler *prof);
 void launch_corr_list(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, int use_state_T,
                       const float *explicit_T, cudaStream_t s, Profiler *prof);
 void launch_lin_list(const PairDev *d_pairs, int npairs, int total_tiles, const LinParams &lp, int parity_threads,

@@ -1,0 +1,82 @@
+"""Controls of the batched loop (no reference counterpart): the autotuner's
+launch shapes and the per-pair early exit.
+
+* Autotuned and default launch shapes give bitwise the same poses (the
+  shapes change how work is spread, not what is summed or in which order).
+* A pair stops once its pose changes by less than early_exit_eps in an outer
+  iteration; its result then differs from the full run by no more than the
+  remaining iterations would have moved it, and pairs that converge early
+  report fewer iterations."""
+import numpy as np
+import pytest
+
+from nicp_b200 import _lib as L
+from nicp_b200 import api, synth
+
+from helpers import converter, gpu_cloud
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [(51, "160x120"), (52, "320x240"), (53, "640x480"), (54, "320x240"), (55, "640x480"), (56, "160x120")]
+
+
+@pytest.fixture(scope="module")
+def batch(ctx):
+    refs, curs, cams, truth = [], [], [], []
+    for seed, name in SPECS:
+        d1, d2, Tgt, cam = synth.render_pair(seed, name, deg=0.5, deg_hi=5.0, meters=0.01, m_hi=0.08)
+        proj, conv = converter(cam, ctx)
+        refs.append(gpu_cloud(ctx, conv, d1, keep_index=False)[0])
+        curs.append(gpu_cloud(ctx, conv, d2, keep_index=False)[0])
+        cams.append(proj.camera())
+        truth.append(Tgt)
+    return refs, curs, cams, truth
+
+
+def _params(ctx, outer=20, inner=2, eps=0.0):
+    prm = L.AlignParams()
+    ctx.lib.nicp_default_align_params(prm)
+    prm.compute_statistics = 0
+    prm.outer_iterations, prm.inner_iterations, prm.early_exit_eps = outer, inner, eps
+    return prm
+
+
+def _run(ctx, batch, prm):
+    refs, curs, cams, _ = batch
+    corr = api.CorrespondenceFinderProjective(ctx).params()
+    lin = api.Linearizer(ctx).params()
+    return api.align_batch(ctx, refs, curs, cams, None, corr, lin, prm)
+
+
+def test_autotuned_shapes_give_identical_results(ctx, batch):
+    prm = _params(ctx)
+    ctx.set_autotune(False)
+    base = _run(ctx, batch, prm)
+    assert ctx.launch_shape()[:2] == (4, 0)
+    ctx.set_autotune(True)
+    try:
+        tuned = _run(ctx, batch, prm)
+        ppt, ctas, mixes = ctx.launch_shape()
+        assert ppt in (1, 2, 4, 8) and ctas in (0, 1, 2) and mixes >= 1
+        again = _run(ctx, batch, prm)  # cached choice, no new trials
+        assert ctx.launch_shape() == (ppt, ctas, mixes)
+    finally:
+        ctx.set_autotune(False)
+    for a, b, c in zip(base, tuned, again):
+        assert np.array_equal(np.array(a.T), np.array(b.T))
+        assert np.array_equal(np.array(a.T), np.array(c.T))
+        assert a.inliers == b.inliers == c.inliers
+
+
+def test_early_exit(ctx, batch):
+    full = _run(ctx, batch, _params(ctx))
+    early = _run(ctx, batch, _params(ctx, eps=1e-4))
+    iters = [r.outer_iterations_run for r in early]
+    assert all(r.outer_iterations_run == 20 for r in full)
+    assert min(iters) < 20, iters
+    for f, e in zip(full, early):
+        er, et = synth.pose_error(np.array(e.T).reshape(4, 4), np.array(f.T).reshape(4, 4))
+        if e.outer_iterations_run < 20:
+            assert er < 2e-3 and et < 2e-3, (er, et, e.outer_iterations_run)
+        else:
+            assert np.array_equal(np.array(e.T), np.array(f.T))
