@@ -123,25 +123,36 @@ struct Acc {
 
 // correspondencefinderprojective.cpp:59-101.  T12: rows 0..2 of the gating
 // transform (the aligner passes _T.inverse()).
-__device__ __forceinline__ bool gate(const CorrParams &cp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
-                                     float4 cn) {
+// The transformed reference point and normal are returned in rp / rn (rn
+// only when the normal gates run, i.e. not demoted).
+__device__ __forceinline__ bool gate_t(const CorrParams &cp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
+                                       float4 cn, float3 &rp, float3 &rn) {
   if (!cp.demoted) {
     if (dot3x(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) return false;
     if (dot3x(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return false;
   }
-  float3 rp = xform_point(T12, rp0);
+  rp = xform_point(T12, rp0);
   float dx = fsb(cpt.x, rp.x), dy = fsb(cpt.y, rp.y), dz = fsb(cpt.z, rp.z);
   if (dot3x(dx, dy, dz, dx, dy, dz) > cp.sq_thr) return false;
   if (!cp.demoted) {
-    float3 rn = xform_normal(T12, rn0);
+    rn = xform_normal(T12, rn0);
     if (dot3x(cn.x, cn.y, cn.z, rn.x, rn.y, rn.z) < cp.cos_thr) return false;
     float kr = rn0.w, kc = cn.w;
     if (kr < cp.flat_thr) kr = cp.flat_thr;
     if (kc < cp.flat_thr) kc = cp.flat_thr;
-    float ratio = __double2float_rn(__ddiv_rn(__dadd_rn((double)kr, 1e-5), __dadd_rn((double)kc, 1e-5)));
+    // equal curvatures (in particular both below the flat threshold) give a
+    // ratio of exactly 1: skip the division
+    float ratio =
+        (kr == kc) ? 1.0f : __double2float_rn(__ddiv_rn(__dadd_rn((double)kr, 1e-5), __dadd_rn((double)kc, 1e-5)));
     if (ratio < cp.min_ratio || ratio > cp.max_ratio) return false;
   }
   return true;
+}
+
+__device__ __forceinline__ bool gate(const CorrParams &cp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
+                                     float4 cn) {
+  float3 rp, rn;
+  return gate_t(cp, T12, rp0, rn0, cpt, cn, rp, rn);
 }
 
 // linearizer.cpp:59-100 for one correspondence, FP32.
@@ -226,10 +237,10 @@ __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12,
 // and w = S^T u:  Omega e = a e + b (u.e) u,  Omega S = a S + b u w^T,
 // S^T Omega S = a (|2v|^2 I - (2v)(2v)^T) + b w w^T.  The class code in the
 // point's w selects (d0, d1); omd holds them for the four classes.
-__device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const float *T12, const float *omd,
-                                                    float4 rp0, float4 rn0, float4 cpt, float4 cn, Acc &acc) {
-  float3 rp = xform_point(T12, rp0);
-  float3 rn = xform_normal(T12, rn0);
+// rp, rn: the reference point and normal already moved by the linearizer's
+// transform.
+__device__ __forceinline__ void lin_terms_structured_xf(const LinParams &lp, const float *omd, float3 rp, float3 rn,
+                                                       float4 cpt, float4 cn, Acc &acc) {
   float alp = 0.0f, bep = 0.0f, aln = 0.0f, ben = 0.0f;
   if (point_has_normal(cpt.w)) {
     const int cls = (int)cpt.w - 1;
@@ -285,6 +296,11 @@ __device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const 
   float u0 = b * ep[2] - c * ep[1], u1 = c * ep[0] - a * ep[2], u2 = a * ep[1] - b * ep[0];
   float w0 = bn * en[2] - cn2 * en[1], w1 = cn2 * en[0] - an * en[2], w2 = an * en[1] - bn * en[0];
   acc.v[24] += ks * (u0 + w0); acc.v[25] += ks * (u1 + w1); acc.v[26] += ks * (u2 + w2);
+}
+
+__device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const float *T12, const float *omd,
+                                                    float4 rp0, float4 rn0, float4 cpt, float4 cn, Acc &acc) {
+  lin_terms_structured_xf(lp, omd, xform_point(T12, rp0), xform_normal(T12, rn0), cpt, cn, acc);
 }
 
 // Reduces every thread's Acc to one FP64 partial of the CTA (fixed order).
@@ -376,7 +392,7 @@ __global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS :
   // [0..11] gating T, [12..23] linearizer T, [24..31] the current cloud's
   // Omega parameters, then pair index, skip flag and structured-Omega flag
   __shared__ float sT[2][32];
-  __shared__ int sPair[2], sSkip[2], sStruct[2];
+  __shared__ int sPair[2], sSkip[2], sStruct[2], sSame[2];
   const bool stats_pass = flags & 8;
   if ((int)blockIdx.x >= total_tiles) return;
   const int ntiles = (total_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
@@ -476,6 +492,12 @@ __global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS :
       sPair[e] = pi;
       sSkip[e] = st->done && !stats_pass;
       sStruct[e] = pairs[pi].cur_structured;
+      // gating and linearizer transforms equal (first inner iteration): the
+      // linearizer reuses the gate's transformed point and normal
+      const float *tg = stats_pass ? st->Tgate_used : st->Tgate;
+      int same = 1;
+      for (int k = 0; k < 12; k++) same &= (tg[k] == st->Tlin[k]);
+      sSame[e] = same;
     }
   };
 
@@ -485,6 +507,12 @@ __global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS :
       Stage &g = stage_of(j);
       int e = (j / kSubsPerTile) & 1;
       int acc_ok = 0;
+      if constexpr (kStructured) {
+        // structured: nothing to gather after the gate; it runs with the
+        // linearizer in the main step
+        cp_async_commit();
+        return;
+      }
       if (g.valid[t] && !sSkip[e]) {
         acc_ok = gate(cp, sT[e], g.rp[t], g.rn[t], g.cp[t], g.cn[t]) ? 2 : 1;
         if constexpr (!kStructured) {
@@ -532,12 +560,23 @@ __global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS :
     if (!sSkip[e]) {
       const Stage &g = stage_of(j);
       const int v = g.valid[t];
-      if (v) acc.v[29] += 1.0f;
-      if (v == 2) {
-        acc.v[30] += 1.0f;
-        if constexpr (kStructured) {
-          lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, g.rp[t], g.rn[t], g.cp[t], g.cn[t], acc);
-        } else {
+      if constexpr (kStructured) {
+        if (v) {
+          acc.v[29] += 1.0f;
+          const float4 rp0 = g.rp[t], rn0 = g.rn[t], cpt = g.cp[t], cn = g.cn[t];
+          float3 rp, rn;
+          if (gate_t(cp, sT[e], rp0, rn0, cpt, cn, rp, rn)) {
+            acc.v[30] += 1.0f;
+            if (sSame[e] && !cp.demoted)
+              lin_terms_structured_xf(lp, sT[e] + 24, rp, rn, cpt, cn, acc);
+            else
+              lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, rp0, rn0, cpt, cn, acc);
+          }
+        }
+      } else {
+        if (v) acc.v[29] += 1.0f;
+        if (v == 2) {
+          acc.v[30] += 1.0f;
           if (sStruct[e])
             lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, g.rp[t], g.rn[t], g.cp[t], g.cn[t], acc);
           else
