@@ -19,6 +19,7 @@ one batched, graph-captured device loop.  Metric: 640x480 pairs/s.
                threads) on a bounded sample of the same workload
   mixed_batch  512 independent pairs of mixed resolution, <= 20 x 2 iterations
                with early exit, batched vs the plain per-pair loop
+  scene_fusion frames fused into one scene (Cloud::add + Merger::merge)
   serving      the request loop (nicp_server_*) under open-loop Poisson load:
                64 camera streams, 30/60/10% 320x240/640x480/1280x720,
                p50/p99 latency and throughput per arrival rate
@@ -384,6 +385,42 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
                                        "corr_lin_ctas_per_sm": shape[1] or "all that fit"}}
 
 
+# ------------------------------------------------------------------ scene fusion leg
+def scene_fusion_leg(ctx, seed, frames=30):
+    """Frame-to-scene fusion as nicp_aligner.cpp:172-209 maintains its scene:
+    every 640x480 frame of the trajectory (Gaussians kept) is added to the
+    scene with its pose (Cloud::add) and the scene is merged in that frame's
+    view (Merger::merge).  Ground-truth poses; wall time per frame of the
+    add + merge calls (both synchronous)."""
+    from nicp_b200 import api, synth
+    imgs, poses, cam = synth.render_sequence(seed, "640x480", n_frames=frames, period=200)
+    proj, conv, _, _, _ = gpu_objects(ctx, cam)
+    conv.keepGaussians = True
+    clouds = []
+    for f in imgs:
+        c = api.Cloud(ctx)
+        conv.compute(c, f)
+        clouds.append(c)
+    per_frame = clouds[0].size()
+    scene = clouds[0]
+    merger = api.Merger(ctx)
+    merger.setDepthImageConverter(conv)
+    merger.setImageSize(cam["rows"], cam["cols"])
+    removed, times = 0, []
+    for k in range(1, frames):
+        T = synth.rel(poses[0], poses[k]).astype(np.float32)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        scene.add(clouds[k], T)
+        merger.merge(scene, T)
+        ctx.synchronize()
+        times.append(time.perf_counter() - t0)
+        removed += merger.removed
+    return {"workload": "%d 640x480 frames fused into one scene (add + merge per frame, ground-truth poses)" % frames,
+            "ms_per_frame": 1e3 * float(np.median(times)), "frames_per_s": 1.0 / float(np.median(times)),
+            "points_per_frame": per_frame, "scene_points": scene.size(), "removed_points": removed}
+
+
 # ------------------------------------------------------------------ serving leg
 SERVE_MIX = (("320x240", 0.3, 19), ("640x480", 0.6, 38), ("1280x720", 0.1, 7))  # (camera, request share, streams)
 
@@ -559,6 +596,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-call leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the 512-pair mixed-resolution batch leg")
+    ap.add_argument("--no-fusion", action="store_true", help="skip the scene-fusion (merger) leg")
     ap.add_argument("--serve-rates", default="500,2000,5000,10000,20000",
                     help="Poisson arrival rates (requests/s) of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per rate")
@@ -719,6 +757,10 @@ def main():
     if not args.no_mixed and rank == 0:
         mixed = mixed_batch_leg(ctx, stream, local, args.seed + 17)
 
+    fusion = None
+    if not args.no_fusion and rank == 0:
+        fusion = scene_fusion_leg(ctx, args.seed + 29)
+
     serving = None
     if not args.no_serve and rank == 0:
         serving = serve_leg(local, [float(r) for r in args.serve_rates.split(",")], args.serve_seconds, args.seed)
@@ -740,7 +782,7 @@ def main():
                 "gpu_launches": int(launches), "clocks": clk,
                 "plain_pairs_per_s": plain, "batched_over_plain": (value / world / plain) if plain else None,
                 "pose_err_vs_truth_median": {"rad": rot_med, "m": tr_med},
-                "points_per_frame": V, "correspondences_per_pair": C, "mixed_batch": mixed,
+                "points_per_frame": V, "correspondences_per_pair": C, "mixed_batch": mixed, "scene_fusion": fusion,
                 "serving": serving}
         print(json.dumps(line), flush=True)
     del clouds

@@ -129,6 +129,10 @@ class Cloud {
     check(ctx_->handle(), nicp_cloud_download_gaussians(h_, means.data(), covariances.data()));
   }
   void transformInPlace(const Isometry3f &T) { check(ctx_->handle(), nicp_cloud_transform(h_, T.data())); }
+  // add(cloud, T) (cloud.cpp:163-189): `cloud` is transformed in place, then appended.
+  void add(Cloud &cloud, const Isometry3f &T = Isometry3f::Identity()) {
+    check(ctx_->handle(), nicp_cloud_add(h_, cloud.h_, T.data()));
+  }
 
  private:
   std::vector<float> field(int which) const {
@@ -311,6 +315,43 @@ class DepthImageConverterIntegralImage {
   float depth_scale_ = 0.001f;
   bool keep_gaussians_ = false;
 };
+
+// merger.{h,cpp}: fuses points of a cloud that land on one pixel of a view;
+// the cloud needs Gaussians (DepthImageConverterIntegralImage::setKeepGaussians).
+class Merger {
+ public:
+  explicit Merger(Context &ctx = default_context()) : ctx_(&ctx) {}
+  float distanceThreshold() const { return distance_threshold_; }
+  void setDistanceThreshold(float v) { distance_threshold_ = v; }
+  float normalThreshold() const { return normal_threshold_; }  // kept; merge() does not use it (merger.cpp:61-63)
+  void setNormalThreshold(float v) { normal_threshold_ = v; }
+  float maxPointDepth() const { return max_point_depth_; }
+  void setMaxPointDepth(float v) { max_point_depth_ = v; }
+  DepthImageConverterIntegralImage *depthImageConverter() const { return converter_; }
+  void setDepthImageConverter(DepthImageConverterIntegralImage *c) { converter_ = c; }
+  void setImageSize(int r, int c) { rows_ = r; cols_ = c; }
+  int removed() const { return removed_; }
+  void merge(Cloud *cloud, const Isometry3f &transform = Isometry3f::Identity());
+
+ private:
+  Context *ctx_;
+  float distance_threshold_ = 0.1f;
+  float normal_threshold_ = std::cos(10.0f * 3.14159265358979f / 180.0f);
+  float max_point_depth_ = 10.0f;
+  DepthImageConverterIntegralImage *converter_ = nullptr;
+  int rows_ = 0, cols_ = 0, removed_ = 0;
+};
+
+inline void Merger::merge(Cloud *cloud, const Isometry3f &transform) {
+  if (!converter_ || !converter_->projector() || rows_ <= 0 || cols_ <= 0)
+    throw Error(NICP_ESTATE, "Merger: set the converter and the image size first");
+  nicp_camera cam = converter_->projector()->camera();
+  cam.rows = rows_;
+  cam.cols = cols_;
+  check(ctx_->handle(),
+        nicp_merge(ctx_->handle(), cloud->handle(), &cam, transform.data(), distance_threshold_, max_point_depth_,
+                   &removed_));
+}
 
 // correspondencefinder{,projective}.{h,cpp}.
 class CorrespondenceFinderProjective {

@@ -221,6 +221,24 @@ int nicp_cloud_upload(nicp_cloud *c, int n, const float *points4, const float *n
 /* Cloud::transformInPlace (cloud.cpp:191-204). */
 int nicp_cloud_transform(nicp_cloud *c, const float T16[16]);
 
+/* Cloud::add (cloud.cpp:163-189): `src` is first transformed in place by T16
+ * (NULL = identity), as the reference does, then its points are appended to
+ * `dst` (grown as needed).  Stats, Gaussians and the structured-Omega flag
+ * survive only when both clouds carry them.  Both clouds belong to one
+ * context. */
+int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[16]);
+
+/* Merger::merge (merger.cpp:15-109; defaults merger.cpp:5-13: distance
+ * threshold 0.1, max point depth 10).  The cloud is projected by the camera
+ * moved by T16 (z-buffer: smallest depth, then lowest index); each point that
+ * lands on another point's pixel within `distance_threshold` in depth adds
+ * its Gaussian's information to that point's and is removed; a point that
+ * won its own pixel takes its (fused) Gaussian's mean as position.  Needs a
+ * cloud with Gaussians (keep_gaussians).  *removed: points removed (may be
+ * NULL). */
+int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *cam, const float T16[16],
+               float distance_threshold, float max_point_depth, int *removed);
+
 /* DepthImageConverterIntegralImage::compute.  depth: rows x cols u16 with
  * row pitch `pitch_bytes` (0 = packed), in host memory or, when
  * depth_on_device != 0, in device memory.  sensor_offset may be NULL

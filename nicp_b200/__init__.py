@@ -5,6 +5,6 @@ ABI of include/nicp_gpu.h); this package holds its Python binding, the
 reference-named classes (api.py) and the synthetic input generator.
 """
 from .api import (AlignerProjective, Cloud, Context, CorrespondenceFinderProjective,  # noqa: F401
-                  DepthImageConverterIntegralImage, Linearizer, NormalInformationMatrixCalculator,
-                  PinholePointProjector, PointInformationMatrixCalculator, StatsCalculatorIntegralImage,
+                  DepthImageConverterIntegralImage, Linearizer, Merger, NormalInformationMatrixCalculator,
+                  PinholePointProjector, PointInformationMatrixCalculator, Server, StatsCalculatorIntegralImage,
                   align_batch, build_batch)

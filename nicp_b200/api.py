@@ -151,6 +151,14 @@ class Cloud:
     def normals(self):
         return self.download()["normals"]
 
+    def add(self, cloud, T=None):
+        """Cloud::add (cloud.cpp:163-189): `cloud` is transformed in place by T
+        (as the reference does) and appended to this cloud."""
+        self.ctx.check(self.ctx.lib.nicp_cloud_add(self.h, cloud.h, L.fptr(L.f16(T))))
+        if not cloud.has_stats:
+            self.has_stats = False
+        return self
+
     def upload(self, points, normals, curvature, omega_p=None, omega_n=None):
         n = len(points)
         p = np.ascontiguousarray(points, np.float32).reshape(n, 4)
@@ -419,6 +427,48 @@ class DepthImageConverterIntegralImage:
 
 
 # ------------------------------------------------------------------ registration
+class Merger:
+    """merger.{h,cpp}: fuses the points of a cloud that land on the same pixel
+    of a view (Gaussian information fusion) and removes the absorbed ones.
+    Defaults merger.cpp:5-13.  The cloud needs Gaussians (a converter with
+    keepGaussians = True)."""
+
+    def __init__(self, ctx=None):
+        self.ctx = ctx or Context.default()
+        self._distanceThreshold = 0.1
+        self._normalThreshold = float(np.float32(math.cos(10 * math.pi / 180.0)))  # kept, unused by merge()
+        self._maxPointDepth = 10.0
+        self._depthImageConverter = None
+        self._rows = self._cols = 0
+        self.removed = 0
+
+    def distanceThreshold(self): return self._distanceThreshold
+    def setDistanceThreshold(self, v): self._distanceThreshold = float(v)
+    def normalThreshold(self): return self._normalThreshold
+    def setNormalThreshold(self, v): self._normalThreshold = float(v)
+    def maxPointDepth(self): return self._maxPointDepth
+    def setMaxPointDepth(self, v): self._maxPointDepth = float(v)
+    def depthImageConverter(self): return self._depthImageConverter
+    def setDepthImageConverter(self, c): self._depthImageConverter = c
+    def imageSize(self): return (self._rows, self._cols)
+
+    def setImageSize(self, r, c):
+        self._rows, self._cols = int(r), int(c)
+
+    def merge(self, cloud, transform=None):
+        if self._rows <= 0 or self._cols <= 0:
+            raise ValueError("Merger: call setImageSize() first")
+        if self._depthImageConverter is None:
+            raise ValueError("Merger: missing depth image converter")
+        cam = self._depthImageConverter.projector().camera(self._rows, self._cols)
+        removed = C.c_int(0)
+        T = np.eye(4, dtype=np.float32) if transform is None else transform
+        self.ctx.check(self.ctx.lib.nicp_merge(self.ctx.h, cloud.h, C.byref(cam), L.fptr(L.f16(T)),
+                                               self._distanceThreshold, self._maxPointDepth, C.byref(removed)))
+        self.removed = removed.value
+        return cloud
+
+
 class CorrespondenceFinderProjective:
     """correspondencefinder{,projective}.{h,cpp}; defaults correspondencefinder.cpp:9-18."""
 

@@ -1022,6 +1022,191 @@ extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_c
   return NICP_OK;
 }
 
+// ------------------------------------------------------------------ scene
+// Grows a cloud's allocation to `capacity` points keeping its first n
+// points (all arrays) and its counts.
+static int cloud_grow(nicp_cloud *c, int capacity, int n) {
+  nicp_ctx *ctx = c->ctx;
+  Layout L;
+  size_t o_pts = L.take(16 * (size_t)capacity), o_nrm = L.take(16 * (size_t)capacity);
+  size_t o_omg = L.take(48 * (size_t)capacity);
+  size_t o_eig = c->has_eig ? L.take(48 * (size_t)capacity) : 0;
+  size_t o_gauss = c->has_gauss ? L.take(48 * (size_t)capacity) : 0;
+  size_t o_cnt = L.take(2 * sizeof(int));
+  size_t P = std::max<size_t>((size_t)c->rows * c->cols, 1);
+  size_t o_idx = L.take(4 * P);
+  char *mem = nullptr;
+  if (cudaMalloc(&mem, L.off) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, NICP_ENOMEM, "cloud allocation failed");
+  }
+  cudaStream_t s = ctx->stream;
+  CK(ctx, cudaMemcpyAsync(mem + o_pts, c->pts, 16 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(mem + o_nrm, c->nrm, 16 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(mem + o_omg, c->omg, 48 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  if (c->has_eig) CK(ctx, cudaMemcpyAsync(mem + o_eig, c->eig, 48 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  if (c->has_gauss) CK(ctx, cudaMemcpyAsync(mem + o_gauss, c->gauss, 48 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(mem + o_cnt, c->count, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  cudaFree(c->mem);
+  ctx->cloud_bytes += L.off - c->bytes;
+  c->mem = mem;
+  c->bytes = L.off;
+  c->capacity = capacity;
+  c->pts = (float4 *)(mem + o_pts);
+  c->nrm = (float4 *)(mem + o_nrm);
+  c->omg = (float4 *)(mem + o_omg);
+  c->eig = c->has_eig ? (float *)(mem + o_eig) : nullptr;
+  c->gauss = c->has_gauss ? (float4 *)(mem + o_gauss) : nullptr;
+  c->count = (int *)(mem + o_cnt);
+  c->index = (int32_t *)(mem + o_idx);
+  return NICP_OK;
+}
+
+static int cloud_counts2(nicp_cloud *c, int out[2]) {
+  out[0] = out[1] = 0;
+  if (!c->mem) return NICP_OK;
+  nicp_ctx *ctx = c->ctx;
+  char *pin;
+  int rc = pin_down(ctx, 2 * sizeof(int), &pin);
+  if (rc) return rc;
+  CK(ctx, cudaMemcpyAsync(pin, c->count, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(out, pin, 2 * sizeof(int));
+  return NICP_OK;
+}
+
+extern "C" int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[16]) {
+  if (!dst || !src || dst == src || dst->ctx != src->ctx) return NICP_EINVAL;
+  nicp_ctx *ctx = dst->ctx;
+  int rc = T16 ? nicp_cloud_transform(src, T16) : NICP_OK;  // Cloud::add moves the added cloud itself
+  if (rc) return rc;
+  int cd[2], cs[2];
+  if ((rc = cloud_counts2(dst, cd)) || (rc = cloud_counts2(src, cs))) return rc;
+  const int nd = cd[0], ns = cs[0];
+  if (ns == 0) return NICP_OK;
+  const bool empty = nd == 0;
+  const bool eig = src->eig_valid && (empty || dst->eig_valid);
+  const bool gauss = src->gauss_valid && (empty || dst->gauss_valid);
+  const bool structured = src->omega_structured &&
+                          (empty || (dst->omega_structured && std::memcmp(dst->omd, src->omd, sizeof(src->omd)) == 0));
+  if (empty) {
+    if ((rc = cloud_reserve(dst, ns, src->rows, src->cols, eig, gauss))) return rc;
+  } else if (dst->capacity < nd + ns || (eig && !dst->has_eig) || (gauss && !dst->has_gauss)) {
+    dst->has_eig = dst->has_eig && eig;
+    dst->has_gauss = dst->has_gauss && gauss;
+    int cap = std::max(nd + ns, dst->capacity + dst->capacity / 2);
+    if ((rc = cloud_grow(dst, cap, nd))) return rc;
+  }
+  cudaStream_t s = ctx->stream;
+  CK(ctx, cudaMemcpyAsync(dst->pts + nd, src->pts, 16 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(dst->nrm + nd, src->nrm, 16 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(dst->omg + 3 * (size_t)nd, src->omg, 48 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
+  if (eig && dst->eig)
+    CK(ctx, cudaMemcpyAsync(dst->eig + 12 * (size_t)nd, src->eig, 48 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
+  if (gauss && dst->gauss)
+    CK(ctx, cudaMemcpyAsync(dst->gauss + 3 * (size_t)nd, src->gauss, 48 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
+  char *pin;
+  if ((rc = pin_up(ctx, 2 * sizeof(int), &pin))) return rc;
+  int *cnt = (int *)pin;
+  cnt[0] = nd + ns;
+  cnt[1] = cd[1] + cs[1];
+  CK(ctx, cudaMemcpyAsync(dst->count, cnt, 2 * sizeof(int), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  dst->eig_valid = eig && dst->eig;
+  dst->gauss_valid = gauss && dst->gauss;
+  dst->omega_structured = structured;
+  if (empty) std::memcpy(dst->omd, src->omd, sizeof(src->omd));
+  return NICP_OK;
+}
+
+extern "C" int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *cam, const float T16[16],
+                          float distance_threshold, float max_point_depth, int *removed) {
+  if (!ctx || !cloud || !cam || !valid_camera(cam) || cloud->ctx != ctx) return NICP_EINVAL;
+  if (removed) *removed = 0;
+  int cnt[2];
+  int rc = cloud_counts2(cloud, cnt);
+  if (rc) return rc;
+  const int n = cnt[0];
+  if (n == 0) return NICP_OK;
+  if (!cloud->gauss_valid)
+    return fail(ctx, NICP_ESTATE, "merge needs the cloud's Gaussians: build it with keep_gaussians");
+  const size_t P = (size_t)cam_rows(*cam) * cam_cols(*cam);
+  const size_t N = (size_t)n;
+  Layout E;  // inside the plan's extra region
+  size_t o_depth = E.take(4 * P);
+  size_t o_int[7];
+  for (int k = 0; k < 7; k++) o_int[k] = E.take(4 * N);
+  size_t scan_bytes = merge_scan_temp_bytes(n);
+  size_t o_scan = E.take(scan_bytes);
+  size_t o_pts = E.take(16 * N), o_nrm = E.take(16 * N), o_omg = E.take(48 * N);
+  size_t o_eig = E.take(cloud->eig_valid ? 48 * N : 16), o_gauss = E.take(48 * N), o_cnt = E.take(8);
+  PairPlan pl;
+  const nicp_cloud *cc = cloud;
+  if ((rc = plan_pairs(ctx, 1, cam, &cc, false, false, pl, E.off))) return rc;
+  char *pin;
+  if ((rc = pin_up(ctx, sizeof(PairDev) + 48, &pin))) return rc;
+  fill_pairs(ctx, pl, cam, &cc, &cc, (PairDev *)pin);
+  HM4 KRt, iKRt;
+  projector_matrices(*cam, HM4::from(T16), KRt, iKRt);
+  float *k12 = (float *)(pin + sizeof(PairDev));
+  rows12(KRt, k12);
+  cudaStream_t s = ctx->stream;
+  char *ex = ctx->ws + pl.o_extra;
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_pairs, pin, sizeof(PairDev), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_krt, k12, 48, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+  CK(ctx, cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s));
+  const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
+  // the serial z-buffer of PinholePointProjector::project, all points kept
+  launch_zbuffer(dpd, 1, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), kZbufDefaultPPT, s, &ctx->prof);
+  launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ex + o_depth), 0, s, &ctx->prof);
+  MergeArgs a{};
+  a.n = n;
+  a.count = cloud->count;
+  a.pts = cloud->pts;
+  a.nrm = cloud->nrm;
+  a.omg = cloud->omg;
+  a.eig = cloud->eig_valid ? cloud->eig : nullptr;
+  a.gauss = cloud->gauss;
+  a.KRt12 = (const float *)(ctx->ws + pl.o_krt);
+  a.rows = cam_rows(*cam);
+  a.cols = cam_cols(*cam);
+  a.min_d = cam->min_distance;
+  a.max_d = cam->max_distance;
+  a.max_depth = max_point_depth;
+  a.dthr = distance_threshold;
+  a.index = (const int32_t *)(ctx->ws + pl.o_cur[0]);
+  a.depth = (const float *)(ex + o_depth);
+  int *ints[7];
+  for (int k = 0; k < 7; k++) ints[k] = (int *)(ex + o_int[k]);
+  a.tgt = ints[0]; a.cnt = ints[1]; a.off = ints[2]; a.fill = ints[3]; a.list = ints[4]; a.keep = ints[5];
+  a.pos = ints[6];
+  a.scan_temp = ex + o_scan;
+  a.scan_temp_bytes = scan_bytes;
+  a.o_pts = (float4 *)(ex + o_pts);
+  a.o_nrm = (float4 *)(ex + o_nrm);
+  a.o_omg = (float4 *)(ex + o_omg);
+  a.o_eig = cloud->eig_valid ? (float *)(ex + o_eig) : nullptr;
+  a.o_gauss = (float4 *)(ex + o_gauss);
+  a.out_count = (int *)(ex + o_cnt);
+  if (launch_merge(a, s)) {
+    cudaError_t e = cudaGetLastError();
+    return fail(ctx, NICP_ECUDA, std::string("merge: ") + cudaGetErrorString(e));
+  }
+  // the compacted cloud back in place
+  CK(ctx, cudaMemcpyAsync(cloud->pts, a.o_pts, 16 * N, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(cloud->nrm, a.o_nrm, 16 * N, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(cloud->omg, a.o_omg, 48 * N, cudaMemcpyDeviceToDevice, s));
+  if (a.o_eig) CK(ctx, cudaMemcpyAsync(cloud->eig, a.o_eig, 48 * N, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(cloud->gauss, a.o_gauss, 48 * N, cudaMemcpyDeviceToDevice, s));
+  CK(ctx, cudaMemcpyAsync(cloud->count, a.out_count, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  int after[2];
+  if ((rc = cloud_counts2(cloud, after))) return rc;
+  if (removed) *removed = n - after[0];
+  return NICP_OK;
+}
+
 // ------------------------------------------------------------------ aligner
 namespace {
 struct AlignCall {

@@ -106,4 +106,29 @@ struct NoAllocLinArgs {
 // Enqueues the scratch-free linearizer on s; allocates nothing.
 int lin_noalloc(const NoAllocLinArgs &args, double *out_dev, cudaStream_t s);
 
+// Merger::merge on the device (k_merge.cu).  n points (host copy of *count);
+// every per-point array below holds n ints; the o_* staging arrays receive the
+// compacted cloud, out_count its counts (points, points with a normal).
+struct MergeArgs {
+  int n;
+  const int *count;
+  const float4 *pts, *nrm, *omg;
+  const float *eig;       // or null
+  float4 *gauss;          // fused in place
+  const float *KRt12;     // device, the projector's KRt for the merge transform
+  int rows, cols;
+  float min_d, max_d, max_depth, dthr;
+  const int32_t *index;   // z-buffer winners, rows*cols
+  const float *depth;     // their depths
+  int *tgt, *cnt, *off, *fill, *list, *keep, *pos;
+  void *scan_temp;
+  size_t scan_temp_bytes;
+  float4 *o_pts, *o_nrm, *o_omg;
+  float *o_eig;
+  float4 *o_gauss;
+  int *out_count;
+};
+size_t merge_scan_temp_bytes(int n);
+int launch_merge(const MergeArgs &a, cudaStream_t s);
+
 }  // namespace nicp

@@ -541,6 +541,68 @@ template <class S> static inline S cast_depth(float scale, uint16_t u) {
   return S(scale) * S((int)u);
 }
 
+// Cloud::transformInPlace (cloud.cpp:191-204), with the Gaussians moved as
+// Gaussian3fVector::transformInPlace does (gaussian3.h:66-73).  Row 3 of m is
+// forced to (0 0 0 1); the identity leaves the cloud untouched.
+template <class S> static void transform_in_place(Cloud<S> &c, M4<S> m) {
+  Cloud<S> *cl = &c;
+  const int count = c.n;
+  set_row3(m);
+  bool ident = true;
+  M4<S> I4 = M4<S>::identity();
+  for (int i = 0; i < 16; i++) ident = ident && (m.a[i] == I4.a[i]);
+  if (ident) return;
+  M4<S> Tr = m;
+  for (int i = 0; i < 4; i++) { Tr(3, i) = S(0); Tr(i, 3) = S(0); }
+  M4<S> Trt = transpose(Tr);
+  for (int i = 0; i < count; i++) {
+    cl->points[i] = mv(m, cl->points[i]);
+    cl->points[i][3] = S(1);
+    cl->normals[i] = mv(m, cl->normals[i]);
+    cl->normals[i][3] = S(0);
+    M4<S> U = M4<S>::zero();
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) U(a, b) = cl->eigvec[9 * i + a * 3 + b];
+    M4<S> RU = mm(m, U);
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) cl->eigvec[9 * i + a * 3 + b] = RU(a, b);
+    // Gaussian3fVector::transformInPlace (gaussian3.h:66-73):
+    // mean' = R mean + t, covariance' = (R C) R^T
+    {
+      S *gm = &cl->gauss_mean[3 * (size_t)i], *gc = &cl->gauss_cov[9 * (size_t)i];
+      S mo[3], RC[9];
+      for (int a = 0; a < 3; a++) {
+        S v = m(a, 0) * gm[0];
+        v = v + m(a, 1) * gm[1];
+        v = v + m(a, 2) * gm[2];
+        mo[a] = v + m(a, 3);
+      }
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+          S v = m(a, 0) * gc[0 * 3 + b];
+          v = v + m(a, 1) * gc[1 * 3 + b];
+          RC[a * 3 + b] = v + m(a, 2) * gc[2 * 3 + b];
+        }
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+          S v = RC[a * 3 + 0] * m(b, 0);
+          v = v + RC[a * 3 + 1] * m(b, 1);
+          gc[a * 3 + b] = v + RC[a * 3 + 2] * m(b, 2);
+        }
+      for (int k = 0; k < 3; k++) gm[k] = mo[k];
+    }
+    for (int which = 0; which < 2; which++) {
+      S *om = which ? &cl->omega_n[9 * i] : &cl->omega_p[9 * i];
+      M4<S> O = M4<S>::zero();
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) O(a, b) = om[a * 3 + b];
+      M4<S> R = mm(mm(Tr, O), Trt);
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) om[a * 3 + b] = R(a, b);
+    }
+  }
+}
+
 // DepthImageConverterIntegralImage::compute (depthimageconverterintegralimage.cpp:18-64).
 template <class S>
 static Cloud<S> *build_cloud(const uint16_t *depth, int rows, int cols, const orc_camera &cam,
@@ -651,61 +713,7 @@ static Cloud<S> *build_cloud(const uint16_t *depth, int rows, int cols, const or
   if (offset) {
     M4<S> m;
     for (int i = 0; i < 16; i++) m.a[i] = S(offset[i]);
-    set_row3(m);
-    bool ident = true;
-    M4<S> I4 = M4<S>::identity();
-    for (int i = 0; i < 16; i++) ident = ident && (m.a[i] == I4.a[i]);
-    if (!ident) {
-      M4<S> Tr = m;
-      for (int i = 0; i < 4; i++) { Tr(3, i) = S(0); Tr(i, 3) = S(0); }
-      M4<S> Trt = transpose(Tr);
-      for (int i = 0; i < count; i++) {
-        cl->points[i] = mv(m, cl->points[i]);
-        cl->points[i][3] = S(1);
-        cl->normals[i] = mv(m, cl->normals[i]);
-        cl->normals[i][3] = S(0);
-        M4<S> U = M4<S>::zero();
-        for (int a = 0; a < 3; a++)
-          for (int b = 0; b < 3; b++) U(a, b) = cl->eigvec[9 * i + a * 3 + b];
-        M4<S> RU = mm(m, U);
-        for (int a = 0; a < 3; a++)
-          for (int b = 0; b < 3; b++) cl->eigvec[9 * i + a * 3 + b] = RU(a, b);
-        // Gaussian3fVector::transformInPlace (gaussian3.h:66-73):
-        // mean' = R mean + t, covariance' = (R C) R^T
-        {
-          S *gm = &cl->gauss_mean[3 * (size_t)i], *gc = &cl->gauss_cov[9 * (size_t)i];
-          S mo[3], RC[9];
-          for (int a = 0; a < 3; a++) {
-            S v = m(a, 0) * gm[0];
-            v = v + m(a, 1) * gm[1];
-            v = v + m(a, 2) * gm[2];
-            mo[a] = v + m(a, 3);
-          }
-          for (int a = 0; a < 3; a++)
-            for (int b = 0; b < 3; b++) {
-              S v = m(a, 0) * gc[0 * 3 + b];
-              v = v + m(a, 1) * gc[1 * 3 + b];
-              RC[a * 3 + b] = v + m(a, 2) * gc[2 * 3 + b];
-            }
-          for (int a = 0; a < 3; a++)
-            for (int b = 0; b < 3; b++) {
-              S v = RC[a * 3 + 0] * m(b, 0);
-              v = v + RC[a * 3 + 1] * m(b, 1);
-              gc[a * 3 + b] = v + RC[a * 3 + 2] * m(b, 2);
-            }
-          for (int k = 0; k < 3; k++) gm[k] = mo[k];
-        }
-        for (int which = 0; which < 2; which++) {
-          S *om = which ? &cl->omega_n[9 * i] : &cl->omega_p[9 * i];
-          M4<S> O = M4<S>::zero();
-          for (int a = 0; a < 3; a++)
-            for (int b = 0; b < 3; b++) O(a, b) = om[a * 3 + b];
-          M4<S> R = mm(mm(Tr, O), Trt);
-          for (int a = 0; a < 3; a++)
-            for (int b = 0; b < 3; b++) om[a * 3 + b] = R(a, b);
-        }
-      }
-    }
+    transform_in_place(*cl, m);
   }
   if (index_out) std::memcpy(index_out, index.data(), NP * sizeof(int32_t));
   return cl;
@@ -1164,6 +1172,140 @@ void orc_cloud_free(orc_cloud *c) {
 }
 
 int orc_cloud_size(const orc_cloud *c) { return c->mode == ORC_F64 ? c->d->n : c->f->n; }
+
+// Cloud::add (cloud.cpp:163-189): `src` is transformed in place by T, then
+// appended to `dst`.
+template <class S> static void cloud_add(Cloud<S> &dst, Cloud<S> &src, const M4<S> &T) {
+  transform_in_place(src, T);
+  Cloud<S> out = dst;
+  const int a = dst.n, b = src.n;
+  out.n = a + b;
+  auto cat = [](std::vector<S> &x, const std::vector<S> &y) { x.insert(x.end(), y.begin(), y.end()); };
+  out.points.insert(out.points.end(), src.points.begin(), src.points.end());
+  out.normals.insert(out.normals.end(), src.normals.begin(), src.normals.end());
+  cat(out.curvature, src.curvature);
+  cat(out.eigval, src.eigval);
+  cat(out.eigvec, src.eigvec);
+  cat(out.omega_p, src.omega_p);
+  cat(out.omega_n, src.omega_n);
+  cat(out.gauss_cov, src.gauss_cov);
+  cat(out.gauss_mean, src.gauss_mean);
+  out.stats_n.insert(out.stats_n.end(), src.stats_n.begin(), src.stats_n.end());
+  dst = out;
+}
+
+// Gaussian<float,3>::_updateInfo (gaussian.h): information matrix = C^-1,
+// information vector = (C^-1) mean; products in the order written.
+template <class S> static void gaussian_info(const S C[9], const S mean[3], S Om[9], S eta[3]) {
+  inv3(C, Om);
+  for (int a = 0; a < 3; a++) {
+    S v = Om[a * 3 + 0] * mean[0];
+    v = v + Om[a * 3 + 1] * mean[1];
+    eta[a] = v + Om[a * 3 + 2] * mean[2];
+  }
+}
+
+// Merger::merge (merger.cpp:15-109).  Project the cloud with `T` (serial
+// z-buffer, as PinholePointProjector::project); then, point by point in
+// index order: a point that wins its own pixel is kept ("collapsed" onto
+// itself); a point whose depth is within `dthr` of the pixel's winner adds
+// its information (Gaussian3f::addInformation) to the winner and is
+// removed.  Survivors that won their pixel take the mean of their (fused)
+// Gaussian as their position; the cloud is compacted in index order.
+// Returns the number of removed points.
+template <class S> static int merge(Cloud<S> &c, const orc_camera &cam, const M4<S> &T, S dthr, S maxd) {
+  Projector<S> P = make_projector<S>(cam, T);
+  const size_t NP = (size_t)P.rows * P.cols;
+  std::vector<int32_t> index(NP);
+  std::vector<S> depth(NP);
+  project(c, P, index.data(), depth.data());
+  const int n = c.n;
+  std::vector<int> collapsed(n, -1);
+  std::vector<char> info(n, 0);
+  std::vector<S> Om(9 * (size_t)n), eta(3 * (size_t)n);
+  auto update_info = [&](int i) {
+    if (info[i]) return;
+    gaussian_info(&c.gauss_cov[9 * (size_t)i], &c.gauss_mean[3 * (size_t)i], &Om[9 * (size_t)i], &eta[3 * (size_t)i]);
+    info[i] = 1;
+  };
+  for (int i = 0; i < n; i++) {
+    int x = -1, y = -1;
+    S d = S(0);
+    if (!project_point(P, c.points[i], x, y, d)) continue;  // x, y stay -1 in the reference
+    if (d < S(0) || d > maxd || y < 0 || y >= P.rows || x < 0 || x >= P.cols) continue;
+    const size_t pix = (size_t)y * P.cols + x;
+    const int target = index[pix];
+    if (target < 0) continue;
+    if (target == i) {
+      collapsed[i] = i;
+    } else if (std::fabs(d - depth[pix]) < dthr) {
+      update_info(target);
+      S Oi[9], ei[3];
+      gaussian_info(&c.gauss_cov[9 * (size_t)i], &c.gauss_mean[3 * (size_t)i], Oi, ei);
+      for (int k = 0; k < 9; k++) Om[9 * (size_t)target + k] = Om[9 * (size_t)target + k] + Oi[k];
+      for (int k = 0; k < 3; k++) eta[3 * (size_t)target + k] = eta[3 * (size_t)target + k] + ei[k];
+      collapsed[i] = target;
+    }
+  }
+  // Gaussian3f::_updateMoments for the fused ones: C = Om^-1, mean = C eta
+  for (int i = 0; i < n; i++) {
+    if (!info[i]) continue;
+    S Cn[9], mn[3];
+    inv3(&Om[9 * (size_t)i], Cn);
+    for (int a = 0; a < 3; a++) {
+      S v = Cn[a * 3 + 0] * eta[3 * (size_t)i + 0];
+      v = v + Cn[a * 3 + 1] * eta[3 * (size_t)i + 1];
+      mn[a] = v + Cn[a * 3 + 2] * eta[3 * (size_t)i + 2];
+    }
+    for (int k = 0; k < 9; k++) c.gauss_cov[9 * (size_t)i + k] = Cn[k];
+    for (int k = 0; k < 3; k++) c.gauss_mean[3 * (size_t)i + k] = mn[k];
+  }
+  int k = 0, removed = 0;
+  for (int i = 0; i < n; i++) {
+    if (collapsed[i] == i)
+      for (int a = 0; a < 3; a++) c.points[i][a] = c.gauss_mean[3 * (size_t)i + a];
+    if (collapsed[i] < 0 || collapsed[i] == i) {
+      c.points[k] = c.points[i];
+      c.normals[k] = c.normals[i];
+      c.curvature[k] = c.curvature[i];
+      c.stats_n[k] = c.stats_n[i];
+      for (int a = 0; a < 3; a++) c.eigval[3 * (size_t)k + a] = c.eigval[3 * (size_t)i + a];
+      for (int a = 0; a < 9; a++) {
+        c.eigvec[9 * (size_t)k + a] = c.eigvec[9 * (size_t)i + a];
+        c.omega_p[9 * (size_t)k + a] = c.omega_p[9 * (size_t)i + a];
+        c.omega_n[9 * (size_t)k + a] = c.omega_n[9 * (size_t)i + a];
+        c.gauss_cov[9 * (size_t)k + a] = c.gauss_cov[9 * (size_t)i + a];
+      }
+      for (int a = 0; a < 3; a++) c.gauss_mean[3 * (size_t)k + a] = c.gauss_mean[3 * (size_t)i + a];
+      k++;
+    } else {
+      removed++;
+    }
+  }
+  c.points.resize(k); c.normals.resize(k); c.curvature.resize(k); c.stats_n.resize(k);
+  c.eigval.resize(3 * (size_t)k); c.eigvec.resize(9 * (size_t)k);
+  c.omega_p.resize(9 * (size_t)k); c.omega_n.resize(9 * (size_t)k);
+  c.gauss_cov.resize(9 * (size_t)k); c.gauss_mean.resize(3 * (size_t)k);
+  c.n = k;
+  return removed;
+}
+
+void orc_cloud_transform(orc_cloud *c, const double *T16) {
+  if (c->mode == ORC_F64) transform_in_place(*c->d, load_T<double>(T16));
+  else transform_in_place(*c->f, load_T<float>(T16));
+}
+
+void orc_cloud_add(orc_cloud *dst, orc_cloud *src, const double *T16) {
+  if (dst->mode == ORC_F64) cloud_add(*dst->d, *src->d, load_T<double>(T16));
+  else cloud_add(*dst->f, *src->f, load_T<float>(T16));
+}
+
+int orc_merge(int mode, orc_cloud *c, const orc_camera *cam, const double *T16, double distance_threshold,
+              double max_point_depth) {
+  if (mode == ORC_F64)
+    return merge(*c->d, *cam, load_T<double>(T16), distance_threshold, max_point_depth);
+  return merge(*c->f, *cam, load_T<float>(T16), (float)distance_threshold, (float)max_point_depth);
+}
 
 template <class S> static int cloud_get(const Cloud<S> &c, int field, double *out) {
   int n = c.n;

@@ -92,6 +92,15 @@ orc_cloud *orc_cloud_from_arrays(int mode, int n, const double *points4, const d
                                  const double *omega_n9);
 void orc_cloud_free(orc_cloud *c);
 int orc_cloud_size(const orc_cloud *c);
+/* Cloud::transformInPlace (cloud.cpp:191-204, gaussian3.h:66-73). */
+void orc_cloud_transform(orc_cloud *c, const double *T16);
+/* Cloud::add (cloud.cpp:163-189): transforms src in place, appends it to dst
+ * (both of the same mode). */
+void orc_cloud_add(orc_cloud *dst, orc_cloud *src, const double *T16);
+/* Merger::merge (merger.cpp:15-109) with the projector of `cam` moved by T16;
+ * returns the number of points removed. */
+int orc_merge(int mode, orc_cloud *c, const orc_camera *cam, const double *T16, double distance_threshold,
+              double max_point_depth);
 /* field: 0 points(4n) 1 normals(4n) 2 curvature(n) 3 omega_p(9n) 4 omega_n(9n)
  *        5 eigenvalues(3n) 6 eigenvectors(9n, row-major 3x3, columns = vectors)
  *        7 stats_n(n) 8 gaussian covariance (9n) 9 gaussian mean (3n) */

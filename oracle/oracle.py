@@ -79,6 +79,9 @@ def load():
         "orc_cloud_from_arrays": (P, [C.c_int, C.c_int, dp, dp, dp, dp, dp]),
         "orc_cloud_free": (None, [P]),
         "orc_cloud_size": (C.c_int, [P]),
+        "orc_cloud_transform": (None, [P, dp]),
+        "orc_cloud_add": (None, [P, P, dp]),
+        "orc_merge": (C.c_int, [C.c_int, P, C.POINTER(Camera), dp, C.c_double, C.c_double]),
         "orc_cloud_get": (C.c_int, [P, C.c_int, dp]),
         "orc_projector_matrices": (None, [C.c_int, C.POINTER(Camera), dp, dp, dp]),
         "orc_project": (None, [C.c_int, P, C.POINTER(Camera), dp, ip, dp]),
@@ -241,6 +244,24 @@ def linearize(mode, ref, cur, pairs, T, prm=None):
     load().orc_linearize(mode, ref.h, cur.h, pairs.ctypes.data_as(ip), len(pairs), _d(T), C.byref(prm),
                          H.ctypes.data_as(dp), b.ctypes.data_as(dp), err.ctypes.data_as(dp), C.byref(inl))
     return H.reshape(6, 6), b, float(err[0]), inl.value
+
+
+def cloud_transform(cloud, T):
+    """Cloud::transformInPlace (cloud.cpp:191-204)."""
+    load().orc_cloud_transform(cloud.h, _d(T))
+
+
+def cloud_add(dst, src, T):
+    """Cloud::add (cloud.cpp:163-189): src is transformed in place by T and
+    appended to dst."""
+    _same_mode(dst.mode, src)
+    load().orc_cloud_add(dst.h, src.h, _d(T))
+
+
+def merge(mode, cloud, cam, T, distance_threshold=0.1, max_point_depth=10.0):
+    """Merger::merge (merger.cpp:15-109); returns the number of removed points."""
+    _same_mode(mode, cloud)
+    return load().orc_merge(mode, cloud.h, C.byref(cam), _d(T), distance_threshold, max_point_depth)
 
 
 def align(mode, ref, cur, cam, guess=None, ref_offset=None, cur_offset=None, prm=None, statistics=False):
