@@ -221,6 +221,19 @@ int nicp_cloud_upload(nicp_cloud *c, int n, const float *points4, const float *n
 /* Cloud::transformInPlace (cloud.cpp:191-204). */
 int nicp_cloud_transform(nicp_cloud *c, const float T16[16]);
 
+/* DepthImage_scale (imageutils.cpp:6-37; used with
+ * DepthImage_convert_16UC1_to_32FC1, imageutils.cpp:85-99, and
+ * PinholePointProjector::scale, pinholepointprojector.cpp:150-155, for
+ * coarse input): out[(rows/step) x (cols/step)] float metres, each pixel the
+ * mean of its step x step block's positive depths, 0 when the block has none
+ * or their variance exceeds max_depth_cov (reference default 0.01).  `depth`
+ * is u16 (times depth_scale) when is_u16, else float metres; row pitch in
+ * bytes (0 = packed); input and output each in host or device memory.  Feed
+ * the result to nicp_cloud_from_depth_f32 with a camera whose `scaling` is
+ * 1/step. */
+int nicp_depth_scale(nicp_ctx *ctx, const void *depth, int is_u16, int rows, int cols, size_t pitch_bytes,
+                     int on_device, float depth_scale, int step, float max_depth_cov, float *out, int out_on_device);
+
 /* Cloud::add (cloud.cpp:163-189): `src` is first transformed in place by T16
  * (NULL = identity), as the reference does, then its points are appended to
  * `dst` (grown as needed).  Stats, Gaussians and the structured-Omega flag

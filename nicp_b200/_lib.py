@@ -109,6 +109,8 @@ SIGNATURES = {
     "nicp_cloud_upload": (C.c_int, [P, C.c_int, f32p, f32p, f32p, f32p, f32p]),
     "nicp_cloud_transform": (C.c_int, [P, f32p]),
     "nicp_cloud_add": (C.c_int, [P, P, f32p]),
+    "nicp_depth_scale": (C.c_int, [P, P, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_float, C.c_int, C.c_float,
+                                   P, C.c_int]),
     "nicp_merge": (C.c_int, [P, P, C.POINTER(Camera), f32p, C.c_float, C.c_float, C.POINTER(C.c_int)]),
     "nicp_cloud_from_depth_u16": (C.c_int, [P, P, C.c_int, C.c_int, C.c_size_t, C.c_int, C.POINTER(Camera),
                                             C.POINTER(CloudParams), f32p, P, i32p]),

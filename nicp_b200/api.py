@@ -427,6 +427,30 @@ class DepthImageConverterIntegralImage:
 
 
 # ------------------------------------------------------------------ registration
+def DepthImage_scale(depth, step, maxDepthCov=0.01, depthScale=0.001, ctx=None):
+    """DepthImage_scale (imageutils.cpp:6-37) on the GPU: a (rows/step) x
+    (cols/step) float image (metres), each pixel the mean of its block's
+    positive depths, 0 when the block has none or their variance exceeds
+    maxDepthCov.  `depth`: uint16 (times depthScale, i.e. with
+    DepthImage_convert_16UC1_to_32FC1 fused in front) or float32 metres.
+    Use it with a projector scaled by 1/step (PinholePointProjector.scale)."""
+    ctx = ctx or Context.default()
+    d = np.ascontiguousarray(depth)
+    if d.dtype not in (np.uint16, np.float32):
+        raise TypeError("depth must be uint16 or float32")
+    rows, cols = d.shape
+    out = np.zeros((rows // step, cols // step), np.float32)
+    ctx.check(ctx.lib.nicp_depth_scale(ctx.h, d.ctypes.data_as(C.c_void_p), 1 if d.dtype == np.uint16 else 0, rows,
+                                       cols, 0, 0, float(depthScale), int(step), float(maxDepthCov),
+                                       out.ctypes.data_as(C.c_void_p), 0))
+    return out
+
+
+def DepthImage_convert_16UC1_to_32FC1(depth_u16, scale=0.001, ctx=None):
+    """imageutils.cpp:85-99 on the GPU: u16 -> float metres (0 stays 0)."""
+    return DepthImage_scale(np.ascontiguousarray(depth_u16, np.uint16), 1, 0.01, scale, ctx)
+
+
 class Merger:
     """merger.{h,cpp}: fuses the points of a cloud that land on the same pixel
     of a view (Gaussian information fusion) and removes the absorbed ones.

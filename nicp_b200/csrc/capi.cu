@@ -1022,6 +1022,47 @@ extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_c
   return NICP_OK;
 }
 
+// ------------------------------------------------------------------ multi-resolution input
+extern "C" int nicp_depth_scale(nicp_ctx *ctx, const void *depth, int is_u16, int rows, int cols, size_t pitch_bytes,
+                                int on_device, float depth_scale, int step, float max_depth_cov, float *out,
+                                int out_on_device) {
+  if (!ctx || !depth || !out || rows <= 0 || cols <= 0 || step < 1) return NICP_EINVAL;
+  const size_t elem = is_u16 ? 2 : 4;
+  if (pitch_bytes == 0) pitch_bytes = elem * (size_t)cols;
+  if (pitch_bytes < elem * (size_t)cols || pitch_bytes % elem) return fail(ctx, NICP_EINVAL, "bad row pitch");
+  const int orows = rows / step, ocols = cols / step;
+  const size_t in_bytes = pitch_bytes * (size_t)rows, out_bytes = 4 * (size_t)orows * ocols;
+  if (orows == 0 || ocols == 0) return NICP_OK;
+  Layout L;
+  size_t o_in = L.take(on_device ? 1 : in_bytes), o_out = L.take(out_on_device ? 1 : out_bytes);
+  int rc;
+  if ((rc = ensure_ws(ctx, L.off))) return rc;
+  cudaStream_t s = ctx->stream;
+  const void *src = depth;
+  if (!on_device) {
+    char *pin;
+    if ((rc = pin_up(ctx, in_bytes, &pin))) return rc;
+    std::memcpy(pin, depth, in_bytes);
+    CK(ctx, cudaMemcpyAsync(ctx->ws + o_in, pin, in_bytes, cudaMemcpyHostToDevice, s));
+    CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+    ctx->h2d_bytes += in_bytes;
+    src = ctx->ws + o_in;
+  }
+  float *dst = out_on_device ? out : (float *)(ctx->ws + o_out);
+  launch_depth_scale(is_u16 ? (const uint16_t *)src : nullptr, is_u16 ? nullptr : (const float *)src,
+                     pitch_bytes / elem, rows, cols, depth_scale, step, max_depth_cov, dst, s);
+  CK(ctx, cudaGetLastError());
+  if (!out_on_device) {
+    char *pin;
+    if ((rc = pin_down(ctx, out_bytes, &pin))) return rc;
+    CK(ctx, cudaMemcpyAsync(pin, dst, out_bytes, cudaMemcpyDeviceToHost, s));
+    CK(ctx, cudaStreamSynchronize(s));
+    std::memcpy(out, pin, out_bytes);
+    ctx->d2h_bytes += out_bytes;
+  }
+  return NICP_OK;
+}
+
 // ------------------------------------------------------------------ scene
 // Grows a cloud's allocation to `capacity` points keeping its first n
 // points (all arrays) and its counts.

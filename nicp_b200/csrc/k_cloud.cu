@@ -586,6 +586,51 @@ void launch_intervals(const float *d_depth, int P, const float *d_K9, float min_
   prof->end(NICP_K_STATS, s);
 }
 
+// DepthImage_scale (imageutils.cpp:6-37), with the u16 -> float conversion
+// of DepthImage_convert_16UC1_to_32FC1 (imageutils.cpp:85-99) fused in front
+// when the input is u16.  One thread per output pixel; sums and the variance
+// test in the reference's order, single-rounded.
+__global__ void k_depth_scale(const uint16_t *__restrict__ u16, const float *__restrict__ f32, size_t pitch_elems,
+                              int rows, int cols, float depth_scale, int step, float max_cov, float *__restrict__ out,
+                              int out_rows, int out_cols) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= out_rows * out_cols) return;
+  const int r = idx / out_cols, c = idx - r * out_cols;
+  const int sr = r * step, sc = c * step;
+  float acc = 0.0f, acc2 = 0.0f;
+  int np = 0;
+  for (int i = 0; i < step; i++)
+    for (int j = 0; j < step; j++) {
+      if (sr + i >= rows || sc + j >= cols) continue;
+      const size_t at = (size_t)(sr + i) * pitch_elems + sc + j;
+      float f;
+      if (u16) {
+        const uint16_t u = u16[at];
+        f = u ? fm(depth_scale, (float)(int)u) : 0.0f;
+      } else {
+        f = f32[at];
+      }
+      acc = fa(acc, f);
+      acc2 = fa(acc2, fm(f, f));
+      np += f > 0.0f;
+    }
+  float v = 0.0f;
+  if (np) {
+    const float mu = __fdiv_rn(acc, (float)np);
+    const float sigma = fsb(__fdiv_rn(acc2, (float)np), fm(mu, mu));
+    if (!(sigma > max_cov)) v = mu;
+  }
+  out[idx] = v;
+}
+
+void launch_depth_scale(const uint16_t *u16, const float *f32, size_t pitch_elems, int rows, int cols,
+                        float depth_scale, int step, float max_cov, float *out, cudaStream_t s) {
+  const int orows = rows / step, ocols = cols / step, n = orows * ocols;
+  if (n > 0)
+    k_depth_scale<<<(n + 255) / 256, 256, 0, s>>>(u16, f32, pitch_elems, rows, cols, depth_scale, step, max_cov, out,
+                                                  orows, ocols);
+}
+
 void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof) {
   prof->begin(NICP_K_UNPROJECT, s);
   k_unproject_count<<<total_tiles, 256, 0, s>>>(d_frames, nframes);

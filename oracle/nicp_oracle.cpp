@@ -606,11 +606,12 @@ template <class S> static void transform_in_place(Cloud<S> &c, M4<S> m) {
 // DepthImageConverterIntegralImage::compute (depthimageconverterintegralimage.cpp:18-64).
 template <class S>
 static Cloud<S> *build_cloud(const uint16_t *depth, int rows, int cols, const orc_camera &cam,
-                             const orc_cloud_params &prm, const double *offset, int32_t *index_out) {
+                             const orc_cloud_params &prm, const double *offset, int32_t *index_out,
+                             const float *depth_f32 = nullptr) {
   Projector<S> P = make_projector<S>(cam, M4<S>::identity());
   size_t NP = (size_t)rows * cols;
   std::vector<S> d(NP);
-  for (size_t i = 0; i < NP; i++) d[i] = cast_depth<S>(prm.depth_scale, depth[i]);
+  for (size_t i = 0; i < NP; i++) d[i] = depth_f32 ? S(depth_f32[i]) : cast_depth<S>(prm.depth_scale, depth[i]);
   std::vector<int32_t> index(NP);
   auto *cl = new Cloud<S>();
   // unProject with Gaussians (pinholepointprojector.cpp:93-134)
@@ -1127,6 +1128,43 @@ template <> Cloud<double> *get<double>(const orc_cloud *c) { return c->d; }
 
 void orc_convert_u16(const uint16_t *src, int rows, int cols, float scale, float *dst) {
   for (size_t i = 0; i < (size_t)rows * cols; i++) dst[i] = cast_depth<float>(scale, src[i]);
+}
+
+// DepthImage_scale (imageutils.cpp:6-37): each output pixel is the mean of
+// the step x step block's positive depths (zeros add nothing to the sums but
+// are not counted), or 0 when the block has none or its variance
+// acc2/np - mu^2 exceeds max_cov.  Float, in the reference's loop order.
+void orc_depth_scale(const float *src, int rows, int cols, int step, float max_cov, float *dst) {
+  const int R = rows / step, Cn = cols / step;
+  for (int r = 0; r < R; r++)
+    for (int c = 0; c < Cn; c++) {
+      float acc = 0, acc2 = 0;
+      int np = 0;
+      const int sr = r * step, sc = c * step;
+      for (int i = 0; i < step; i++)
+        for (int j = 0; j < step; j++)
+          if (sr + i < rows && sc + j < cols) {
+            const float f = src[(size_t)(sr + i) * cols + sc + j];
+            acc += f;
+            acc2 += f * f;
+            np += f > 0;
+          }
+      float out = 0;
+      if (np) {
+        float mu = acc / np;
+        float sigma = acc2 / np - mu * mu;
+        if (!(sigma > max_cov)) out = mu;
+      }
+      dst[(size_t)r * Cn + c] = out;
+    }
+}
+
+orc_cloud *orc_cloud_build_f32(int mode, const float *depth, int rows, int cols, const orc_camera *cam,
+                               const orc_cloud_params *prm, const double *offset, int32_t *index_out) {
+  auto *c = new orc_cloud{mode, nullptr, nullptr};
+  if (mode == ORC_F64) c->d = build_cloud<double>(nullptr, rows, cols, *cam, *prm, offset, index_out, depth);
+  else c->f = build_cloud<float>(nullptr, rows, cols, *cam, *prm, offset, index_out, depth);
+  return c;
 }
 
 orc_cloud *orc_cloud_build_u16(int mode, const uint16_t *depth, int rows, int cols, const orc_camera *cam,

@@ -85,6 +85,10 @@ orc_cloud *orc_cloud_build_u16(int mode, const uint16_t *depth, int rows, int co
                                const orc_camera *cam, const orc_cloud_params *prm,
                                const double *sensor_offset, int32_t *index_out);
 
+/* The same from a float depth image in metres (DepthImage). */
+orc_cloud *orc_cloud_build_f32(int mode, const float *depth, int rows, int cols, const orc_camera *cam,
+                               const orc_cloud_params *prm, const double *offset, int32_t *index_out);
+
 /* A cloud assembled from arrays (for feeding the oracle the GPU's own
  * cloud).  points4/normals4: n*4; omega_p9/omega_n9: n*9 (3x3 row-major). */
 orc_cloud *orc_cloud_from_arrays(int mode, int n, const double *points4, const double *normals4,
@@ -92,6 +96,8 @@ orc_cloud *orc_cloud_from_arrays(int mode, int n, const double *points4, const d
                                  const double *omega_n9);
 void orc_cloud_free(orc_cloud *c);
 int orc_cloud_size(const orc_cloud *c);
+/* DepthImage_scale (imageutils.cpp:6-37), float; dst: (rows/step) x (cols/step). */
+void orc_depth_scale(const float *src, int rows, int cols, int step, float max_cov, float *dst);
 /* Cloud::transformInPlace (cloud.cpp:191-204, gaussian3.h:66-73). */
 void orc_cloud_transform(orc_cloud *c, const double *T16);
 /* Cloud::add (cloud.cpp:163-189): transforms src in place, appends it to dst

@@ -76,10 +76,13 @@ def load():
         "orc_convert_u16": (None, [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_float, C.POINTER(C.c_float)]),
         "orc_cloud_build_u16": (P, [C.c_int, C.POINTER(C.c_uint16), C.c_int, C.c_int, C.POINTER(Camera),
                                     C.POINTER(CloudParams), dp, ip]),
+        "orc_cloud_build_f32": (P, [C.c_int, C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(Camera),
+                                    C.POINTER(CloudParams), dp, ip]),
         "orc_cloud_from_arrays": (P, [C.c_int, C.c_int, dp, dp, dp, dp, dp]),
         "orc_cloud_free": (None, [P]),
         "orc_cloud_size": (C.c_int, [P]),
         "orc_cloud_transform": (None, [P, dp]),
+        "orc_depth_scale": (None, [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(C.c_float)]),
         "orc_cloud_add": (None, [P, P, dp]),
         "orc_merge": (C.c_int, [C.c_int, P, C.POINTER(Camera), dp, C.c_double, C.c_double]),
         "orc_cloud_get": (C.c_int, [P, C.c_int, dp]),
@@ -202,6 +205,17 @@ def build_cloud(mode, depth_u16, cam, prm=None, sensor_offset=None):
     return Cloud(h, mode), index
 
 
+def build_cloud_f32(mode, depth_f32, cam, prm=None, sensor_offset=None):
+    """DepthImageConverterIntegralImage::compute on a float depth image (metres)."""
+    depth = np.ascontiguousarray(depth_f32, dtype=np.float32)
+    rows, cols = depth.shape
+    prm = prm or cloud_params()
+    index = np.zeros((rows, cols), dtype=np.int32)
+    h = load().orc_cloud_build_f32(mode, depth.ctypes.data_as(C.POINTER(C.c_float)), rows, cols, C.byref(cam),
+                                   C.byref(prm), _d(sensor_offset), index.ctypes.data_as(ip))
+    return Cloud(h, mode), index
+
+
 def projector_matrices(mode, cam, T=None):
     K, iK = np.zeros(16), np.zeros(16)
     load().orc_projector_matrices(mode, C.byref(cam), _d(T), K.ctypes.data_as(dp), iK.ctypes.data_as(dp))
@@ -244,6 +258,25 @@ def linearize(mode, ref, cur, pairs, T, prm=None):
     load().orc_linearize(mode, ref.h, cur.h, pairs.ctypes.data_as(ip), len(pairs), _d(T), C.byref(prm),
                          H.ctypes.data_as(dp), b.ctypes.data_as(dp), err.ctypes.data_as(dp), C.byref(inl))
     return H.reshape(6, 6), b, float(err[0]), inl.value
+
+
+def depth_scale(depth_f32, step, max_depth_cov=0.01):
+    """DepthImage_scale (imageutils.cpp:6-37) of a float depth image."""
+    d = np.ascontiguousarray(depth_f32, dtype=np.float32)
+    rows, cols = d.shape
+    out = np.zeros((rows // step, cols // step), np.float32)
+    load().orc_depth_scale(d.ctypes.data_as(C.POINTER(C.c_float)), rows, cols, step, max_depth_cov,
+                           out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def convert_u16(depth_u16, scale=0.001):
+    """DepthImage_convert_16UC1_to_32FC1 (imageutils.cpp:85-99)."""
+    d = np.ascontiguousarray(depth_u16, dtype=np.uint16)
+    out = np.zeros(d.shape, np.float32)
+    load().orc_convert_u16(d.ctypes.data_as(C.POINTER(C.c_uint16)), d.shape[0], d.shape[1], np.float32(scale),
+                           out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
 
 
 def cloud_transform(cloud, T):
