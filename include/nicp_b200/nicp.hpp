@@ -46,6 +46,11 @@ struct Isometry3f {
   float &operator()(int r, int c) { return m[r * 4 + c]; }
   float operator()(int r, int c) const { return m[r * 4 + c]; }
   const float *data() const { return m; }
+  static Isometry3f fromArray(const float a[16]) {
+    Isometry3f r;
+    for (int i = 0; i < 16; i++) r.m[i] = a[i];
+    return r;
+  }
   Isometry3f operator*(const Isometry3f &o) const {
     Isometry3f r;
     for (int i = 0; i < 4; i++)
@@ -129,6 +134,17 @@ class Cloud {
     check(ctx_->handle(), nicp_cloud_download_gaussians(h_, means.data(), covariances.data()));
   }
   void transformInPlace(const Isometry3f &T) { check(ctx_->handle(), nicp_cloud_transform(h_, T.data())); }
+  // save(filename, T, step, binary) / load(T, filename) (cloud.cpp:13-150): the .nicp format.
+  bool save(const char *filename, const Isometry3f &T = Isometry3f::Identity(), int step = 1,
+            bool binary = true) const {
+    return nicp_cloud_save(h_, filename, T.data(), step, binary ? 1 : 0) == NICP_OK;
+  }
+  bool load(Isometry3f &T, const char *filename) {
+    float t[16];
+    if (nicp_cloud_load(h_, filename, nullptr, t, nullptr) != NICP_OK) return false;
+    T = Isometry3f::fromArray(t);
+    return true;
+  }
   // add(cloud, T) (cloud.cpp:163-189): `cloud` is transformed in place, then appended.
   void add(Cloud &cloud, const Isometry3f &T = Isometry3f::Identity()) {
     check(ctx_->handle(), nicp_cloud_add(h_, cloud.h_, T.data()));

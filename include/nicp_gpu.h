@@ -211,6 +211,12 @@ int nicp_cloud_size(nicp_cloud *c, int *n);
  * NICP_ESTATE when the cloud was not built with keep_gaussians. */
 int nicp_cloud_download_gaussians(nicp_cloud *cloud, float *mean3, float *cov9);
 
+/* The Stats of each point (stats.h:13-116; kept with keep_stats): eigenvalues
+ * (n*3, ascending), eigenvectors (n*9, row-major, columns are the vectors),
+ * the window mean (n*3) and the window's point count (n; 0 where the stats
+ * calculator did not reach the pixel).  Any pointer may be NULL. */
+int nicp_cloud_download_stats(nicp_cloud *cloud, float *eigval3, float *eigvec9, float *mean3, int *n);
+
 /* Any output may be NULL.  points4/normals4: n*4 floats (w = 1 / 0);
  * curvature: n; omega_p9/omega_n9: n*9 (3x3 blocks); eigval3: n*3;
  * eigvec9: n*9 (columns are eigenvectors; needs keep_stats). */
@@ -220,6 +226,28 @@ int nicp_cloud_upload(nicp_cloud *c, int n, const float *points4, const float *n
                       const float *curvature, const float *omega_p9, const float *omega_n9);
 /* Cloud::transformInPlace (cloud.cpp:191-204). */
 int nicp_cloud_transform(nicp_cloud *c, const float T16[16]);
+
+/* Cloud::save (cloud.cpp:20-25,100-150): writes every step-th point in the
+ * reference's .nicp format -- header "NICPCLOUD <n/step> <binary>", t2v(T16)
+ * (NULL = identity), then per point text "POINTWITHSTATS x y z nx ny nz
+ * <Stats 4x4 row by row>" or binary Point (16 B), Normal (16 B) and the raw
+ * 96-byte Stats (4x4 column-major, int n, 3 eigenvalues, bool
+ * curvatureComputed at byte 80, float curvature at byte 84; padding zeroed).
+ * Stats come from keep_stats; a cloud built without them is written with
+ * zeroed Stats, as the reference writes a cloud with no stats. */
+int nicp_cloud_save(nicp_cloud *cloud, const char *filename, const float T16[16], int step, int binary);
+/* Cloud::load (cloud.cpp:13-18,42-98): reads a .nicp file (text or binary)
+ * into the cloud and its pose v2t(x) into T16_out (may be NULL).  The file
+ * holds points, normals and Stats only; the information matrices are
+ * recomputed from them with prm's calculators (NULL = defaults), as
+ * Point/NormalInformationMatrixCalculator::compute would.  *num_points: the
+ * points read.  NICP_EINVAL for a bad header or a short file. */
+int nicp_cloud_load(nicp_cloud *cloud, const char *filename, const nicp_cloud_params *prm, float T16_out[16],
+                    int *num_points);
+/* One line of the trajectory file of nicp_simple_aligner.cpp:175-181:
+ * "timestamp tx ty tz qx qy qz qw\n" (normalised quaternion of the rotation,
+ * numbers as iostream prints floats).  NICP_EINVAL if `capacity` is short. */
+int nicp_trajectory_line(const char *timestamp, const float T16[16], char *out, size_t capacity);
 
 /* DepthImage_scale (imageutils.cpp:6-37; used with
  * DepthImage_convert_16UC1_to_32FC1, imageutils.cpp:85-99, and

@@ -106,9 +106,13 @@ SIGNATURES = {
     "nicp_cloud_size": (C.c_int, [P, C.POINTER(C.c_int)]),
     "nicp_cloud_download": (C.c_int, [P, f32p, f32p, f32p, f32p, f32p, f32p, f32p]),
     "nicp_cloud_download_gaussians": (C.c_int, [P, f32p, f32p]),
+    "nicp_cloud_download_stats": (C.c_int, [P, f32p, f32p, f32p, i32p]),
     "nicp_cloud_upload": (C.c_int, [P, C.c_int, f32p, f32p, f32p, f32p, f32p]),
     "nicp_cloud_transform": (C.c_int, [P, f32p]),
     "nicp_cloud_add": (C.c_int, [P, P, f32p]),
+    "nicp_cloud_save": (C.c_int, [P, C.c_char_p, f32p, C.c_int, C.c_int]),
+    "nicp_cloud_load": (C.c_int, [P, C.c_char_p, C.POINTER(CloudParams), f32p, C.POINTER(C.c_int)]),
+    "nicp_trajectory_line": (C.c_int, [C.c_char_p, f32p, C.c_char_p, C.c_size_t]),
     "nicp_depth_scale": (C.c_int, [P, P, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_float, C.c_int, C.c_float,
                                    P, C.c_int]),
     "nicp_merge": (C.c_int, [P, P, C.POINTER(Camera), f32p, C.c_float, C.c_float, C.POINTER(C.c_int)]),

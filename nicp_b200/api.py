@@ -136,6 +136,15 @@ class Cloud:
             out["eigenvectors"] = U.reshape(n, 3, 3)
         return out
 
+    def stats(self):
+        """Stats per point (keep_stats): dict of eigenvalues (n x 3),
+        eigenvectors (n x 3 x 3, columns), mean (n x 3), n (window points)."""
+        k = self.size()
+        ev, U, m = np.zeros((k, 3), np.float32), np.zeros((k, 9), np.float32), np.zeros((k, 3), np.float32)
+        cnt = np.zeros(k, np.int32)
+        self.ctx.check(self.ctx.lib.nicp_cloud_download_stats(self.h, L.fptr(ev), L.fptr(U), L.fptr(m), L.iptr(cnt)))
+        return dict(eigenvalues=ev, eigenvectors=U.reshape(k, 3, 3), mean=m, n=cnt)
+
     def gaussians(self):
         """Cloud::gaussians() (cloud.h:107): (means n x 3, covariances n x 3 x 3);
         the cloud must have been built with keepGaussians."""
@@ -150,6 +159,24 @@ class Cloud:
 
     def normals(self):
         return self.download()["normals"]
+
+    def save(self, filename, T=None, step=1, binary=True):
+        """Cloud::save (cloud.cpp:20-25,100-150): the reference's .nicp file."""
+        self.ctx.check(self.ctx.lib.nicp_cloud_save(self.h, str(filename).encode(), L.fptr(L.f16(T)), int(step),
+                                                    1 if binary else 0))
+        return True
+
+    def load(self, filename, params=None):
+        """Cloud::load (cloud.cpp:13-18,42-98): returns the file's pose T; the
+        information matrices are recomputed with `params` (CloudParams,
+        default the calculators' defaults)."""
+        T = np.zeros(16, np.float32)
+        n = C.c_int(0)
+        self.ctx.check(self.ctx.lib.nicp_cloud_load(self.h, str(filename).encode(),
+                                                    C.byref(params) if params is not None else None, L.fptr(T),
+                                                    C.byref(n)))
+        self.has_stats = True
+        return T.reshape(4, 4)
 
     def add(self, cloud, T=None):
         """Cloud::add (cloud.cpp:163-189): `cloud` is transformed in place by T
@@ -427,6 +454,14 @@ class DepthImageConverterIntegralImage:
 
 
 # ------------------------------------------------------------------ registration
+def trajectory_line(timestamp, T):
+    """A line of nicp_simple_aligner's trajectory file (lines 175-181):
+    "timestamp tx ty tz qx qy qz qw"."""
+    buf = C.create_string_buffer(512)
+    L.check(L.load().nicp_trajectory_line(str(timestamp).encode(), L.fptr(L.f16(T)), buf, len(buf)))
+    return buf.value.decode()
+
+
 def DepthImage_scale(depth, step, maxDepthCov=0.01, depthScale=0.001, ctx=None):
     """DepthImage_scale (imageutils.cpp:6-37) on the GPU: a (rows/step) x
     (cols/step) float image (metres), each pixel the mean of its block's

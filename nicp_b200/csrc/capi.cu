@@ -166,7 +166,7 @@ static int cloud_reserve(nicp_cloud *c, int capacity, int rows, int cols, bool e
   Layout L;
   size_t o_pts = L.take(16 * (size_t)capacity), o_nrm = L.take(16 * (size_t)capacity);
   size_t o_omg = L.take(48 * (size_t)capacity);
-  size_t o_eig = eig ? L.take(48 * (size_t)capacity) : 0;
+  size_t o_eig = eig ? L.take(4 * kStatsWords * (size_t)capacity) : 0;
   size_t o_gauss = gauss ? L.take(48 * (size_t)capacity) : 0;
   size_t o_cnt = L.take(2 * sizeof(int));  // points, points with a normal
   size_t o_idx = L.take(4 * std::max<size_t>(P, 1));
@@ -447,8 +447,8 @@ extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *c
   CK(ctx, cudaMemcpyAsync(nrm.data(), c->nrm, 16 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
   CK(ctx, cudaMemcpyAsync(omg.data(), c->omg, 48 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
   if (ev3 || U9) {
-    eig.resize(12 * (size_t)n);
-    CK(ctx, cudaMemcpyAsync(eig.data(), c->eig, 48 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    eig.resize(kStatsWords * (size_t)n);
+    CK(ctx, cudaMemcpyAsync(eig.data(), c->eig, 4 * kStatsWords * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
   }
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   for (int i = 0; i < n; i++) {
@@ -465,8 +465,29 @@ extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *c
       float *d = on9 + 9 * (size_t)i;
       d[0] = o[6]; d[1] = o[7]; d[2] = o[8]; d[3] = o[7]; d[4] = o[9]; d[5] = o[10]; d[6] = o[8]; d[7] = o[10]; d[8] = o[11];
     }
-    if (ev3) for (int k = 0; k < 3; k++) ev3[3 * (size_t)i + k] = eig[12 * (size_t)i + k];
-    if (U9) for (int k = 0; k < 9; k++) U9[9 * (size_t)i + k] = eig[12 * (size_t)i + 3 + k];
+    if (ev3) for (int k = 0; k < 3; k++) ev3[3 * (size_t)i + k] = eig[kStatsWords * (size_t)i + k];
+    if (U9) for (int k = 0; k < 9; k++) U9[9 * (size_t)i + k] = eig[kStatsWords * (size_t)i + 3 + k];
+  }
+  return NICP_OK;
+}
+
+extern "C" int nicp_cloud_download_stats(nicp_cloud *c, float *eigval3, float *eigvec9, float *mean3, int *n_out) {
+  if (!c) return NICP_EINVAL;
+  nicp_ctx *ctx = c->ctx;
+  int n = 0;
+  int rc = nicp_cloud_size(c, &n);
+  if (rc) return rc;
+  if (n == 0) return NICP_OK;
+  if (!c->eig_valid) return fail(ctx, NICP_ESTATE, "cloud was built without keep_stats");
+  std::vector<float> e(kStatsWords * (size_t)n);
+  CK(ctx, cudaMemcpyAsync(e.data(), c->eig, 4 * kStatsWords * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < n; i++) {
+    const float *r = &e[kStatsWords * (size_t)i];
+    if (eigval3) for (int k = 0; k < 3; k++) eigval3[3 * (size_t)i + k] = r[k];
+    if (eigvec9) for (int k = 0; k < 9; k++) eigvec9[9 * (size_t)i + k] = r[3 + k];
+    if (mean3) for (int k = 0; k < 3; k++) mean3[3 * (size_t)i + k] = r[12 + k];
+    if (n_out) n_out[i] = (int)r[15];
   }
   return NICP_OK;
 }
@@ -1071,7 +1092,7 @@ static int cloud_grow(nicp_cloud *c, int capacity, int n) {
   Layout L;
   size_t o_pts = L.take(16 * (size_t)capacity), o_nrm = L.take(16 * (size_t)capacity);
   size_t o_omg = L.take(48 * (size_t)capacity);
-  size_t o_eig = c->has_eig ? L.take(48 * (size_t)capacity) : 0;
+  size_t o_eig = c->has_eig ? L.take(4 * kStatsWords * (size_t)capacity) : 0;
   size_t o_gauss = c->has_gauss ? L.take(48 * (size_t)capacity) : 0;
   size_t o_cnt = L.take(2 * sizeof(int));
   size_t P = std::max<size_t>((size_t)c->rows * c->cols, 1);
@@ -1085,7 +1106,7 @@ static int cloud_grow(nicp_cloud *c, int capacity, int n) {
   CK(ctx, cudaMemcpyAsync(mem + o_pts, c->pts, 16 * (size_t)n, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(mem + o_nrm, c->nrm, 16 * (size_t)n, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(mem + o_omg, c->omg, 48 * (size_t)n, cudaMemcpyDeviceToDevice, s));
-  if (c->has_eig) CK(ctx, cudaMemcpyAsync(mem + o_eig, c->eig, 48 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  if (c->has_eig) CK(ctx, cudaMemcpyAsync(mem + o_eig, c->eig, 4 * kStatsWords * (size_t)n, cudaMemcpyDeviceToDevice, s));
   if (c->has_gauss) CK(ctx, cudaMemcpyAsync(mem + o_gauss, c->gauss, 48 * (size_t)n, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(mem + o_cnt, c->count, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaStreamSynchronize(s));
@@ -1144,7 +1165,8 @@ extern "C" int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[
   CK(ctx, cudaMemcpyAsync(dst->nrm + nd, src->nrm, 16 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(dst->omg + 3 * (size_t)nd, src->omg, 48 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
   if (eig && dst->eig)
-    CK(ctx, cudaMemcpyAsync(dst->eig + 12 * (size_t)nd, src->eig, 48 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
+    CK(ctx, cudaMemcpyAsync(dst->eig + kStatsWords * (size_t)nd, src->eig, 4 * kStatsWords * (size_t)ns,
+                            cudaMemcpyDeviceToDevice, s));
   if (gauss && dst->gauss)
     CK(ctx, cudaMemcpyAsync(dst->gauss + 3 * (size_t)nd, src->gauss, 48 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
   char *pin;
@@ -1181,7 +1203,7 @@ extern "C" int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *c
   size_t scan_bytes = merge_scan_temp_bytes(n);
   size_t o_scan = E.take(scan_bytes);
   size_t o_pts = E.take(16 * N), o_nrm = E.take(16 * N), o_omg = E.take(48 * N);
-  size_t o_eig = E.take(cloud->eig_valid ? 48 * N : 16), o_gauss = E.take(48 * N), o_cnt = E.take(8);
+  size_t o_eig = E.take(cloud->eig_valid ? 4 * kStatsWords * N : 16), o_gauss = E.take(48 * N), o_cnt = E.take(8);
   PairPlan pl;
   const nicp_cloud *cc = cloud;
   if ((rc = plan_pairs(ctx, 1, cam, &cc, false, false, pl, E.off))) return rc;
@@ -1239,7 +1261,7 @@ extern "C" int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *c
   CK(ctx, cudaMemcpyAsync(cloud->pts, a.o_pts, 16 * N, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(cloud->nrm, a.o_nrm, 16 * N, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(cloud->omg, a.o_omg, 48 * N, cudaMemcpyDeviceToDevice, s));
-  if (a.o_eig) CK(ctx, cudaMemcpyAsync(cloud->eig, a.o_eig, 48 * N, cudaMemcpyDeviceToDevice, s));
+  if (a.o_eig) CK(ctx, cudaMemcpyAsync(cloud->eig, a.o_eig, 4 * kStatsWords * N, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(cloud->gauss, a.o_gauss, 48 * N, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(cloud->count, a.out_count, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s));
   int after[2];
@@ -1575,6 +1597,52 @@ int cloud_normal_counts(nicp_ctx *ctx, int n, const nicp_cloud *const *c, int *o
 }
 
 size_t cloud_bytes(const nicp_cloud *c) { return c ? c->bytes : 0; }
+
+// Host copies of a cloud (for the .nicp writer): points (w reported as 1),
+// normals + curvature, and the kStatsWords-word Stats records when kept.
+int cloud_host_arrays(nicp_cloud *c, std::vector<float> &pts4, std::vector<float> &nrm4, std::vector<float> &stats,
+                      bool &has_stats) {
+  int n = 0;
+  int rc = nicp_cloud_size(c, &n);
+  if (rc) return rc;
+  nicp_ctx *ctx = c->ctx;
+  pts4.resize(4 * (size_t)n);
+  nrm4.resize(4 * (size_t)n);
+  has_stats = c->eig_valid;
+  stats.assign(has_stats ? kStatsWords * (size_t)n : 0, 0.0f);
+  if (n == 0) return NICP_OK;
+  CK(ctx, cudaMemcpyAsync(pts4.data(), c->pts, 16 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaMemcpyAsync(nrm4.data(), c->nrm, 16 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (has_stats)
+    CK(ctx, cudaMemcpyAsync(stats.data(), c->eig, 4 * kStatsWords * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < n; i++) pts4[4 * (size_t)i + 3] = 1.0f;
+  return NICP_OK;
+}
+
+// Fills a cloud from host arrays (the .nicp reader): points with their w
+// codes, normals + curvature, information matrices (12 floats per point, the
+// omg layout), Stats records; `normals` points have a normal.
+int cloud_set_host_arrays(nicp_cloud *c, int n, const float *pts4, const float *nrm4, const float *omg12,
+                          const float *stats, int normals, bool structured, const float omd[8]) {
+  nicp_ctx *ctx = c->ctx;
+  int rc = cloud_reserve(c, n, c->rows, c->cols, true, false);
+  if (rc) return rc;
+  if (n > 0) {
+    CK(ctx, cudaMemcpyAsync(c->pts, pts4, 16 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(c->nrm, nrm4, 16 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(c->omg, omg12, 48 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(c->eig, stats, 4 * kStatsWords * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  int counts[2] = {n, normals};
+  CK(ctx, cudaMemcpyAsync(c->count, counts, sizeof(counts), cudaMemcpyHostToDevice, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  c->eig_valid = true;
+  c->gauss_valid = false;
+  c->omega_structured = structured;
+  std::memcpy(c->omd, omd, sizeof(c->omd));
+  return NICP_OK;
+}
 
 }  // namespace internal
 }  // namespace nicp

@@ -5,8 +5,10 @@
 //   nrm[V]   float4 (nx, ny, nz, curvature)               16 B / point
 //   omg[3V]  float4 x3: (Op00 Op01 Op02 Op11) (Op12 Op22 On00 On01)
 //                       (On02 On11 On12 On22)              48 B / point
-//   eig[12V] optional: eigenvalues (3) + eigenvectors (9, row-major, columns
-//            are vectors) for parity dumps of the reference's Stats.
+//   eig[16V] optional (keep_stats): the reference's Stats -- eigenvalues (3),
+//            eigenvectors (9, row-major, columns are vectors), window mean
+//            (3), window point count (1).
+//   gauss[3V] optional (keep_gaussians): Gaussian3f mean + covariance.
 // Images are packed row-major (pitch == cols).
 //
 // Arithmetic that decides a discrete outcome (which pixel a point lands on,
@@ -39,6 +41,10 @@ constexpr int kZbufDefaultPPT = 4;      // points per thread unless the autotune
 // the correspondence kernel reject a pixel whose point has no normal without
 // gathering it.
 constexpr float kNoNormalW = 0.5f;
+// Per-point Stats kept with keep_stats: eigenvalues (3), eigenvectors (9,
+// row-major, columns are the vectors), window mean (3), window point count
+// n (as float) -- the content of the reference's Stats (stats.h:13-116).
+constexpr int kStatsWords = 16;
 __host__ __device__ __forceinline__ bool point_has_normal(float w) { return w >= 1.0f; }
 
 // ---- per-frame descriptor for the cloud-build kernels

@@ -414,6 +414,8 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
   double U[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   bool reached = false;
   int omega_class = 0;
+  double mean[3] = {0.0, 0.0, 0.0};
+  int nwin = 0;
   int rad = interval_radius(f.K, d, f.min_d, f.max_d, f.world_radius);
   if (rad >= 0 && rad >= f.min_radius) {
     if (rad > f.max_radius) rad = f.max_radius;
@@ -435,6 +437,8 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
     if (n >= f.min_points) {
       double dn = 1.0 / S[0];
       double mu0 = S[1] * dn, mu1 = S[2] * dn, mu2 = S[3] * dn;
+      mean[0] = mu0; mean[1] = mu1; mean[2] = mu2;
+      nwin = n;
       double C[6] = {S[4] * dn - mu0 * mu0, S[5] * dn - mu0 * mu1, S[6] * dn - mu0 * mu2,
                      S[7] * dn - mu1 * mu1, S[8] * dn - mu1 * mu2, S[9] * dn - mu2 * mu2};
       // FP64 solve.  (An FP32 trigonometric solve refined in FP64 was
@@ -494,11 +498,13 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restr
   o[1] = make_float4(om[4], om[5], om[6], om[7]);
   o[2] = make_float4(om[8], om[9], om[10], om[11]);
   if (f.keep_stats) {
-    float *e = f.eig + 12 * (size_t)idx;
+    float *e = f.eig + kStatsWords * (size_t)idx;
     if (!reached) { lam[0] = lam[1] = lam[2] = 0; }
     e[0] = (float)lam[0]; e[1] = (float)lam[1]; e[2] = (float)lam[2];
 #pragma unroll
     for (int k = 0; k < 9; k++) e[3 + k] = (float)U[k];
+    e[12] = (float)mean[0]; e[13] = (float)mean[1]; e[14] = (float)mean[2];
+    e[15] = (float)nwin;
   }
 }
 
@@ -558,12 +564,19 @@ __global__ void k_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *
     gauss[3 * i + 2] = make_float4(Co[5], Co[6], Co[7], Co[8]);
   }
   if (eig) {
-    float *e = eig + 12 * (size_t)i;
+    // StatsVector::transformInPlace (stats.h): the 4x4 Stats times m --
+    // eigenvectors rotated, the mean column (w = 1: the window mean of a
+    // reached point, or the identity's (0 0 0 1) of a default Stats) moved
+    // like a point
+    float *e = eig + kStatsWords * (size_t)i;
     float U[9];
     for (int k = 0; k < 9; k++) U[k] = e[3 + k];
     for (int a = 0; a < 3; a++)
       for (int b = 0; b < 3; b++)
         e[3 + a * 3 + b] = fa(fa(fm(R[a * 3 + 0], U[0 * 3 + b]), fm(R[a * 3 + 1], U[1 * 3 + b])), fm(R[a * 3 + 2], U[2 * 3 + b]));
+    float mo[3];
+    for (int a = 0; a < 3; a++) mo[a] = row4(A + 4 * a, e[12], e[13], e[14], 1.0f);
+    e[12] = mo[0]; e[13] = mo[1]; e[14] = mo[2];
   }
 }
 

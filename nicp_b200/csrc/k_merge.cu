@@ -171,7 +171,7 @@ __global__ void k_merge_compact(const int *__restrict__ tgt, const int *__restri
 #pragma unroll
       for (int k = 0; k < 3; k++) o_omg[3 * (size_t)j + k] = omg[3 * (size_t)i + k];
       if (eig)
-        for (int k = 0; k < 12; k++) o_eig[12 * (size_t)j + k] = eig[12 * (size_t)i + k];
+        for (int k = 0; k < kStatsWords; k++) o_eig[kStatsWords * (size_t)j + k] = eig[kStatsWords * (size_t)i + k];
       if (gauss)
 #pragma unroll
         for (int k = 0; k < 3; k++) o_gauss[3 * (size_t)j + k] = gauss[3 * (size_t)i + k];
