@@ -227,6 +227,23 @@ int nicp_cloud_upload(nicp_cloud *c, int n, const float *points4, const float *n
 /* Cloud::transformInPlace (cloud.cpp:191-204). */
 int nicp_cloud_transform(nicp_cloud *c, const float T16[16]);
 
+/* CorrespondenceFinderNN::compute (correspondencefindernn.cpp:44-97): for
+ * each reference point moved by T16 (the aligner passes _T.inverse()), the
+ * nearest current point in (p, normal_scaling * n) within the squared
+ * inlier distance, then the reference's gates (normals present, point
+ * distance, normal angle).  Exact nearest neighbour (ties: lowest index)
+ * where the reference asks FLANN for an approximate one.  pairs_out: 2*K
+ * int32 (reference, current) in reference-index order (may be NULL);
+ * capacity = number of reference points. */
+int nicp_correspond_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const float T16[16],
+                       float normal_scaling, const nicp_corr_params *corr, int32_t *pairs_out, int *num_pairs);
+/* AlignerNN::align (alignernn.cpp:21-118): the Gauss-Newton loop of
+ * nicp_align with nearest-neighbour correspondences (no projection, so no
+ * camera), recomputed once per outer iteration.  guess16 may be NULL. */
+int nicp_align_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const float guess16[16],
+                  float normal_scaling, const nicp_corr_params *corr, const nicp_lin_params *lin,
+                  const nicp_align_params *prm, nicp_align_result *out);
+
 /* Cloud::save (cloud.cpp:20-25,100-150): writes every step-th point in the
  * reference's .nicp format -- header "NICPCLOUD <n/step> <binary>", t2v(T16)
  * (NULL = identity), then per point text "POINTWITHSTATS x y z nx ny nz

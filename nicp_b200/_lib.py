@@ -110,6 +110,9 @@ SIGNATURES = {
     "nicp_cloud_upload": (C.c_int, [P, C.c_int, f32p, f32p, f32p, f32p, f32p]),
     "nicp_cloud_transform": (C.c_int, [P, f32p]),
     "nicp_cloud_add": (C.c_int, [P, P, f32p]),
+    "nicp_correspond_nn": (C.c_int, [P, P, P, f32p, C.c_float, C.POINTER(CorrParams), i32p, C.POINTER(C.c_int)]),
+    "nicp_align_nn": (C.c_int, [P, P, P, f32p, C.c_float, C.POINTER(CorrParams), C.POINTER(LinParams),
+                                C.POINTER(AlignParams), C.POINTER(AlignResult)]),
     "nicp_cloud_save": (C.c_int, [P, C.c_char_p, f32p, C.c_int, C.c_int]),
     "nicp_cloud_load": (C.c_int, [P, C.c_char_p, C.POINTER(CloudParams), f32p, C.POINTER(C.c_int)]),
     "nicp_trajectory_line": (C.c_int, [C.c_char_p, f32p, C.c_char_p, C.c_size_t]),

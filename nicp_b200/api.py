@@ -784,6 +784,58 @@ class AlignerProjective:
         return self._T
 
 
+class CorrespondenceFinderNN(CorrespondenceFinderProjective):
+    """correspondencefindernn.{h,cpp}: nearest neighbour in (p, s n) within
+    the inlier distance, then the normal gates.  The search is exact (ties:
+    lowest index) where the reference's FLANN kd-tree is approximate."""
+
+    def __init__(self, ctx=None):
+        super().__init__(ctx)
+        self._normalScaling = 1.0  # correspondencefindernn.cpp:5-9
+
+    def normalScaling(self): return self._normalScaling
+    def setNormalScaling(self, v): self._normalScaling = float(v)
+
+    def compute(self, referenceScene, currentScene, T):
+        n = referenceScene.size()
+        pairs = np.zeros((max(n, 1), 2), np.int32)
+        k = C.c_int(0)
+        self.ctx.check(self.ctx.lib.nicp_correspond_nn(self.ctx.h, referenceScene.h, currentScene.h,
+                                                       L.fptr(L.f16(T)), self._normalScaling,
+                                                       C.byref(self.params()), L.iptr(pairs), C.byref(k)))
+        self._correspondences = pairs[:k.value].copy()
+        return self._correspondences
+
+
+class AlignerNN(AlignerProjective):
+    """alignernn.{h,cpp}: AlignerProjective's loop with nearest-neighbour
+    correspondences (CorrespondenceFinderNN); needs no projector."""
+
+    def align(self):
+        import time
+        lin, cf = self._linearizer, self._correspondenceFinder
+        if lin is None or not isinstance(cf, CorrespondenceFinderNN):
+            raise ValueError("AlignerNN: a linearizer and a CorrespondenceFinderNN must be set")
+        if self._referenceCloud is None or self._currentCloud is None:
+            raise ValueError("AlignerNN: reference and current clouds must be set")
+        r = L.AlignResult()
+        t0 = time.perf_counter()
+        self.ctx.check(self.ctx.lib.nicp_align_nn(self.ctx.h, self._referenceCloud.h, self._currentCloud.h,
+                                                  L.fptr(L.f16(self._initialGuess)), cf.normalScaling(),
+                                                  C.byref(cf.params()), C.byref(lin.params()), C.byref(self.params()),
+                                                  C.byref(r)))
+        self._totalTime = (time.perf_counter() - t0) * 1e3
+        self._T = np.array(r.T).reshape(4, 4)
+        self._error = r.error
+        self._inliers = r.inliers
+        lin._error, lin._inliers = r.error, r.inliers
+        self._translationalEigenRatio = r.translational_ratio
+        self._rotationalEigenRatio = r.rotational_ratio
+        self._solutionValid = bool(r.solution_valid == 1)
+        self.last_result = r
+        return self._T
+
+
 # ------------------------------------------------------------------ batching (no reference counterpart)
 def build_batch(ctx, frames, cams, prm, clouds, on_device=False):
     """Builds clouds for many uint16 frames in one pass of launches.  frames:

@@ -21,7 +21,7 @@ BUILD = os.path.join(HERE, "_build")
 GPU_LIB = os.path.join(HERE, "libnicp_b200.so")
 SYNTH_LIB = os.path.join(HERE, "libnicp_synth.so")
 
-CUDA_SOURCES = ["k_cloud.cu", "k_align.cu", "k_merge.cu", "capi.cu"]
+CUDA_SOURCES = ["k_cloud.cu", "k_align.cu", "k_merge.cu", "k_nn.cu", "capi.cu"]
 HOST_SOURCES = ["stats_host.cpp", "server.cpp", "cloud_io.cpp"]
 HEADERS = ["common.cuh", "kernels.hpp", "host_math.hpp"]
 

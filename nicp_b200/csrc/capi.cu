@@ -1084,6 +1084,232 @@ extern "C" int nicp_depth_scale(nicp_ctx *ctx, const void *depth, int is_u16, in
   return NICP_OK;
 }
 
+// ------------------------------------------------------------------ nearest-neighbour association
+static int cloud_counts2(nicp_cloud *c, int out[2]);
+
+namespace {
+// Workspace of one NN alignment: the grid over the current cloud, the match
+// / flag / position arrays over the reference points, the pair list, FP64
+// partials, the pair descriptor and state.
+struct NNPlan {
+  int nr = 0, nc = 0, tiles = 0;
+  NNGrid grid{};
+  size_t o_keys, o_skeys, o_idx, o_sidx, o_feat, o_sfeat, o_cstart, o_cend, o_temp, temp_bytes;
+  size_t o_match, o_flag, o_pos, o_pairs, o_np, o_part, o_pd, o_st, o_guess, o_roff;
+};
+
+// Bounding box of the current cloud (host), then the grid: cell h =
+// cbrt(volume / points) (about one cell per point of a surface patch; at
+// least 1 mm), at most 2^24 cells.
+int nn_plan(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, float radius, NNPlan &pl) {
+  int rc;
+  int cr[2], cc[2];
+  if ((rc = cloud_counts2(const_cast<nicp_cloud *>(ref), cr)) || (rc = cloud_counts2(const_cast<nicp_cloud *>(cur), cc)))
+    return rc;
+  pl.nr = cr[0];
+  pl.nc = cc[0];
+  std::vector<float4> pts(std::max(pl.nc, 1));
+  if (pl.nc > 0) {
+    CK(ctx, cudaMemcpyAsync(pts.data(), cur->pts, 16 * (size_t)pl.nc, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  for (int j = 0; j < pl.nc; j++) {
+    const float v[3] = {pts[j].x, pts[j].y, pts[j].z};
+    for (int a = 0; a < 3; a++) {
+      if (j == 0 || v[a] < lo[a]) lo[a] = v[a];
+      if (j == 0 || v[a] > hi[a]) hi[a] = v[a];
+    }
+  }
+  double ext[3], vol = 1.0;
+  for (int a = 0; a < 3; a++) {
+    ext[a] = std::max(1e-3, (double)hi[a] - lo[a]);
+    vol *= ext[a];
+  }
+  double h = std::max(1e-3, std::cbrt(vol / std::max(pl.nc, 1)));
+  for (;;) {
+    double cells = 1.0;
+    for (int a = 0; a < 3; a++) cells *= std::floor(ext[a] / h) + 1;
+    if (cells <= (double)(1 << 24)) break;
+    h *= 1.25;
+  }
+  NNGrid &g = pl.grid;
+  g.h = (float)h;
+  g.inv_h = (float)(1.0 / h);
+  for (int a = 0; a < 3; a++) {
+    g.origin[a] = lo[a];
+    g.dim[a] = (int)std::floor(ext[a] / h) + 1;
+  }
+  g.max_shell = (int)std::ceil(radius / h) + 1;
+  const size_t ncells = (size_t)g.dim[0] * g.dim[1] * g.dim[2];
+  const size_t NC = std::max(pl.nc, 1), NR = std::max(pl.nr, 1);
+  pl.tiles = (int)((NR + kCorrTilePixels - 1) / kCorrTilePixels);
+  pl.temp_bytes = std::max(nn_temp_bytes((int)NC), nn_temp_bytes((int)NR));
+  Layout L;
+  pl.o_keys = L.take(4 * NC); pl.o_skeys = L.take(4 * NC); pl.o_idx = L.take(4 * NC); pl.o_sidx = L.take(4 * NC);
+  pl.o_feat = L.take(24 * NC); pl.o_sfeat = L.take(24 * NC);
+  pl.o_cstart = L.take(4 * ncells); pl.o_cend = L.take(4 * ncells);
+  pl.o_temp = L.take(pl.temp_bytes);
+  pl.o_match = L.take(4 * NR); pl.o_flag = L.take(4 * NR); pl.o_pos = L.take(4 * NR);
+  pl.o_pairs = L.take(8 * NR); pl.o_np = L.take(4);
+  pl.o_part = L.take(8 * kPartialWords * (size_t)pl.tiles);
+  pl.o_pd = L.take(sizeof(PairDev)); pl.o_st = L.take(sizeof(PairState));
+  pl.o_guess = L.take(128); pl.o_roff = L.take(128);
+  return ensure_ws(ctx, L.off);
+}
+
+int nn_build(nicp_ctx *ctx, const NNPlan &pl, const nicp_cloud *cur, float nscale) {
+  char *ws = ctx->ws;
+  NNBuild b{};
+  b.nc = pl.nc;
+  b.cur_pts = cur->pts;
+  b.cur_nrm = cur->nrm;
+  b.nscale = nscale;
+  b.grid = pl.grid;
+  const size_t ncells = (size_t)pl.grid.dim[0] * pl.grid.dim[1] * pl.grid.dim[2];
+  b.key_bits = 1;
+  while (b.key_bits < 32 && ((size_t)1 << b.key_bits) < ncells) b.key_bits++;
+  b.keys = (unsigned *)(ws + pl.o_keys); b.skeys = (unsigned *)(ws + pl.o_skeys);
+  b.idx = (unsigned *)(ws + pl.o_idx); b.sidx = (unsigned *)(ws + pl.o_sidx);
+  b.feat6 = (float *)(ws + pl.o_feat); b.sfeat6 = (float *)(ws + pl.o_sfeat);
+  b.cstart = (int *)(ws + pl.o_cstart); b.cend = (int *)(ws + pl.o_cend);
+  b.temp = ws + pl.o_temp;
+  b.temp_bytes = pl.temp_bytes;
+  if (launch_nn_build(b, ctx->stream)) return fail(ctx, NICP_ECUDA, "nearest-neighbour index build failed");
+  return NICP_OK;
+}
+
+NNQuery nn_query(nicp_ctx *ctx, const NNPlan &pl, const nicp_cloud *ref, const nicp_cloud *cur, float nscale,
+                 const nicp_corr_params &cp, const float *Tg, const PairState *state) {
+  char *ws = ctx->ws;
+  NNQuery q{};
+  q.nr = pl.nr;
+  q.ref_pts = ref->pts; q.ref_nrm = ref->nrm;
+  q.cur_pts = cur->pts; q.cur_nrm = cur->nrm;
+  q.Tg = Tg;
+  q.state = state;
+  q.nscale = nscale;
+  q.sq = cp.inlier_distance_threshold * cp.inlier_distance_threshold;
+  q.cos_thr = cp.inlier_normal_angular_threshold;
+  q.demoted = cp.demoted_to_gicp;
+  q.grid = pl.grid;
+  q.cstart = (const int *)(ws + pl.o_cstart); q.cend = (const int *)(ws + pl.o_cend);
+  q.sfeat6 = (const float *)(ws + pl.o_sfeat); q.sidx = (const unsigned *)(ws + pl.o_sidx);
+  q.match = (int *)(ws + pl.o_match);
+  return q;
+}
+}  // namespace
+
+extern "C" int nicp_correspond_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const float T16[16],
+                                  float normal_scaling, const nicp_corr_params *corr, int32_t *pairs_out,
+                                  int *num_pairs) {
+  if (!ctx || !ref || !cur || !T16 || !corr || !num_pairs) return NICP_EINVAL;
+  NNPlan pl;
+  int rc = nn_plan(ctx, ref, cur, corr->inlier_distance_threshold, pl);
+  if (rc) return rc;
+  *num_pairs = 0;
+  if (pl.nr == 0 || pl.nc == 0) return NICP_OK;
+  if ((rc = nn_build(ctx, pl, cur, normal_scaling))) return rc;
+  char *pin;
+  if ((rc = pin_up(ctx, 48, &pin))) return rc;
+  rows12(HM4::from(T16), (float *)pin);
+  cudaStream_t s = ctx->stream;
+  CK(ctx, cudaMemcpyAsync(ctx->ws + pl.o_guess, pin, 48, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+  NNQuery q = nn_query(ctx, pl, ref, cur, normal_scaling, *corr, (const float *)(ctx->ws + pl.o_guess), nullptr);
+  if (launch_nn_correspond(q, (int *)(ctx->ws + pl.o_flag), (int *)(ctx->ws + pl.o_pos), ctx->ws + pl.o_temp,
+                           pl.temp_bytes, (int32_t *)(ctx->ws + pl.o_pairs), (int *)(ctx->ws + pl.o_np), s))
+    return fail(ctx, NICP_ECUDA, "nearest-neighbour query failed");
+  int K = 0;
+  CK(ctx, cudaMemcpyAsync(&K, ctx->ws + pl.o_np, 4, cudaMemcpyDeviceToHost, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  if (pairs_out && K > 0)
+    CK(ctx, cudaMemcpy(pairs_out, ctx->ws + pl.o_pairs, 8 * (size_t)K, cudaMemcpyDeviceToHost));
+  *num_pairs = K;
+  return NICP_OK;
+}
+
+extern "C" int nicp_align_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const float guess16[16],
+                             float normal_scaling, const nicp_corr_params *corr, const nicp_lin_params *lin,
+                             const nicp_align_params *prm, nicp_align_result *out) {
+  if (!ctx || !ref || !cur || !corr || !lin || !prm || !out) return NICP_EINVAL;
+  if (prm->outer_iterations < 0 || prm->inner_iterations < 1 || prm->outer_iterations > 1000 ||
+      prm->inner_iterations > 100)
+    return fail(ctx, NICP_EINVAL, "iteration counts out of range");
+  if (!ref->mem || !cur->mem || ref->ctx != ctx || cur->ctx != ctx)
+    return fail(ctx, NICP_EINVAL, "both clouds must be built on this context");
+  NNPlan pl;
+  int rc = nn_plan(ctx, ref, cur, corr->inlier_distance_threshold, pl);
+  if (rc) return rc;
+  if ((rc = nn_build(ctx, pl, cur, normal_scaling))) return rc;
+  char *ws = ctx->ws;
+  cudaStream_t s = ctx->stream;
+  // the pair descriptor: the pair list plays the pixel image of the list
+  // kernels (1 x nr), one FP64 partial per 1024 list entries
+  char *pin;
+  if ((rc = pin_up(ctx, sizeof(PairDev) + 256, &pin))) return rc;
+  PairDev &d = *(PairDev *)pin;
+  std::memset(&d, 0, sizeof(d));
+  d.ref_pts = ref->pts; d.ref_nrm = ref->nrm; d.ref_count = ref->count;
+  d.cur_pts = cur->pts; d.cur_nrm = cur->nrm; d.cur_omg = cur->omg; d.cur_count = cur->count;
+  d.rows = 1;
+  d.cols = std::max(pl.nr, 1);
+  d.tile_base = 0;
+  d.ref_capacity = std::max(pl.nr, 1);
+  d.K[0] = d.K[4] = d.K[8] = 1.0f;
+  d.partials = (double *)(ws + pl.o_part);
+  d.pairs = (int32_t *)(ws + pl.o_pairs);
+  d.num_pairs = (int *)(ws + pl.o_np);
+  d.state = (PairState *)(ws + pl.o_st);
+  double *gs = (double *)(pin + sizeof(PairDev));
+  HM4 G = HM4::from(guess16);
+  for (int k = 0; k < 16; k++) gs[k] = G.a[k];
+  double *ro = gs + 16;
+  for (int k = 0; k < 16; k++) ro[k] = (k % 5 == 0) ? 1.0 : 0.0;
+  CK(ctx, cudaMemcpyAsync(ws + pl.o_pd, pin, sizeof(PairDev), cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaMemcpyAsync(ws + pl.o_guess, gs, 256, cudaMemcpyHostToDevice, s));
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+  const PairDev *dpd = (const PairDev *)(ws + pl.o_pd);
+  LinParams lp = lin_params(*lin);
+  const int xb = lin->cross_block_f32 ? kSolveCrossF32 : 0;
+  launch_init_pairs(dpd, 1, (const double *)(ws + pl.o_guess), (const double *)(ws + pl.o_guess + 128), s,
+                    &ctx->prof);
+  NNQuery q = nn_query(ctx, pl, ref, cur, normal_scaling, *corr, nullptr, (const PairState *)(ws + pl.o_st));
+  for (int i = 0; i < prm->outer_iterations; i++) {
+    // correspondences with the state's T^-1 (alignernn.cpp:40-45)
+    if (launch_nn_correspond(q, (int *)(ws + pl.o_flag), (int *)(ws + pl.o_pos), ws + pl.o_temp, pl.temp_bytes,
+                             d.pairs, d.num_pairs, s))
+      return fail(ctx, NICP_ECUDA, "nearest-neighbour query failed");
+    for (int k = 0; k < prm->inner_iterations; k++) {
+      launch_lin_list(dpd, 1, pl.tiles, lp, 1, 1, nullptr, s, &ctx->prof);
+      launch_solve(dpd, 1, prm->lambda, ((k == prm->inner_iterations - 1) ? 1 : 0) | xb, prm->early_exit_eps, 0, s,
+                   &ctx->prof);
+    }
+  }
+  if (prm->compute_statistics) {
+    launch_lin_list(dpd, 1, pl.tiles, lp, 1, 2, nullptr, s, &ctx->prof);
+    launch_solve(dpd, 1, 0.0f, 4 | xb, 0.0, 1, s, &ctx->prof);
+  }
+  CK(ctx, cudaGetLastError());
+  PairState st;
+  CK(ctx, cudaMemcpyAsync(&st, ws + pl.o_st, sizeof(PairState), cudaMemcpyDeviceToHost, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  std::memcpy(out->T, st.T, sizeof(out->T));
+  out->error = st.error;
+  out->inliers = st.inliers;
+  out->num_correspondences = st.num_corr;
+  out->outer_iterations_run = st.iterations;
+  out->status = st.status;
+  out->translational_ratio = out->rotational_ratio = 0;
+  out->solution_valid = -1;
+  if (prm->compute_statistics) {
+    solution_statistics(st.Hstat, st.T, &out->translational_ratio, &out->rotational_ratio);
+    out->solution_valid = !(out->rotational_ratio > prm->rotational_min_eigen_ratio ||
+                            out->translational_ratio > prm->translational_min_eigen_ratio);
+  }
+  return NICP_OK;
+}
+
 // ------------------------------------------------------------------ scene
 // Grows a cloud's allocation to `capacity` points keeping its first n
 // points (all arrays) and its counts.

@@ -130,6 +130,44 @@ struct MergeArgs {
   float4 *o_gauss;
   int *out_count;
 };
+// Uniform grid over the current cloud's xyz (k_nn.cu).
+struct NNGrid {
+  float origin[3];
+  float h, inv_h;
+  int dim[3];
+  int max_shell;  // shells needed to cover the radius
+};
+struct NNBuild {
+  int nc;
+  const float4 *cur_pts, *cur_nrm;
+  float nscale;
+  NNGrid grid;
+  int key_bits;
+  unsigned *keys, *skeys, *idx, *sidx;
+  float *feat6, *sfeat6;
+  int *cstart, *cend;
+  void *temp;
+  size_t temp_bytes;
+};
+struct NNQuery {
+  int nr;
+  const float4 *ref_pts, *ref_nrm;
+  const float4 *cur_pts, *cur_nrm;
+  const float *Tg;          // rows 0..2 of the transform, or null: the pair state's Tgate
+  const PairState *state;
+  float nscale, sq, cos_thr;
+  int demoted;
+  NNGrid grid;
+  const int *cstart, *cend;
+  const float *sfeat6;
+  const unsigned *sidx;
+  int *match;
+};
+size_t nn_temp_bytes(int n);
+int launch_nn_build(const NNBuild &b, cudaStream_t s);
+int launch_nn_correspond(const NNQuery &q, int *flag, int *pos, void *temp, size_t temp_bytes, int32_t *pairs,
+                         int *num_pairs, cudaStream_t s);
+
 size_t merge_scan_temp_bytes(int n);
 int launch_merge(const MergeArgs &a, cudaStream_t s);
 

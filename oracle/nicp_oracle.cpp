@@ -1110,6 +1110,126 @@ static void align(const Cloud<S> &ref, const Cloud<S> &cur, const orc_camera &ca
   }
 }
 
+// CorrespondenceFinderNN::compute (correspondencefindernn.cpp:44-97) with
+// an exact nearest neighbour where the reference asks FLANN's randomized
+// kd-tree (approximate, 16 checks) for the nearest current point within
+// the squared radius in the 6-D space (p, s n): here every current point is
+// tested, the smallest squared distance wins and ties keep the lowest index.
+// Distances sum the six squared differences in coordinate order.  T is the
+// transform applied to the reference (the aligner passes _T.inverse()).
+template <class S>
+static int correspond_nn(const Cloud<S> &ref, const Cloud<S> &cur, M4<S> T, S nscale,
+                         const orc_align_params &prm, int32_t *pairs) {
+  set_row3(T);
+  const S thr = S(prm.inlier_distance_threshold);
+  const S sq = thr * thr;
+  const S cosT = S(prm.inlier_normal_angular_threshold);
+  const int nr = ref.n, nc = cur.n;
+  std::vector<S> cf(6 * (size_t)nc);
+  for (int j = 0; j < nc; j++) {  // _model2linear(dest, src, nscale)
+    for (int a = 0; a < 3; a++) cf[6 * (size_t)j + a] = cur.points[j][a];
+    for (int a = 0; a < 3; a++) cf[6 * (size_t)j + 3 + a] = nscale * cur.normals[j][a];
+  }
+  M4<S> sR = M4<S>::zero();  // T.linear() * nscale
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) sR(a, b) = T(a, b) * nscale;
+  std::vector<int32_t> match(nr, -1);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < nr; i++) {
+    V4<S> p = mv(T, ref.points[i]);
+    V4<S> n0 = ref.normals[i];
+    n0[3] = S(0);
+    V4<S> sn = mv(sR, n0);
+    const S q[6] = {p[0], p[1], p[2], sn[0], sn[1], sn[2]};
+    int best = -1;
+    S bd = S(0);
+    for (int j = 0; j < nc; j++) {
+      const S *c = &cf[6 * (size_t)j];
+      S d = S(0);
+      for (int a = 0; a < 6; a++) {
+        S e = q[a] - c[a];
+        d = d + e * e;
+      }
+      if (d < sq && (best < 0 || d < bd)) { best = j; bd = d; }
+    }
+    if (best < 0) continue;
+    // the gates (correspondencefindernn.cpp:80-93)
+    M4<S> R = T;
+    for (int a = 0; a < 3; a++) R(a, 3) = S(0);
+    V4<S> rn = mv(R, n0);
+    V4<S> rp = p;
+    const V4<S> &cn = cur.normals[best], &cp = cur.points[best];
+    S rn2 = rn[0] * rn[0]; rn2 = rn2 + rn[1] * rn[1]; rn2 = rn2 + rn[2] * rn[2];
+    S cn2 = cn[0] * cn[0]; cn2 = cn2 + cn[1] * cn[1]; cn2 = cn2 + cn[2] * cn[2];
+    if (!prm.corr_demoted_to_gicp && (rn2 == S(0) || cn2 == S(0))) continue;
+    S dx = rp[0] - cp[0], dy = rp[1] - cp[1], dz = rp[2] - cp[2];
+    S dd = dx * dx; dd = dd + dy * dy; dd = dd + dz * dz;
+    if (dd > sq) continue;
+    if (std::isnan(cn[0]) || std::isnan(cn[1]) || std::isnan(cn[2]) || std::isnan(rn[0]) || std::isnan(rn[1]) ||
+        std::isnan(rn[2]))
+      continue;
+    S dot = rn[0] * cn[0]; dot = dot + rn[1] * cn[1]; dot = dot + rn[2] * cn[2];
+    if (!prm.corr_demoted_to_gicp && dot < cosT) continue;
+    match[i] = best;
+  }
+  int K = 0;
+  for (int i = 0; i < nr; i++)
+    if (match[i] >= 0) {
+      pairs[2 * K] = i;
+      pairs[2 * K + 1] = match[i];
+      K++;
+    }
+  return K;
+}
+
+// AlignerNN::align (alignernn.cpp:21-118): AlignerProjective's loop with
+// nearest-neighbour correspondences (no projection).
+template <class S>
+static void align_nn(const Cloud<S> &ref, const Cloud<S> &cur, const double *guess, S nscale,
+                     const orc_align_params &prm, bool f64mode, int stats, orc_align_result *out) {
+  M4<S> T = guess ? load_T<S>(guess) : M4<S>::identity();
+  std::vector<int32_t> pairs(2 * (size_t)std::max(ref.n, 1));
+  double H[36], b[6], err = 0;
+  int inl = 0, K = 0;
+  for (int i = 0; i < prm.outer_iterations; i++) {
+    set_row3(T);
+    K = correspond_nn(ref, cur, iso_inverse(T), nscale, prm, pairs.data());
+    M4<S> invT = iso_inverse(T);
+    for (int k = 0; k < prm.inner_iterations; k++) {
+      set_row3(invT);
+      linearize(ref, cur, pairs.data(), K, invT, prm, f64mode, H, b, &err, &inl);
+      S Hs[36], bs[6], dx[6];
+      for (int q = 0; q < 36; q++) Hs[q] = S(H[q]);
+      for (int q = 0; q < 6; q++) { Hs[q * 6 + q] = Hs[q * 6 + q] + S(prm.lambda); bs[q] = -S(b[q]); }
+      ldlt_solve(Hs, bs, dx);
+      invT = mm(v2t(dx), invT);
+    }
+    T = iso_inverse(invT);
+    S x[6];
+    t2v(T, x);
+    T = v2t(x);
+    set_row3(T);
+  }
+  for (int i = 0; i < 16; i++) out->T[i] = (double)T.a[i];
+  out->error = err;
+  out->inliers = inl;
+  out->num_correspondences = K;
+  out->translational_ratio = out->rotational_ratio = 0;
+  out->solution_valid = 0;
+  if (stats) {
+    M4<S> invT = iso_inverse(T);
+    set_row3(invT);
+    double Hs[36], bs[6], e2;
+    int i2;
+    linearize(ref, cur, pairs.data(), K, invT, prm, f64mode, Hs, bs, &e2, &i2);
+    M4<double> Td;
+    for (int i = 0; i < 16; i++) Td.a[i] = (double)T.a[i];
+    solution_statistics(Hs, Td, &out->translational_ratio, &out->rotational_ratio);
+    out->solution_valid = !(out->rotational_ratio > prm.rotational_min_eigen_ratio ||
+                            out->translational_ratio > prm.translational_min_eigen_ratio);
+  }
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -1413,6 +1533,18 @@ void orc_align(int mode, const orc_cloud *ref, const orc_cloud *cur, const orc_c
                orc_align_result *out) {
   if (mode == ORC_F64) align(*ref->d, *cur->d, *cam, guess, roff, coff, *prm, true, stats, out);
   else align(*ref->f, *cur->f, *cam, guess, roff, coff, *prm, false, stats, out);
+}
+
+int orc_correspond_nn(int mode, const orc_cloud *ref, const orc_cloud *cur, const double *T16, double normal_scaling,
+                      const orc_align_params *prm, int32_t *pairs) {
+  if (mode == ORC_F64) return correspond_nn(*ref->d, *cur->d, load_T<double>(T16), normal_scaling, *prm, pairs);
+  return correspond_nn(*ref->f, *cur->f, load_T<float>(T16), (float)normal_scaling, *prm, pairs);
+}
+
+void orc_align_nn(int mode, const orc_cloud *ref, const orc_cloud *cur, const double *guess, double normal_scaling,
+                  const orc_align_params *prm, int stats, orc_align_result *out) {
+  if (mode == ORC_F64) align_nn(*ref->d, *cur->d, guess, normal_scaling, *prm, true, stats, out);
+  else align_nn(*ref->f, *cur->f, guess, (float)normal_scaling, *prm, false, stats, out);
 }
 
 template <class S> static void eig_api(const double *A6, double *l3, double *U9) {

@@ -143,6 +143,15 @@ typedef struct {
   int solution_valid;
 } orc_align_result;
 
+/* CorrespondenceFinderNN::compute (correspondencefindernn.cpp:44-97) with an
+ * exact nearest neighbour in (p, normal_scaling * n); pairs: 2*K int32 in
+ * reference-index order; returns K. */
+int orc_correspond_nn(int mode, const orc_cloud *ref, const orc_cloud *cur, const double *T16, double normal_scaling,
+                      const orc_align_params *prm, int32_t *pairs);
+/* AlignerNN::align (alignernn.cpp:21-118). */
+void orc_align_nn(int mode, const orc_cloud *ref, const orc_cloud *cur, const double *guess, double normal_scaling,
+                  const orc_align_params *prm, int stats, orc_align_result *out);
+
 void orc_align(int mode, const orc_cloud *ref, const orc_cloud *cur, const orc_camera *cam,
                const double *guess16, const double *ref_offset16, const double *cur_offset16,
                const orc_align_params *prm, int compute_statistics, orc_align_result *out);

@@ -85,6 +85,9 @@ def load():
         "orc_depth_scale": (None, [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(C.c_float)]),
         "orc_cloud_add": (None, [P, P, dp]),
         "orc_merge": (C.c_int, [C.c_int, P, C.POINTER(Camera), dp, C.c_double, C.c_double]),
+        "orc_correspond_nn": (C.c_int, [C.c_int, P, P, dp, C.c_double, C.POINTER(AlignParams), ip]),
+        "orc_align_nn": (None, [C.c_int, P, P, dp, C.c_double, C.POINTER(AlignParams), C.c_int,
+                                C.POINTER(AlignResult)]),
         "orc_cloud_get": (C.c_int, [P, C.c_int, dp]),
         "orc_projector_matrices": (None, [C.c_int, C.POINTER(Camera), dp, dp, dp]),
         "orc_project": (None, [C.c_int, P, C.POINTER(Camera), dp, ip, dp]),
@@ -277,6 +280,27 @@ def convert_u16(depth_u16, scale=0.001):
     load().orc_convert_u16(d.ctypes.data_as(C.POINTER(C.c_uint16)), d.shape[0], d.shape[1], np.float32(scale),
                            out.ctypes.data_as(C.POINTER(C.c_float)))
     return out
+
+
+def correspond_nn(mode, ref, cur, T, normal_scaling=1.0, prm=None):
+    """CorrespondenceFinderNN::compute with an exact nearest neighbour."""
+    prm = prm or align_params()
+    _same_mode(mode, ref, cur)
+    pairs = np.zeros(2 * max(len(ref), 1), dtype=np.int32)
+    k = load().orc_correspond_nn(mode, ref.h, cur.h, _d(T), normal_scaling, C.byref(prm), pairs.ctypes.data_as(ip))
+    return pairs[:2 * k].reshape(k, 2)
+
+
+def align_nn(mode, ref, cur, guess=None, normal_scaling=1.0, prm=None, statistics=False):
+    """AlignerNN::align (alignernn.cpp:21-118)."""
+    prm = prm or align_params()
+    _same_mode(mode, ref, cur)
+    r = AlignResult()
+    load().orc_align_nn(mode, ref.h, cur.h, _d(guess), normal_scaling, C.byref(prm), 1 if statistics else 0,
+                        C.byref(r))
+    return dict(T=np.array(r.T).reshape(4, 4), error=r.error, inliers=r.inliers,
+                num_correspondences=r.num_correspondences, translational_ratio=r.translational_ratio,
+                rotational_ratio=r.rotational_ratio, solution_valid=r.solution_valid)
 
 
 def cloud_transform(cloud, T):
