@@ -20,6 +20,7 @@ one batched, graph-captured device loop.  Metric: 640x480 pairs/s.
   mixed_batch  512 independent pairs of mixed resolution, <= 20 x 2 iterations
                with early exit, batched vs the plain per-pair loop
   scene_fusion frames fused into one scene (Cloud::add + Merger::merge)
+  nn_align     AlignerNN on 640x480 pairs (exact nearest-neighbour association)
   serving      the request loop (nicp_server_*) under open-loop Poisson load:
                64 camera streams, 30/60/10% 320x240/640x480/1280x720,
                p50/p99 latency and throughput per arrival rate
@@ -421,6 +422,38 @@ def scene_fusion_leg(ctx, seed, frames=30):
             "points_per_frame": per_frame, "scene_points": scene.size(), "removed_points": removed}
 
 
+# ------------------------------------------------------------------ nearest-neighbour leg
+def nn_align_leg(ctx, seed, reps=3):
+    """AlignerNN (alignernn.cpp:21-118) on consecutive 640x480 frames of the
+    trajectory: exact 6-D nearest-neighbour correspondences every outer
+    iteration (10 outer x 1 inner).  Wall time of align() (it synchronises)."""
+    from nicp_b200 import api, synth
+    imgs, poses, cam = synth.render_sequence(seed, "640x480", n_frames=reps + 1, period=200)
+    proj, conv, _, _, _ = gpu_objects(ctx, cam)
+    clouds = []
+    for f in imgs:
+        c = api.Cloud(ctx)
+        conv.compute(c, f)
+        clouds.append(c)
+    al = api.AlignerNN(None, api.Linearizer(ctx), api.CorrespondenceFinderNN(ctx), ctx)
+    al.computeStatistics = False
+    times, errs = [], []
+    for k in range(reps + 1):  # the first pass loads the kernels
+        i = min(k, reps - 1)
+        al.setReferenceCloud(clouds[i])
+        al.setCurrentCloud(clouds[i + 1])
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        T = al.align()
+        times.append(time.perf_counter() - t0)
+        errs.append(synth.pose_error(T, synth.rel(poses[i], poses[i + 1])))
+    return {"workload": "640x480 consecutive frames, exact NN association, 10 outer x 1 inner",
+            "ms_per_pair": 1e3 * float(np.median(times[1:])),
+            "pose_err_vs_truth_median": {"rad": float(np.median([e[0] for e in errs])),
+                                         "m": float(np.median([e[1] for e in errs]))},
+            "correspondences": int(al.last_result.num_correspondences)}
+
+
 # ------------------------------------------------------------------ serving leg
 SERVE_MIX = (("320x240", 0.3, 19), ("640x480", 0.6, 38), ("1280x720", 0.1, 7))  # (camera, request share, streams)
 
@@ -597,6 +630,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the 512-pair mixed-resolution batch leg")
     ap.add_argument("--no-fusion", action="store_true", help="skip the scene-fusion (merger) leg")
+    ap.add_argument("--no-nn", action="store_true", help="skip the nearest-neighbour aligner leg")
     ap.add_argument("--serve-rates", default="500,2000,5000,10000,20000",
                     help="Poisson arrival rates (requests/s) of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per rate")
@@ -761,6 +795,10 @@ def main():
     if not args.no_fusion and rank == 0:
         fusion = scene_fusion_leg(ctx, args.seed + 29)
 
+    nn = None
+    if not args.no_nn and rank == 0:
+        nn = nn_align_leg(ctx, args.seed + 41)
+
     serving = None
     if not args.no_serve and rank == 0:
         serving = serve_leg(local, [float(r) for r in args.serve_rates.split(",")], args.serve_seconds, args.seed)
@@ -782,7 +820,7 @@ def main():
                 "gpu_launches": int(launches), "clocks": clk,
                 "plain_pairs_per_s": plain, "batched_over_plain": (value / world / plain) if plain else None,
                 "pose_err_vs_truth_median": {"rad": rot_med, "m": tr_med},
-                "points_per_frame": V, "correspondences_per_pair": C, "mixed_batch": mixed, "scene_fusion": fusion,
+                "points_per_frame": V, "correspondences_per_pair": C, "mixed_batch": mixed, "scene_fusion": fusion, "nn_align": nn,
                 "serving": serving}
         print(json.dumps(line), flush=True)
     del clouds
