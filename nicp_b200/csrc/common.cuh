@@ -255,13 +255,13 @@ __device__ inline void t_null_vector(const T *B, T mu, T *v) {
   t_cross(r0, r2, c1);
   t_cross(r1, r2, c2);
   T d0 = t_dot(c0, c0), d1 = t_dot(c1, c1), d2 = t_dot(c2, c2);
-  const T *best = c0;
-  T db = d0;
-  if (d1 > db) { best = c1; db = d1; }
-  if (d2 > db) { best = c2; db = d2; }
+  // select by value (a pointer into the candidates would put them in local memory)
+  T b0 = c0[0], b1 = c0[1], b2 = c0[2], db = d0;
+  if (d1 > db) { b0 = c1[0]; b1 = c1[1]; b2 = c1[2]; db = d1; }
+  if (d2 > db) { b0 = c2[0]; b1 = c2[1]; b2 = c2[2]; db = d2; }
   if (!(db > T(0))) { v[0] = 1; v[1] = 0; v[2] = 0; return; }
   T inv = T(1) / sqrt(db);
-  v[0] = best[0] * inv; v[1] = best[1] * inv; v[2] = best[2] * inv;
+  v[0] = b0 * inv; v[1] = b1 * inv; v[2] = b2 * inv;
 }
 
 template <typename T>

@@ -261,10 +261,10 @@ __device__ __forceinline__ void point_moments(float4 p, bool valid, float m[10])
 }
 
 constexpr int kRowThreads = 128;
-constexpr int kRowPix = 4;
+constexpr int kRowPix = 5;  // 128 x 5 = 640: one chunk per 640-pixel row
 
 // One CTA per image row: inclusive prefix along x of the 10 moments.  Each
-// thread keeps the points of its 4 pixels; the moments are formed twice
+// thread keeps the points of its kRowPix pixels; the moments are formed twice
 // (for the thread total, then at store time) to keep register use low.
 template <class M>
 __global__ void __launch_bounds__(kRowThreads) k_moments_rows(const FrameDev *__restrict__ frames, int nframes) {
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(32 * kColWarps) k_moments_cols(const FrameDev 
 
 // ------------------------------------------------------------ stats + omegas
 template <class M>
-__global__ void __launch_bounds__(kStatsThreads) k_stats(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(kStatsThreads, 3) k_stats(const FrameDev *__restrict__ frames, int nframes) {
   int fi = find_frame<2>(frames, nframes, blockIdx.x);
   const FrameDev &f = frames[fi];
   int pix = (blockIdx.x - f.stat_tile_base) * kStatsThreads + threadIdx.x;
