@@ -517,9 +517,12 @@ def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=4
     srv.drain(len(wmeta), timeout_s=300)
 
     out = []
-    # an unmeasured 1 s Poisson phase at 2000 requests/s first: every worker
-    # meets every resolution (pools, workspaces, first launches)
-    for rate, window, measured in [(2000.0, 1.0, False)] + [(r, seconds, True) for r in rates]:
+    # unmeasured Poisson phases first: 1 s at 2000 requests/s (every worker
+    # meets every resolution: pools, first launches), then 1 s at 10000
+    # requests/s (batches reach max size: workspaces and pools grow to their
+    # steady-state sizes before any measured rate)
+    warm = [(2000.0, 1.0, False), (10000.0, 1.0, False)]
+    for rate, window, measured in warm + [(r, seconds, True) for r in rates]:
         rng = np.random.default_rng(seed + int(rate) + (0 if measured else 7))
         n = int(min(max_requests, rate * window))
         cams = rng.choice(len(SERVE_MIX), size=n, p=shares)
@@ -601,7 +604,7 @@ def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=4
     return {"streams": len(streams), "mix": {n: s for n, s, _ in SERVE_MIX}, "budget_gb": 60, "workers": workers,
             "max_batch": 64, "submitter_threads": submitters, "arrivals": "poisson, open loop",
             "seconds_per_rate": seconds,
-            "warmup": "3 requests per stream (burst), then 1 s of Poisson arrivals at 2000 requests/s", "rates": out}
+            "warmup": "3 requests per stream (burst), then 1 s of Poisson arrivals at 2000 and 1 s at 10000 requests/s", "rates": out}
 
 
 def workload_config(args):

@@ -263,78 +263,118 @@ __device__ __forceinline__ void point_moments(float4 p, bool valid, float m[10])
 constexpr int kRowThreads = 128;
 constexpr int kRowPix = 5;  // 128 x 5 = 640: one chunk per 640-pixel row
 
-// One CTA per image row: inclusive prefix along x of the 10 moments.  Each
-// thread keeps the points of its kRowPix pixels; the moments are formed twice
-// (for the thread total, then at store time) to keep register use low.
+// One chunk of one image row (kRowThreads x kRowPix pixels from x0):
+// inclusive prefix along x of the 10 moments, starting from carry[] (the
+// chunks to its left), which is advanced by the chunk total.  Each thread
+// keeps the points of its kRowPix pixels (depths d[]); the moments are
+// formed twice (for the thread total, then per pixel for emit) to keep
+// register use low.  emit(k, c, acc) receives pixel c = x0 + t kRowPix + k
+// with its 10 prefix values.  Contains two __syncthreads.
+template <class M, class Emit>
+__device__ __forceinline__ void row_chunk_scan(const FrameDev &f, int r, int x0, const float d[kRowPix],
+                                               typename MomAcc<M>::T carry[10],
+                                               typename MomAcc<M>::T (*wtot)[10], Emit &&emit) {
+  typedef typename MomAcc<M>::T A;
+  const int cols = f.cols;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int c0 = x0 + threadIdx.x * kRowPix;
+  float4 pt[kRowPix];
+  unsigned vmask = 0;
+  A acc[10];
+#pragma unroll
+  for (int m = 0; m < 10; m++) acc[m] = A(0);
+#pragma unroll
+  for (int k = 0; k < kRowPix; k++) {
+    const int c = c0 + k;
+    const bool valid = c < cols && depth_valid(d[k], f.min_d, f.max_d);
+    pt[k] = valid ? unproject_pixel(f.iKRt, c, r, d[k]) : make_float4(0, 0, 0, 0);
+    vmask |= (valid ? 1u : 0u) << k;
+    A mk[10];
+    point_moments(pt[k], valid, mk);
+#pragma unroll
+    for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
+  }
+  // warp inclusive scan of the thread totals; acc becomes the exclusive offset
+#pragma unroll
+  for (int m = 0; m < 10; m++) {
+    A inc = acc[m];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      A y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc = inc + y;
+    }
+    if (lane == 31) wtot[wid][m] = inc;
+    acc[m] = inc - acc[m];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < 10; m++) {
+    A off = carry[m] + acc[m], tot = A(0);
+    for (int w = 0; w < kRowThreads / 32; w++) {
+      A t = wtot[w][m];
+      if (w < wid) off = off + t;
+      tot = tot + t;
+    }
+    acc[m] = off;
+    carry[m] = carry[m] + tot;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kRowPix; k++) {
+    A mk[10];
+    point_moments(pt[k], (vmask >> k) & 1u, mk);
+#pragma unroll
+    for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
+    emit(k, c0 + k, acc);
+  }
+}
+
+__device__ __forceinline__ void load_row_depths(const FrameDev &f, int r, int c0, float d[kRowPix]) {
+#pragma unroll
+  for (int k = 0; k < kRowPix; k++) d[k] = c0 + k < f.cols ? depth_of(f, r * f.cols + c0 + k) : 0.0f;
+}
+
+// One CTA per image row: inclusive prefix along x of the 10 moments.  A
+// chunk's results are staged in shared memory ([plane][column], conflict-free
+// for both the owner's 5-pixel runs and the copy-out) and written with
+// consecutive threads on consecutive columns, so that every warp store fills
+// whole sectors.
+template <class M>
+constexpr int rows_smem_bytes() { return 10 * kRowThreads * kRowPix * (int)sizeof(typename MomAcc<M>::T); }
+
 template <class M>
 __global__ void __launch_bounds__(kRowThreads) k_moments_rows(const FrameDev *__restrict__ frames, int nframes) {
   typedef typename MomAcc<M>::T A;
+  constexpr int kChunk = kRowThreads * kRowPix;
+  extern __shared__ __align__(16) unsigned char rows_raw[];
+  A *stage = reinterpret_cast<A *>(rows_raw);  // [10][kChunk]
   __shared__ A wtot[kRowThreads / 32][10];
   int fi = find_frame<1>(frames, nframes, blockIdx.x);
   const FrameDev &f = frames[fi];
-  int r = blockIdx.x - f.row_base;
-  int cols = f.cols;
-  size_t P = (size_t)f.rows * cols;
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int r = blockIdx.x - f.row_base;
+  const int cols = f.cols;
+  const size_t P = (size_t)f.rows * cols;
+  const size_t row0 = (size_t)r * cols;
   A carry[10];
 #pragma unroll
   for (int m = 0; m < 10; m++) carry[m] = A(0);
-  for (int x0 = 0; x0 < cols; x0 += kRowThreads * kRowPix) {
-    int c0 = x0 + threadIdx.x * kRowPix;
-    float4 pt[kRowPix];
-    unsigned vmask = 0;
-    A acc[10];
+  for (int x0 = 0; x0 < cols; x0 += kChunk) {
+    float d[kRowPix];
+    load_row_depths(f, r, x0 + threadIdx.x * kRowPix, d);
+    // the previous chunk's copy-out has finished with the stage once every
+    // thread has passed the first barrier inside the scan
+    row_chunk_scan<M>(f, r, x0, d, carry, wtot, [&](int, int c, const A *acc) {
 #pragma unroll
-    for (int m = 0; m < 10; m++) acc[m] = A(0);
-#pragma unroll
-    for (int k = 0; k < kRowPix; k++) {
-      int c = c0 + k;
-      bool in = c < cols;
-      float d = in ? depth_of(f, r * cols + c) : 0.0f;
-      bool valid = in && depth_valid(d, f.min_d, f.max_d);
-      pt[k] = valid ? unproject_pixel(f.iKRt, c, r, d) : make_float4(0, 0, 0, 0);
-      vmask |= (valid ? 1u : 0u) << k;
-      A mk[10];
-      point_moments(pt[k], valid, mk);
-#pragma unroll
-      for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
-    }
-    // warp inclusive scan of the thread totals; acc becomes the exclusive offset
+      for (int m = 0; m < 10; m++) stage[m * kChunk + (c - x0)] = acc[m];
+    });
+    __syncthreads();
+    const int n = min(kChunk, cols - x0);
 #pragma unroll
     for (int m = 0; m < 10; m++) {
-      A inc = acc[m];
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        A y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc = inc + y;
-      }
-      if (lane == 31) wtot[wid][m] = inc;
-      acc[m] = inc - acc[m];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int m = 0; m < 10; m++) {
-      A off = carry[m] + acc[m], tot = A(0);
-      for (int w = 0; w < kRowThreads / 32; w++) {
-        A t = wtot[w][m];
-        if (w < wid) off = off + t;
-        tot = tot + t;
-      }
-      acc[m] = off;
-      carry[m] = carry[m] + tot;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < kRowPix; k++) {
-      int c = c0 + k;
-      A mk[10];
-      point_moments(pt[k], (vmask >> k) & 1u, mk);
-#pragma unroll
-      for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
-      if (c < cols) {
-        size_t i = (size_t)r * cols + c;
-#pragma unroll
-        for (int m = 0; m < 10; m++) M::store(f.moments, m * P + i, (double)acc[m]);
+      for (int j = 0; j < kRowPix; j++) {
+        const int q = j * kRowThreads + threadIdx.x;
+        if (q < n) M::store(f.moments, m * P + row0 + x0 + q, (double)stage[m * kChunk + q]);
       }
     }
   }
@@ -651,12 +691,22 @@ void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cu
   prof->end(NICP_K_UNPROJECT, s, 2);
 }
 
+template <class M>
+static void launch_rows(const FrameDev *d_frames, int nframes, int total_rows, cudaStream_t s) {
+  static bool configured = false;  // one attribute call per instantiation
+  if (!configured) {
+    cudaFuncSetAttribute(k_moments_rows<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, rows_smem_bytes<M>());
+    configured = true;
+  }
+  k_moments_rows<M><<<total_rows, kRowThreads, rows_smem_bytes<M>(), s>>>(d_frames, nframes);
+}
+
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_rows, int total_col_ctas,
                     cudaStream_t s, Profiler *prof) {
   prof->begin(NICP_K_MOMENTS_ROWS, s);
-  if (precision == NICP_MOMENTS_F32) k_moments_rows<MomF32><<<total_rows, kRowThreads, 0, s>>>(d_frames, nframes);
-  else if (precision == NICP_MOMENTS_TWOFLOAT) k_moments_rows<MomTwoFloat><<<total_rows, kRowThreads, 0, s>>>(d_frames, nframes);
-  else k_moments_rows<MomF64><<<total_rows, kRowThreads, 0, s>>>(d_frames, nframes);
+  if (precision == NICP_MOMENTS_F32) launch_rows<MomF32>(d_frames, nframes, total_rows, s);
+  else if (precision == NICP_MOMENTS_TWOFLOAT) launch_rows<MomTwoFloat>(d_frames, nframes, total_rows, s);
+  else launch_rows<MomF64>(d_frames, nframes, total_rows, s);
   prof->end(NICP_K_MOMENTS_ROWS, s);
   prof->begin(NICP_K_MOMENTS_COLS, s);
   if (precision == NICP_MOMENTS_F32) k_moments_cols<MomF32><<<total_col_ctas, 32 * kColWarps, 0, s>>>(d_frames, nframes);
