@@ -161,7 +161,7 @@ def run_step(ctx, frames_ptrs, cam_c, prm_c, clouds, corr, lin, prm, on_device):
 
 
 # Algorithmic bytes per unit (the per-stage figures of the scope table):
-#   S1 unproject     2P + 4P + 12V          S2 moments   2P + 10 s P (+ the column pass reads and writes it)
+#   S1 unproject     2P + 4P + 12V          S2 moments   bands: 2P + 3 (10 s P / 16); sweep: 2P + 10 s P / 16 + 10 s P
 #   S3 stats + Omega 10 s P + 6P + 76V      S4 z-buffer  12V + 8V (+ 8P init, 8P resolve read, 4P write)
 #   S5 corr + lin    8P + 56 C: both index images, then per correspondence
 #                    point xyz, normal xyz and curvature of both clouds; the
@@ -172,10 +172,10 @@ def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     s = 8
     if kernel == "unproject":
         return (2 * P + 4 * P + 12 * V) * pairs
-    if kernel == "moments_rows":
-        return (2 * P + 10 * s * P) * pairs
-    if kernel == "moments_cols":
-        return (2 * 10 * s * P) * pairs
+    if kernel == "moments_bands":  # band totals (depth, totals write) + carries (read, write)
+        return (2 * P + 3 * 10 * s * P / 16) * pairs
+    if kernel == "moments_sweep":  # depth, carry rows, every integral value written once
+        return (2 * P + 10 * s * P / 16 + 10 * s * P) * pairs
     if kernel == "stats_omega":
         return (10 * s * P + 6 * P + 76 * V) * pairs
     if kernel == "zbuffer":
@@ -751,8 +751,8 @@ def main():
         "corr_lin": (8 * P + 56 * C) * npairs,
         "zbuffer": (12 * V + 8 * V) * npairs,
         "stats_omega": (10 * 8 * P + 6 * P + 76 * V) * F,
-        "moments_rows": (2 * P + 80 * P) * F,
-        "moments_cols": (160 * P) * F,
+        "moments_bands": (2 * P + 3 * 80 * P / 16) * F / 2,  # two kernels per stage launch
+        "moments_sweep": (2 * P + 80 * P / 16 + 80 * P) * F,
         "unproject": (2 * P + 4 * P + 12 * V) * F / 2,  # two kernels per stage launch
         "resolve": (12 * P) * npairs,
     }.get(top, 0.0)

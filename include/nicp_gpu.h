@@ -173,7 +173,7 @@ size_t nicp_ctx_device_bytes(const nicp_ctx *ctx);
  * every launch of the kernels below is bracketed by events; reading
  * synchronizes and resets the counters. */
 enum {
-  NICP_K_UNPROJECT = 0, NICP_K_MOMENTS_ROWS, NICP_K_MOMENTS_COLS, NICP_K_STATS,
+  NICP_K_UNPROJECT = 0, NICP_K_MOMENTS_BANDS, NICP_K_MOMENTS_SWEEP, NICP_K_STATS,
   NICP_K_ZBUFFER, NICP_K_RESOLVE, NICP_K_CORR_LIN, NICP_K_CORR_LIST, NICP_K_LIN_LIST,
   NICP_K_SOLVE, NICP_K_TRANSFORM, NICP_K_COUNT
 };

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libnicp_b200.so")
 
 NICP_OK, NICP_EINVAL, NICP_ENOMEM, NICP_EBUDGET, NICP_ETIMEOUT, NICP_ECUDA, NICP_ESTATE = range(7)
 NICP_MOMENTS_F64, NICP_MOMENTS_F32, NICP_MOMENTS_TWOFLOAT = range(3)
-KERNELS = ["unproject", "moments_rows", "moments_cols", "stats_omega", "zbuffer", "resolve", "corr_lin",
+KERNELS = ["unproject", "moments_bands", "moments_sweep", "stats_omega", "zbuffer", "resolve", "corr_lin",
            "corr_list", "lin_list", "solve", "transform"]
 K = {name: i for i, name in enumerate(KERNELS)}
 

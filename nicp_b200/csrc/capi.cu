@@ -397,7 +397,7 @@ extern "C" int nicp_ctx_transfer_bytes(const nicp_ctx *ctx, unsigned long long *
 }
 
 extern "C" const char *nicp_kernel_name(int k) {
-  static const char *names[NICP_K_COUNT] = {"unproject", "moments_rows", "moments_cols", "stats_omega",
+  static const char *names[NICP_K_COUNT] = {"unproject", "moments_bands", "moments_sweep", "stats_omega",
                                             "zbuffer",   "resolve",      "corr_lin",     "corr_list",
                                             "lin_list",  "solve",        "transform"};
   return (k >= 0 && k < NICP_K_COUNT) ? names[k] : "?";
@@ -604,7 +604,8 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     }
     int nf = i1 - i0;
     Layout L;
-    std::vector<size_t> o_stage(nf, 0), o_tiles(nf), o_mom(nf);
+    std::vector<size_t> o_stage(nf, 0), o_tiles(nf), o_mom(nf), o_band(nf);
+    const int nb_rows = moment_band_rows();
     size_t o_frames = L.take(sizeof(FrameDev) * nf);
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
@@ -615,12 +616,13 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       if (!f.on_device || !packed || !aligned) o_stage[k] = L.take(P * esz) + 1;  // +1: "staged"
       o_tiles[k] = L.take(4 * ((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
       o_mom[k] = unproject_only ? 0 : L.take(P * 10 * msz);
+      o_band[k] = unproject_only ? 0 : L.take((size_t)((f.rows + nb_rows - 1) / nb_rows) * 10 * f.cols * msz);
     }
     if ((rc = ensure_ws(ctx, L.off))) return rc;
     char *pin;
     if ((rc = pin_up(ctx, sizeof(FrameDev) * nf, &pin))) return rc;
     FrameDev *fd = reinterpret_cast<FrameDev *>(pin);
-    int tiles = 0, rowsum = 0, stiles = 0, colctas = 0;
+    int tiles = 0, bands = 0, stiles = 0, carryctas = 0;
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
       const nicp_camera &cam = cams[i0 + k];
@@ -643,13 +645,13 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.rows = f.rows;
       d.cols = f.cols;
       d.tile_base = tiles;
-      d.row_base = rowsum;
+      d.band_base = bands;
       d.stat_tile_base = stiles;
-      d.col_base = colctas;
+      d.col_base = carryctas;
       tiles += (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels);
-      rowsum += f.rows;
+      bands += (f.rows + nb_rows - 1) / nb_rows;
       stiles += (int)((P + kStatsThreads - 1) / kStatsThreads);
-      colctas += 10 * ((f.cols + 31) / 32);
+      carryctas += (10 * f.cols + 127) / 128;
       d.depth_scale = prm->depth_scale;
       d.min_d = cam.min_distance;
       d.max_d = cam.max_distance;
@@ -694,6 +696,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.count = cl->count;
       d.tile_counts = (int *)(ctx->ws + o_tiles[k]);
       d.moments = unproject_only ? nullptr : (void *)(ctx->ws + o_mom[k]);
+      d.band_tot = unproject_only ? nullptr : (void *)(ctx->ws + o_band[k]);
     }
     FrameDev *dfr = (FrameDev *)(ctx->ws + o_frames);
     CK(ctx, cudaMemcpyAsync(dfr, pin, sizeof(FrameDev) * nf, cudaMemcpyHostToDevice, s));
@@ -701,7 +704,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
     launch_unproject(dfr, nf, tiles, s, &ctx->prof);
     if (!unproject_only) {
-      launch_moments(prm->moments_precision, dfr, nf, rowsum, colctas, s, &ctx->prof);
+      launch_moments(prm->moments_precision, dfr, nf, bands, carryctas, s, &ctx->prof);
       launch_stats(prm->moments_precision, dfr, nf, stiles, s, &ctx->prof);
     }
     CK(ctx, cudaGetLastError());

@@ -53,9 +53,9 @@ struct FrameDev {
   const float *depth_f32;
   int rows, cols;
   int tile_base;              // first unprojection tile of this frame in the grid
-  int row_base;               // first image row of this frame in the row grid
+  int band_base;              // first 16-row moment band of this frame in the band grid
   int stat_tile_base;         // first stats tile of this frame
-  int col_base;               // first column-scan CTA of this frame (10 planes x strips)
+  int col_base;               // first band-carry CTA of this frame (128 of its 10 x cols columns each)
   float depth_scale;
   float min_d, max_d;
   float iKRt[12];             // unprojection matrix (rows 0..2 of 4x4)
@@ -77,6 +77,7 @@ struct FrameDev {
   // scratch
   int *tile_counts;           // per unprojection tile
   void *moments;              // 10 planes of rows*cols values (double / float / float2)
+  void *band_tot;             // per 16-row band: 10 x cols totals, then carries (double / float)
 };
 
 // ---- per-pair device state of the Gauss-Newton loop

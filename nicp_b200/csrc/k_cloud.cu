@@ -7,12 +7,12 @@
 //       128-bit loads.  The first pass counts valid pixels per tile, the second
 //       re-reads the tile (from L2), sums the counts of the preceding tiles of
 //       its frame and writes indices and points at their final positions.
-//   k_moments_rows / k_moments_cols
+//   k_moments_band_totals / k_moments_band_carry / k_moments_band_sweep
 //       integral image of the 10 unique point moments (n, Sx, Sy, Sz, Sxx,
 //       Sxy, Sxz, Syy, Syz, Szz) -- pointintegralimage.cpp:7-44 -- as 10
-//       planes.  Rows: one CTA per image row, block scans with carries.
-//       Columns: one CTA per (plane, 32-column strip); each warp scans a band
-//       of rows, band totals are combined through shared memory.
+//       planes, over bands of 16 image rows: band column totals, their
+//       prefix over the bands, then one sweep per band that writes every
+//       value once.
 //   k_stats
 //       one thread per pixel: interval radius, 4-corner box query, FP64 3x3
 //       covariance and eigensolve, curvature, oriented normal, and both
@@ -31,7 +31,7 @@ namespace nicp {
 template <int Field>
 __device__ __forceinline__ int frame_base(const FrameDev &f) {
   if (Field == 0) return f.tile_base;
-  if (Field == 1) return f.row_base;
+  if (Field == 1) return f.band_base;
   if (Field == 2) return f.stat_tile_base;
   return f.col_base;
 }
@@ -329,107 +329,217 @@ __device__ __forceinline__ void row_chunk_scan(const FrameDev &f, int r, int x0,
   }
 }
 
-__device__ __forceinline__ void load_row_depths(const FrameDev &f, int r, int c0, float d[kRowPix]) {
+// Raw depth words (u16 value or float bits), loaded ahead of use; the
+// conversion happens where the depth is consumed, so that a prefetch does
+// not wait for its own load.
+__device__ __forceinline__ unsigned depth_raw(const FrameDev &f, int pix) {
+  return f.depth_u16 ? (unsigned)f.depth_u16[pix] : __float_as_uint(f.depth_f32[pix]);
+}
+__device__ __forceinline__ float depth_from_raw(const FrameDev &f, unsigned w) {
+  if (f.depth_u16) return w ? fm(f.depth_scale, (float)(int)w) : 0.0f;
+  return __uint_as_float(w);
+}
+__device__ __forceinline__ void load_row_raw(const FrameDev &f, int r, int c0, unsigned w[kRowPix]) {
 #pragma unroll
-  for (int k = 0; k < kRowPix; k++) d[k] = c0 + k < f.cols ? depth_of(f, r * f.cols + c0 + k) : 0.0f;
+  for (int k = 0; k < kRowPix; k++) w[k] = c0 + k < f.cols ? depth_raw(f, r * f.cols + c0 + k) : 0u;
 }
 
-// One CTA per image row: inclusive prefix along x of the 10 moments.  A
-// chunk's results are staged in shared memory ([plane][column], conflict-free
-// for both the owner's 5-pixel runs and the copy-out) and written with
-// consecutive threads on consecutive columns, so that every warp store fills
-// whole sectors.
-template <class M>
-constexpr int rows_smem_bytes() { return 10 * kRowThreads * kRowPix * (int)sizeof(typename MomAcc<M>::T); }
+// ---- integral image in three passes over bands of kBandRows image rows.
+// With R(r, c) the prefix along x of row r, the integral image is
+// I(r, c) = carry_b(c) + the sum of R(r', c) over the rows r' <= r of r's
+// band b, where carry_b(c) = the sum over the bands above of their column
+// totals.
+//   k_moments_band_totals  per band: column sums of the raw moments over the
+//                          band's rows, then their prefix along x (= the
+//                          sum of the band's row prefixes)
+//   k_moments_band_carry   per (plane, column): exclusive prefix of the
+//                          band totals over the bands, in place
+//   k_moments_band_sweep   per band: row prefixes (row_chunk_scan) added
+//                          down the band onto carry_b; every integral value
+//                          is written once, from shared memory, coalesced
+constexpr int kBandRows = 16;
+constexpr int kChunkPix = kRowThreads * kRowPix;
 
 template <class M>
-__global__ void __launch_bounds__(kRowThreads) k_moments_rows(const FrameDev *__restrict__ frames, int nframes) {
+constexpr int band_smem_bytes() { return 10 * kChunkPix * (int)sizeof(typename MomAcc<M>::T); }
+
+template <class M>
+__global__ void __launch_bounds__(kRowThreads) k_moments_band_totals(const FrameDev *__restrict__ frames, int nframes) {
   typedef typename MomAcc<M>::T A;
-  constexpr int kChunk = kRowThreads * kRowPix;
-  extern __shared__ __align__(16) unsigned char rows_raw[];
-  A *stage = reinterpret_cast<A *>(rows_raw);  // [10][kChunk]
+  extern __shared__ __align__(16) unsigned char band_raw[];
+  A *cs = reinterpret_cast<A *>(band_raw);  // [10][kChunkPix]
   __shared__ A wtot[kRowThreads / 32][10];
-  int fi = find_frame<1>(frames, nframes, blockIdx.x);
+  const int fi = find_frame<1>(frames, nframes, blockIdx.x);
   const FrameDev &f = frames[fi];
-  const int r = blockIdx.x - f.row_base;
+  const int b = blockIdx.x - f.band_base;
   const int cols = f.cols;
-  const size_t P = (size_t)f.rows * cols;
-  const size_t row0 = (size_t)r * cols;
+  const int r0 = b * kBandRows, nr = min(f.rows - r0, kBandRows);
+  A *tot = static_cast<A *>(f.band_tot) + (size_t)b * 10 * cols;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   A carry[10];
 #pragma unroll
   for (int m = 0; m < 10; m++) carry[m] = A(0);
-  for (int x0 = 0; x0 < cols; x0 += kChunk) {
-    float d[kRowPix];
-    load_row_depths(f, r, x0 + threadIdx.x * kRowPix, d);
-    // the previous chunk's copy-out has finished with the stage once every
-    // thread has passed the first barrier inside the scan
-    row_chunk_scan<M>(f, r, x0, d, carry, wtot, [&](int, int c, const A *acc) {
+  for (int x0 = 0; x0 < cols; x0 += kChunkPix) {
+    const int n = min(kChunkPix, cols - x0);
+    // column sums over the band (thread t: columns x0 + t + kRowThreads j)
+#pragma unroll 1
+    for (int j = 0; j < kRowPix; j++) {
+      const int q = j * kRowThreads + t;
+      A acc[10];
 #pragma unroll
-      for (int m = 0; m < 10; m++) stage[m * kChunk + (c - x0)] = acc[m];
-    });
+      for (int m = 0; m < 10; m++) acc[m] = A(0);
+      if (q < n) {
+        const int c = x0 + q;
+        unsigned w[kBandRows];
+#pragma unroll
+        for (int i = 0; i < kBandRows; i++) w[i] = i < nr ? depth_raw(f, (r0 + i) * cols + c) : 0u;
+#pragma unroll
+        for (int i = 0; i < kBandRows; i++) {
+          const float d = depth_from_raw(f, w[i]);
+          const bool valid = i < nr && depth_valid(d, f.min_d, f.max_d);
+          const float4 p = valid ? unproject_pixel(f.iKRt, c, r0 + i, d) : make_float4(0, 0, 0, 0);
+          A mk[10];
+          point_moments(p, valid, mk);
+#pragma unroll
+          for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 10; m++) cs[m * kChunkPix + q] = acc[m];
+    }
     __syncthreads();
-    const int n = min(kChunk, cols - x0);
+    // inclusive prefix along x of the column sums, in place (thread t:
+    // entries t kRowPix .. t kRowPix + kRowPix - 1)
+    A loc[10];
 #pragma unroll
     for (int m = 0; m < 10; m++) {
+      A sum = A(0);
 #pragma unroll
-      for (int j = 0; j < kRowPix; j++) {
-        const int q = j * kRowThreads + threadIdx.x;
-        if (q < n) M::store(f.moments, m * P + row0 + x0 + q, (double)stage[m * kChunk + q]);
+      for (int k = 0; k < kRowPix; k++) sum = sum + cs[m * kChunkPix + t * kRowPix + k];
+      A inc = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        A y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc = inc + y;
+      }
+      if (lane == 31) wtot[wid][m] = inc;
+      loc[m] = inc - sum;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 10; m++) {
+      A off = carry[m] + loc[m], all = A(0);
+      for (int w = 0; w < kRowThreads / 32; w++) {
+        const A v = wtot[w][m];
+        if (w < wid) off = off + v;
+        all = all + v;
+      }
+      carry[m] = carry[m] + all;
+#pragma unroll
+      for (int k = 0; k < kRowPix; k++) {
+        off = off + cs[m * kChunkPix + t * kRowPix + k];
+        cs[m * kChunkPix + t * kRowPix + k] = off;
       }
     }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 10; m++)
+#pragma unroll
+      for (int j = 0; j < kRowPix; j++) {
+        const int q = j * kRowThreads + t;
+        if (q < n) tot[(size_t)m * cols + x0 + q] = cs[m * kChunkPix + q];
+      }
+    __syncthreads();  // the copy-out has read cs before the next chunk overwrites it
   }
 }
 
-constexpr int kColWarps = 8;
-constexpr int kColBatch = 8;
-
-// One CTA per (plane, 32-column strip): inclusive prefix along y.  Each warp
-// scans a band of rows (lane = column), loading kColBatch rows ahead; band
-// totals are combined through shared memory and added in a second pass.
+// One thread per (plane, column) of a frame: band totals -> band carries.
 template <class M>
-__global__ void __launch_bounds__(32 * kColWarps) k_moments_cols(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(128) k_moments_band_carry(const FrameDev *__restrict__ frames, int nframes) {
   typedef typename MomAcc<M>::T A;
-  __shared__ A btot[kColWarps][32];
-  int fi = find_frame<3>(frames, nframes, blockIdx.x);
+  constexpr int kAhead = 8;
+  const int fi = find_frame<3>(frames, nframes, blockIdx.x);
   const FrameDev &f = frames[fi];
-  int local = blockIdx.x - f.col_base;
-  int strips = (f.cols + 31) / 32;
-  int plane = local / strips, strip = local - plane * strips;
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int x = strip * 32 + lane;
-  int rows = f.rows, cols = f.cols;
-  size_t P = (size_t)rows * cols;
-  int band = (rows + kColWarps - 1) / kColWarps;
-  int y0 = wid * band, y1 = min(rows, y0 + band);
-  size_t base = (size_t)plane * P + x;
-  A s = A(0);
-  if (x < cols) {
-    for (int y = y0; y < y1; y += kColBatch) {
-      A v[kColBatch];
+  const int q = (blockIdx.x - f.col_base) * 128 + threadIdx.x;
+  const size_t stride = (size_t)10 * f.cols;
+  if (q >= (int)stride) return;
+  const int nb = (f.rows + kBandRows - 1) / kBandRows;
+  A *tot = static_cast<A *>(f.band_tot) + q;
+  A acc = A(0);
+  for (int b0 = 0; b0 < nb; b0 += kAhead) {
+    A v[kAhead];
 #pragma unroll
-      for (int k = 0; k < kColBatch; k++)
-        v[k] = (y + k < y1) ? (A)M::load(f.moments, base + (size_t)(y + k) * cols) : A(0);
+    for (int k = 0; k < kAhead; k++) v[k] = b0 + k < nb ? tot[(size_t)(b0 + k) * stride] : A(0);
 #pragma unroll
-      for (int k = 0; k < kColBatch; k++) {
-        s = s + v[k];
-        if (y + k < y1) M::store(f.moments, base + (size_t)(y + k) * cols, (double)s);
+    for (int k = 0; k < kAhead; k++)
+      if (b0 + k < nb) {
+        tot[(size_t)(b0 + k) * stride] = acc;
+        acc = acc + v[k];
       }
-    }
   }
-  btot[wid][lane] = s;
-  __syncthreads();
-  A carry = A(0);
-  for (int w = 0; w < wid; w++) carry = carry + btot[w][lane];
-  if (x < cols && wid > 0) {
-    for (int y = y0; y < y1; y += kColBatch) {
-      A v[kColBatch];
+}
+
+template <class M>
+__global__ void __launch_bounds__(kRowThreads) k_moments_band_sweep(const FrameDev *__restrict__ frames, int nframes) {
+  typedef typename MomAcc<M>::T A;
+  extern __shared__ __align__(16) unsigned char band_raw[];
+  A *state = reinterpret_cast<A *>(band_raw);  // [10][kChunkPix]: I(r, c) of the current row
+  __shared__ A wtot[kRowThreads / 32][10];
+  __shared__ A rowc[kBandRows][10];  // row carries across chunks (frames wider than a chunk)
+  const int fi = find_frame<1>(frames, nframes, blockIdx.x);
+  const FrameDev &f = frames[fi];
+  const int b = blockIdx.x - f.band_base;
+  const int cols = f.cols;
+  const size_t P = (size_t)f.rows * cols;
+  const int r0 = b * kBandRows, r1 = min(f.rows, r0 + kBandRows);
+  const A *carry_b = static_cast<const A *>(f.band_tot) + (size_t)b * 10 * cols;
+  const int t = threadIdx.x;
+  for (int x0 = 0; x0 < cols; x0 += kChunkPix) {
+    const int n = min(kChunkPix, cols - x0);
+    const int c0 = x0 + t * kRowPix;
+    // the band's carry row; made visible to the owners of the columns by the
+    // first barrier inside the first scan
 #pragma unroll
-      for (int k = 0; k < kColBatch; k++)
-        v[k] = (y + k < y1) ? (A)M::load(f.moments, base + (size_t)(y + k) * cols) : A(0);
+    for (int m = 0; m < 10; m++)
 #pragma unroll
-      for (int k = 0; k < kColBatch; k++)
-        if (y + k < y1) M::store(f.moments, base + (size_t)(y + k) * cols, (double)(v[k] + carry));
+      for (int j = 0; j < kRowPix; j++) {
+        const int q = j * kRowThreads + t;
+        state[m * kChunkPix + q] = q < n ? carry_b[(size_t)m * cols + x0 + q] : A(0);
+      }
+    unsigned wn[kRowPix];
+    load_row_raw(f, r0, c0, wn);
+    for (int r = r0; r < r1; r++) {
+      float d[kRowPix];
+#pragma unroll
+      for (int k = 0; k < kRowPix; k++) d[k] = depth_from_raw(f, wn[k]);
+      if (r + 1 < r1) load_row_raw(f, r + 1, c0, wn);
+      A carry[10];
+#pragma unroll
+      for (int m = 0; m < 10; m++) carry[m] = x0 ? rowc[r - r0][m] : A(0);
+      // every thread has finished the previous row's copy-out once it has
+      // passed the first barrier inside the scan
+      row_chunk_scan<M>(f, r, x0, d, carry, wtot, [&](int, int c, const A *acc) {
+        if (c < cols) {
+#pragma unroll
+          for (int m = 0; m < 10; m++)
+            state[m * kChunkPix + (c - x0)] = state[m * kChunkPix + (c - x0)] + acc[m];
+        }
+      });
+      if (t == 0 && x0 + kChunkPix < cols) {
+#pragma unroll
+        for (int m = 0; m < 10; m++) rowc[r - r0][m] = carry[m];
+      }
+      __syncthreads();
+      const size_t row0 = (size_t)r * cols + x0;
+#pragma unroll
+      for (int m = 0; m < 10; m++)
+#pragma unroll
+        for (int j = 0; j < kRowPix; j++) {
+          const int q = j * kRowThreads + t;
+          if (q < n) M::store(f.moments, m * P + row0 + q, (double)state[m * kChunkPix + q]);
+        }
     }
+    __syncthreads();  // the last copy-out has read the state before the next chunk's carry row
   }
 }
 
@@ -692,27 +802,31 @@ void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cu
 }
 
 template <class M>
-static void launch_rows(const FrameDev *d_frames, int nframes, int total_rows, cudaStream_t s) {
+static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas, cudaStream_t s,
+                         Profiler *prof) {
   static bool configured = false;  // one attribute call per instantiation
   if (!configured) {
-    cudaFuncSetAttribute(k_moments_rows<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, rows_smem_bytes<M>());
+    cudaFuncSetAttribute(k_moments_band_totals<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes<M>());
+    cudaFuncSetAttribute(k_moments_band_sweep<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes<M>());
     configured = true;
   }
-  k_moments_rows<M><<<total_rows, kRowThreads, rows_smem_bytes<M>(), s>>>(d_frames, nframes);
+  prof->begin(NICP_K_MOMENTS_BANDS, s);
+  k_moments_band_totals<M><<<total_bands, kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, nframes);
+  k_moments_band_carry<M><<<total_carry_ctas, 128, 0, s>>>(d_frames, nframes);
+  prof->end(NICP_K_MOMENTS_BANDS, s, 2);
+  prof->begin(NICP_K_MOMENTS_SWEEP, s);
+  k_moments_band_sweep<M><<<total_bands, kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, nframes);
+  prof->end(NICP_K_MOMENTS_SWEEP, s);
 }
 
-void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_rows, int total_col_ctas,
+int moment_band_rows() { return kBandRows; }
+
+void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
                     cudaStream_t s, Profiler *prof) {
-  prof->begin(NICP_K_MOMENTS_ROWS, s);
-  if (precision == NICP_MOMENTS_F32) launch_rows<MomF32>(d_frames, nframes, total_rows, s);
-  else if (precision == NICP_MOMENTS_TWOFLOAT) launch_rows<MomTwoFloat>(d_frames, nframes, total_rows, s);
-  else launch_rows<MomF64>(d_frames, nframes, total_rows, s);
-  prof->end(NICP_K_MOMENTS_ROWS, s);
-  prof->begin(NICP_K_MOMENTS_COLS, s);
-  if (precision == NICP_MOMENTS_F32) k_moments_cols<MomF32><<<total_col_ctas, 32 * kColWarps, 0, s>>>(d_frames, nframes);
-  else if (precision == NICP_MOMENTS_TWOFLOAT) k_moments_cols<MomTwoFloat><<<total_col_ctas, 32 * kColWarps, 0, s>>>(d_frames, nframes);
-  else k_moments_cols<MomF64><<<total_col_ctas, 32 * kColWarps, 0, s>>>(d_frames, nframes);
-  prof->end(NICP_K_MOMENTS_COLS, s);
+  if (precision == NICP_MOMENTS_F32) launch_bands<MomF32>(d_frames, nframes, total_bands, total_carry_ctas, s, prof);
+  else if (precision == NICP_MOMENTS_TWOFLOAT)
+    launch_bands<MomTwoFloat>(d_frames, nframes, total_bands, total_carry_ctas, s, prof);
+  else launch_bands<MomF64>(d_frames, nframes, total_bands, total_carry_ctas, s, prof);
 }
 
 void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof) {

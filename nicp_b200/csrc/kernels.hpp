@@ -63,7 +63,10 @@ struct Profiler {
 void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof);
 void launch_depth_scale(const uint16_t *u16, const float *f32, size_t pitch_elems, int rows, int cols,
                         float depth_scale, int step, float max_cov, float *out, cudaStream_t s);
-void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_rows, int total_col_ctas,
+// Integral image over 16-row bands (moment_band_rows()): total_bands band
+// CTAs, total_carry_ctas = sum over frames of ceil(10 cols / 128).
+int moment_band_rows();
+void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
                     cudaStream_t s, Profiler *prof);
 void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s,
                   Profiler *prof);

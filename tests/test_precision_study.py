@@ -35,7 +35,7 @@ from helpers import (angle_between, cams, converter, decision_stable_pixels, flo
 pytestmark = pytest.mark.gpu
 
 MOMENTS = [("fp64", L.NICP_MOMENTS_F64), ("twofloat", L.NICP_MOMENTS_TWOFLOAT), ("fp32", L.NICP_MOMENTS_F32)]
-BUILD_KERNELS = ("unproject", "moments_rows", "moments_cols", "stats_omega")
+BUILD_KERNELS = ("unproject", "moments_bands", "moments_sweep", "stats_omega")
 
 
 def _rel(a, b):
