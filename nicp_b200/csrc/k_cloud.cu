@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(128) k_moments_band_carry(const FrameDev *__re
 }
 
 template <class M>
-__global__ void __launch_bounds__(kRowThreads) k_moments_band_sweep(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const FrameDev *__restrict__ frames, int nframes) {
   typedef typename MomAcc<M>::T A;
   extern __shared__ __align__(16) unsigned char band_raw[];
   A *state = reinterpret_cast<A *>(band_raw);  // [10][kChunkPix]: I(r, c) of the current row
