@@ -1630,7 +1630,7 @@ static int autotune_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a, 
     c.zb_ppt = ppts[i];
     if (!(rc = trial(c, &ms)) && ms < best_ms) { best_ms = ms; *best = c; }
   }
-  const int ctas[] = {1, 2};
+  const int ctas[] = {2, 3};  // fused kernel CTAs (128 threads) per SM
   for (int i = 0; i < 2 && !rc; i++) {
     nicp_ctx::Launch c = *best;
     c.corr_ctas = ctas[i];

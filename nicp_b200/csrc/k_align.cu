@@ -304,8 +304,9 @@ __device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const 
 }
 
 // Reduces every thread's Acc to one FP64 partial of the CTA (fixed order).
+template <int kThreads>
 __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) {
-  __shared__ double wsum[kCorrThreads / 32][32];
+  __shared__ double wsum[kThreads / 32][32];
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double v[32];
 #pragma unroll
@@ -327,7 +328,7 @@ __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) 
   if (wid == 0) {
     double s = 0.0;
 #pragma unroll
-    for (int w = 0; w < kCorrThreads / 32; w++) s += wsum[w][lane];
+    for (int w = 0; w < kThreads / 32; w++) s += wsum[w][lane];
     out[lane] = s;
   }
 }
@@ -336,29 +337,34 @@ __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) 
 // A pair image is cut into tiles of kCorrTilePixels; every tile yields one
 // FP64 partial, so results do not depend on the grid or the batch.  A CTA
 // walks its tiles (blockIdx.x, +gridDim.x, ...) in sub-tiles of 256 pixels
-// (one per thread).  For each pixel the thread reads the two indices, then
+// (kFusedPX per thread, at slots t and t + kFusedThreads, so that every
+// access of one slot row is coalesced; the per-sub-tile bookkeeping and the
+// per-tile reduction are shared by a thread's pixels).  For each pixel the
+// thread reads the two indices, then
 // stages the 7 gathered float4 (reference point and normal, current point
 // and normal, 3 x Omega) into its own shared-memory slot with cp.async;
 // kCorrStages sub-tiles are in flight while the oldest one is gated and
 // linearized.  Each thread reads back only what it copied itself, so the
 // pipeline needs no barrier.
-constexpr int kSubPix = kCorrThreads;                    // pixels per sub-tile
+constexpr int kFusedThreads = 128;
+constexpr int kFusedPX = 2;
+constexpr int kSubPix = kFusedThreads * kFusedPX;        // pixels per sub-tile
 constexpr int kSubsPerTile = kCorrTilePixels / kSubPix;  // 4
 constexpr int kCorrStages = 3;
 
-// Structure-of-arrays stage: thread t owns element t of every array, so a
-// warp's accesses to one field are consecutive 16-byte words (no bank
-// conflicts).
+// Structure-of-arrays stage: thread t owns slots t + k kFusedThreads of
+// every array, so a warp's accesses to one field are consecutive 16-byte
+// words (no bank conflicts).
 struct GatherStageS {  // structured Omega: rebuilt from the current normal
-  float4 rp[kCorrThreads], rn[kCorrThreads], cp[kCorrThreads], cn[kCorrThreads];
-  int valid[kCorrThreads];
+  float4 rp[kSubPix], rn[kSubPix], cp[kSubPix], cn[kSubPix];
+  int valid[kSubPix];
 };
 struct GatherStageG : GatherStageS {  // general Omega: gathered for accepted pixels
-  float4 o0[kCorrThreads], o1[kCorrThreads], o2[kCorrThreads];
-  int ci[kCorrThreads];
+  float4 o0[kSubPix], o1[kSubPix], o2[kSubPix];
+  int ci[kSubPix];
 };
 #ifndef NICP_CORR_S_CTAS
-#define NICP_CORR_S_CTAS 3
+#define NICP_CORR_S_CTAS 4
 #endif
 template <bool kStructured>
 using GatherStage = typename std::conditional<kStructured, GatherStageS, GatherStageG>::type;
@@ -381,7 +387,7 @@ __device__ __forceinline__ void cp_async_wait() {
 // kStructured: every pair's current cloud has structured information
 // matrices (no Omega gathers, smaller stages).
 template <bool kStructured>
-__global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS : 2)
+__global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS : 3)
     k_corr_lin(const PairDev *__restrict__ pairs, int npairs, int total_tiles, CorrParams cp, LinParams lp,
                int flags) {
   extern __shared__ __align__(16) unsigned char corr_smem_raw[];
@@ -414,65 +420,88 @@ __global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS :
   };
 
   // Phase I (one iteration ahead, plain loads into registers): the two index
-  // words of sub-tile j.
-  unsigned long long zI = ~0ull;
-  int cI = -1;
+  // words of the thread's pixels of sub-tile j.
+  unsigned long long zI[kFusedPX];
+  int cI[kFusedPX];
   auto load_indices = [&](int j) {
-    zI = ~0ull;
-    cI = -1;
+#pragma unroll
+    for (int k = 0; k < kFusedPX; k++) {
+      zI[k] = ~0ull;
+      cI[k] = -1;
+    }
     if (j >= nsub) return;
     int tile = tile_of(j);
     lookup(tile, lt_tile, lt_pi, lt_skip);
     if (lt_skip) return;
     const PairDev &pd = pairs[lt_pi];
-    int p = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + threadIdx.x;
-    if (p >= pd.rows * pd.cols) return;
-    if (flags & 1) zI = pd.zbuf[p];
-    else cI = pd.ref_index[p];  // stashed in cI until phase G1 reads the current index
-    if (flags & 1) cI = pd.cur_index[p];
-    else zI = (unsigned long long)(unsigned)pd.cur_index[p];
+    const int P = pd.rows * pd.cols;
+    const int p0 = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + t;
+#pragma unroll
+    for (int k = 0; k < kFusedPX; k++) {
+      const int p = p0 + k * kFusedThreads;
+      if (p < P) {
+        if (flags & 1) zI[k] = pd.zbuf[p];
+        else cI[k] = pd.ref_index[p];  // stashed in cI until phase G1 reads the current index
+        if (flags & 1) cI[k] = pd.cur_index[p];
+        else zI[k] = (unsigned long long)(unsigned)pd.cur_index[p];
+      }
+    }
   };
 
   // Phase G1 (two sub-tiles ahead): decode the indices, reset the z-buffer,
   // gather points and normals of both clouds.
   auto issue_g1 = [&](int j) {
     Stage &g = stage_of(j);
-    int ri = -1, ci = -1, valid = 0;
+    int ci[kFusedPX], valid[kFusedPX];
+#pragma unroll
+    for (int k = 0; k < kFusedPX; k++) {
+      ci[k] = -1;
+      valid[k] = 0;
+    }
     if (j < nsub) {
       int tile = tile_of(j);
       lookup(tile, gt_tile, gt_pi, gt_skip);
       const PairDev &pd = pairs[gt_pi];
       if (!gt_skip) {
-        int p = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + threadIdx.x;
-        if (p < pd.rows * pd.cols) {
-          if (flags & 1) {
-            ri = zbuf_index(zI, drop_no_normal);
-            ci = cI;
-            if (flags & 2) pd.zbuf[p] = ~0ull;
-            if (flags & 4) pd.ref_index[p] = ri;
-          } else {
-            ri = cI;
-            ci = (int)(unsigned)zI;
-          }
-          if (gt_ctile != tile) {  // point counts, read once per tile
-            gt_ctile = tile;
-            gt_rc = *pd.ref_count;
-            gt_cc = *pd.cur_count;
-          }
-          valid = ri >= 0 && ci >= 0 && ri < gt_rc && ci < gt_cc;
-          if (valid && cp.row_limit_threads > 1)
-            valid = p / pd.cols < (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
-          if (valid) {
-            cp_async16(&g.rp[t], pd.ref_pts + ri);
-            cp_async16(&g.rn[t], pd.ref_nrm + ri);
-            cp_async16(&g.cp[t], pd.cur_pts + ci);
-            cp_async16(&g.cn[t], pd.cur_nrm + ci);
+        if (gt_ctile != tile) {  // point counts, read once per tile
+          gt_ctile = tile;
+          gt_rc = *pd.ref_count;
+          gt_cc = *pd.cur_count;
+        }
+        const int P = pd.rows * pd.cols;
+        const int p0 = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + t;
+#pragma unroll
+        for (int k = 0; k < kFusedPX; k++) {
+          const int p = p0 + k * kFusedThreads, sl = t + k * kFusedThreads;
+          if (p < P) {
+            int ri;
+            if (flags & 1) {
+              ri = zbuf_index(zI[k], drop_no_normal);
+              ci[k] = cI[k];
+              if (flags & 2) pd.zbuf[p] = ~0ull;
+              if (flags & 4) pd.ref_index[p] = ri;
+            } else {
+              ri = cI[k];
+              ci[k] = (int)(unsigned)zI[k];
+            }
+            valid[k] = ri >= 0 && ci[k] >= 0 && ri < gt_rc && ci[k] < gt_cc;
+            if (valid[k] && cp.row_limit_threads > 1)
+              valid[k] = p / pd.cols < (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
+            if (valid[k]) {
+              cp_async16(&g.rp[sl], pd.ref_pts + ri);
+              cp_async16(&g.rn[sl], pd.ref_nrm + ri);
+              cp_async16(&g.cp[sl], pd.cur_pts + ci[k]);
+              cp_async16(&g.cn[sl], pd.cur_nrm + ci[k]);
+            }
           }
         }
       }
     }
-    if constexpr (!kStructured) g.ci[t] = ci;
-    g.valid[t] = valid;
+#pragma unroll
+    for (int k = 0; k < kFusedPX; k++) {
+      if constexpr (!kStructured) g.ci[t + k * kFusedThreads] = ci[k];
+      g.valid[t + k * kFusedThreads] = valid[k];
+    }
     cp_async_commit();
   };
 
@@ -513,18 +542,23 @@ __global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS :
         cp_async_commit();
         return;
       }
-      if (g.valid[t] && !sSkip[e]) {
-        acc_ok = gate(cp, sT[e], g.rp[t], g.rn[t], g.cp[t], g.cn[t]) ? 2 : 1;
-        if constexpr (!kStructured) {
-          if (acc_ok == 2 && !sStruct[e]) {
-            const float4 *o = pairs[sPair[e]].cur_omg + 3 * (size_t)g.ci[t];
-            cp_async16(&g.o0[t], o);
-            cp_async16(&g.o1[t], o + 1);
-            cp_async16(&g.o2[t], o + 2);
+#pragma unroll
+      for (int k = 0; k < kFusedPX; k++) {
+        const int sl = t + k * kFusedThreads;
+        acc_ok = 0;
+        if (g.valid[sl] && !sSkip[e]) {
+          acc_ok = gate(cp, sT[e], g.rp[sl], g.rn[sl], g.cp[sl], g.cn[sl]) ? 2 : 1;
+          if constexpr (!kStructured) {
+            if (acc_ok == 2 && !sStruct[e]) {
+              const float4 *o = pairs[sPair[e]].cur_omg + 3 * (size_t)g.ci[sl];
+              cp_async16(&g.o0[sl], o);
+              cp_async16(&g.o1[sl], o + 1);
+              cp_async16(&g.o2[sl], o + 2);
+            }
           }
         }
+        g.valid[sl] = acc_ok;  // 0 none, 1 candidate rejected, 2 accepted
       }
-      g.valid[t] = acc_ok;  // 0 none, 1 candidate rejected, 2 accepted
     }
     cp_async_commit();
   };
@@ -559,33 +593,38 @@ __global__ void __launch_bounds__(kCorrThreads, kStructured ? NICP_CORR_S_CTAS :
     }
     if (!sSkip[e]) {
       const Stage &g = stage_of(j);
-      const int v = g.valid[t];
-      if constexpr (kStructured) {
-        if (v) {
-          acc.v[29] += 1.0f;
-          const float4 rp0 = g.rp[t], rn0 = g.rn[t], cpt = g.cp[t], cn = g.cn[t];
-          float3 rp, rn;
-          if (gate_t(cp, sT[e], rp0, rn0, cpt, cn, rp, rn)) {
-            acc.v[30] += 1.0f;
-            if (sSame[e] && !cp.demoted)
-              lin_terms_structured_xf(lp, sT[e] + 24, rp, rn, cpt, cn, acc);
-            else
-              lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, rp0, rn0, cpt, cn, acc);
+#pragma unroll
+      for (int k = 0; k < kFusedPX; k++) {
+        const int sl = t + k * kFusedThreads;
+        const int v = g.valid[sl];
+        if constexpr (kStructured) {
+          if (v) {
+            acc.v[29] += 1.0f;
+            const float4 rp0 = g.rp[sl], rn0 = g.rn[sl], cpt = g.cp[sl], cn = g.cn[sl];
+            float3 rp, rn;
+            if (gate_t(cp, sT[e], rp0, rn0, cpt, cn, rp, rn)) {
+              acc.v[30] += 1.0f;
+              if (sSame[e] && !cp.demoted)
+                lin_terms_structured_xf(lp, sT[e] + 24, rp, rn, cpt, cn, acc);
+              else
+                lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, rp0, rn0, cpt, cn, acc);
+            }
           }
-        }
-      } else {
-        if (v) acc.v[29] += 1.0f;
-        if (v == 2) {
-          acc.v[30] += 1.0f;
-          if (sStruct[e])
-            lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, g.rp[t], g.rn[t], g.cp[t], g.cn[t], acc);
-          else
-            lin_terms(lp, sT[e] + 12, g.rp[t], g.rn[t], g.cp[t], g.cn[t], g.o0[t], g.o1[t], g.o2[t], acc);
+        } else {
+          if (v) acc.v[29] += 1.0f;
+          if (v == 2) {
+            acc.v[30] += 1.0f;
+            if (sStruct[e])
+              lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, g.rp[sl], g.rn[sl], g.cp[sl], g.cn[sl], acc);
+            else
+              lin_terms(lp, sT[e] + 12, g.rp[sl], g.rn[sl], g.cp[sl], g.cn[sl], g.o0[sl], g.o1[sl], g.o2[sl],
+                        acc);
+          }
         }
       }
       if (sub == kSubsPerTile - 1) {
         const PairDev &pd = pairs[sPair[e]];
-        block_reduce_store(acc, pd.partials + (size_t)(tile_of(j) - pd.tile_base) * kPartialWords);
+        block_reduce_store<kFusedThreads>(acc, pd.partials + (size_t)(tile_of(j) - pd.tile_base) * kPartialWords);
       }
     }
   }
@@ -717,7 +756,7 @@ __global__ void __launch_bounds__(kCorrThreads) k_lin_list(const PairDev *__rest
     const float4 *o = pd.cur_omg + 3 * (size_t)ci;
     lin_terms(lp, Tl, pd.ref_pts[ri], pd.ref_nrm[ri], pd.cur_pts[ci], pd.cur_nrm[ci], o[0], o[1], o[2], acc);
   }
-  block_reduce_store(acc, pd.partials + (size_t)tile * kPartialWords);
+  block_reduce_store<kCorrThreads>(acc, pd.partials + (size_t)tile * kPartialWords);
 }
 
 // ------------------------------------------------------------ solve
@@ -885,7 +924,7 @@ static int corr_lin_grid(int total_tiles, int ctas_per_sm) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lin<kStructured>, kCorrThreads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lin<kStructured>, kFusedThreads,
                                                   corr_smem<kStructured>());
     per_sm_max = std::max(1, per_sm);
     sm_count = std::max(1, sms);
@@ -901,10 +940,10 @@ void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const 
   prof->begin(NICP_K_CORR_LIN, s);
   if (structured) {
     int grid = corr_lin_grid<true>(total_tiles, ctas_per_sm);
-    k_corr_lin<true><<<grid, kCorrThreads, corr_smem<true>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
+    k_corr_lin<true><<<grid, kFusedThreads, corr_smem<true>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
   } else {
     int grid = corr_lin_grid<false>(total_tiles, ctas_per_sm);
-    k_corr_lin<false><<<grid, kCorrThreads, corr_smem<false>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
+    k_corr_lin<false><<<grid, kFusedThreads, corr_smem<false>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
   }
   prof->end(NICP_K_CORR_LIN, s);
 }
@@ -970,7 +1009,7 @@ __global__ void __launch_bounds__(kCorrThreads) k_lin_noalloc(NoAllocLinArgs a, 
     const float4 *o = a.cur_omg + 3 * (size_t)ci;
     lin_terms(a.lp, a.T, a.ref_pts[ri], a.ref_nrm[ri], a.cur_pts[ci], a.cur_nrm[ci], o[0], o[1], o[2], acc);
   }
-  block_reduce_store(acc, partials + (size_t)tile * kPartialWords);
+  block_reduce_store<kCorrThreads>(acc, partials + (size_t)tile * kPartialWords);
 }
 
 // Sums the tile partials in the same fixed order as k_solve and writes
