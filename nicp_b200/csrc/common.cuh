@@ -246,49 +246,51 @@ __device__ __forceinline__ T t_dot(const T *a, const T *b) {
 __device__ __forceinline__ void d_cross(const double *a, const double *b, double *c) { t_cross(a, b, c); }
 __device__ __forceinline__ double d_dot(const double *a, const double *b) { return t_dot(a, b); }
 
-template <typename T>
-__device__ inline void t_null_vector(const T *B, T mu, T *v) {
-  T r0[3] = {B[0] - mu, B[1], B[2]};
-  T r1[3] = {B[1], B[3] - mu, B[4]};
-  T r2[3] = {B[2], B[4], B[5] - mu};
-  T c0[3], c1[3], c2[3];
-  t_cross(r0, r1, c0);
-  t_cross(r0, r2, c1);
-  t_cross(r1, r2, c2);
-  T d0 = t_dot(c0, c0), d1 = t_dot(c1, c1), d2 = t_dot(c2, c2);
+// A unit vector spanning the null space of B - mu I (B symmetric,
+// {b00 b01 b02 b11 b12 b22}): the largest cross product of two rows.
+__device__ inline void d_null_vector(const double *B, double mu, double *v) {
+  double r0[3] = {B[0] - mu, B[1], B[2]};
+  double r1[3] = {B[1], B[3] - mu, B[4]};
+  double r2[3] = {B[2], B[4], B[5] - mu};
+  double c0[3], c1[3], c2[3];
+  d_cross(r0, r1, c0);
+  d_cross(r0, r2, c1);
+  d_cross(r1, r2, c2);
+  double d0 = d_dot(c0, c0), d1 = d_dot(c1, c1), d2 = d_dot(c2, c2);
   // select by value (a pointer into the candidates would put them in local memory)
-  T b0 = c0[0], b1 = c0[1], b2 = c0[2], db = d0;
+  double b0 = c0[0], b1 = c0[1], b2 = c0[2], db = d0;
   if (d1 > db) { b0 = c1[0]; b1 = c1[1]; b2 = c1[2]; db = d1; }
   if (d2 > db) { b0 = c2[0]; b1 = c2[1]; b2 = c2[2]; db = d2; }
-  if (!(db > T(0))) { v[0] = 1; v[1] = 0; v[2] = 0; return; }
-  T inv = T(1) / sqrt(db);
+  if (!(db > 0.0)) { v[0] = 1; v[1] = 0; v[2] = 0; return; }
+  const double inv = rsqrt(db);
   v[0] = b0 * inv; v[1] = b1 * inv; v[2] = b2 * inv;
 }
 
-template <typename T>
-__device__ inline void t_plane_vector(const T *B, const T *e, T mu, T *v) {
-  T u[3];
+// The eigenvector of eigenvalue mu within the plane orthogonal to the unit
+// eigenvector e.
+__device__ inline void d_plane_vector(const double *B, const double *e, double mu, double *v) {
+  double u[3];
   if (fabs(e[0]) > fabs(e[1])) {
-    T il = T(1) / sqrt(e[0] * e[0] + e[2] * e[2]);
+    const double il = rsqrt(e[0] * e[0] + e[2] * e[2]);
     u[0] = -e[2] * il; u[1] = 0; u[2] = e[0] * il;
   } else {
-    T il = T(1) / sqrt(e[1] * e[1] + e[2] * e[2]);
+    const double il = rsqrt(e[1] * e[1] + e[2] * e[2]);
     u[0] = 0; u[1] = e[2] * il; u[2] = -e[1] * il;
   }
-  T w[3];
-  t_cross(e, u, w);
-  T Bu[3] = {B[0] * u[0] + B[1] * u[1] + B[2] * u[2], B[1] * u[0] + B[3] * u[1] + B[4] * u[2],
-             B[2] * u[0] + B[4] * u[1] + B[5] * u[2]};
-  T Bw[3] = {B[0] * w[0] + B[1] * w[1] + B[2] * w[2], B[1] * w[0] + B[3] * w[1] + B[4] * w[2],
-             B[2] * w[0] + B[4] * w[1] + B[5] * w[2]};
-  T m00 = t_dot(u, Bu) - mu, m01 = t_dot(u, Bw), m11 = t_dot(w, Bw) - mu;
-  T n0 = m00 * m00 + m01 * m01, n1 = m01 * m01 + m11 * m11;
-  T a, b;
+  double w[3];
+  d_cross(e, u, w);
+  double Bu[3] = {B[0] * u[0] + B[1] * u[1] + B[2] * u[2], B[1] * u[0] + B[3] * u[1] + B[4] * u[2],
+                  B[2] * u[0] + B[4] * u[1] + B[5] * u[2]};
+  double Bw[3] = {B[0] * w[0] + B[1] * w[1] + B[2] * w[2], B[1] * w[0] + B[3] * w[1] + B[4] * w[2],
+                  B[2] * w[0] + B[4] * w[1] + B[5] * w[2]};
+  double m00 = d_dot(u, Bu) - mu, m01 = d_dot(u, Bw), m11 = d_dot(w, Bw) - mu;
+  double n0 = m00 * m00 + m01 * m01, n1 = m01 * m01 + m11 * m11;
+  double a, b;
   if (n0 >= n1) {
-    if (n0 > T(0)) { T il = T(1) / sqrt(n0); a = -m01 * il; b = m00 * il; }
+    if (n0 > 0.0) { const double il = rsqrt(n0); a = -m01 * il; b = m00 * il; }
     else { a = 1; b = 0; }
   } else {
-    T il = T(1) / sqrt(n1); a = -m11 * il; b = m01 * il;
+    const double il = rsqrt(n1); a = -m11 * il; b = m01 * il;
   }
   v[0] = a * u[0] + b * w[0];
   v[1] = a * u[1] + b * w[1];
@@ -296,56 +298,60 @@ __device__ inline void t_plane_vector(const T *B, const T *e, T mu, T *v) {
 }
 
 // A = {a00 a01 a02 a11 a12 a22}; lam ascending; U row-major, column k <-> lam[k].
-template <typename T>
-__device__ inline void t_eig3(const T *A, T *lam, T *U) {
-  T amax = fabs(A[0]);
+// With B = A / max|a|, m = tr(B) / 3 and p = sqrt(|B - m I|_F^2 / 6), the
+// eigenvalues are m + 2 p cos(phi + 2 pi k / 3), phi = acos(det((B - m I) / p) / 2) / 3;
+// the largest (k = 0) and the smallest (k = 1) come from one sincos:
+// cos(phi + 2 pi / 3) = -cos(phi) / 2 - sin(phi) sqrt(3) / 2.
+__device__ inline void d_eig3(const double *A, double *lam, double *U) {
+  double amax = fabs(A[0]);
   for (int i = 1; i < 6; i++) amax = fmax(amax, fabs(A[i]));
-  if (!(amax > T(0))) {
+  if (!(amax > 0.0)) {
     lam[0] = lam[1] = lam[2] = 0;
-    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? T(1) : T(0);
+    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? 1.0 : 0.0;
     return;
   }
-  T is = T(1) / amax;
-  T B[6];
+  const double is = 1.0 / amax;
+  double B[6];
   for (int i = 0; i < 6; i++) B[i] = A[i] * is;
-  T m = (B[0] + B[3] + B[5]) / T(3);
-  T b00 = B[0] - m, b11 = B[3] - m, b22 = B[5] - m;
-  T off = B[1] * B[1] + B[2] * B[2] + B[4] * B[4];
-  T p2 = b00 * b00 + b11 * b11 + b22 * b22 + T(2) * off;
-  if (!(p2 > T(0))) {
+  const double third = 1.0 / 3.0;
+  const double m = (B[0] + B[3] + B[5]) * third;
+  const double b00 = B[0] - m, b11 = B[3] - m, b22 = B[5] - m;
+  const double off = B[1] * B[1] + B[2] * B[2] + B[4] * B[4];
+  const double p2 = b00 * b00 + b11 * b11 + b22 * b22 + 2.0 * off;
+  if (!(p2 > 0.0)) {
     lam[0] = lam[1] = lam[2] = m * amax;
-    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? T(1) : T(0);
+    for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? 1.0 : 0.0;
     return;
   }
-  T p = sqrt(p2 / T(6));
-  T ip = T(1) / p;
-  T c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip, c01 = B[1] * ip, c02 = B[2] * ip, c12 = B[4] * ip;
-  T det = c00 * (c11 * c22 - c12 * c12) - c01 * (c01 * c22 - c12 * c02) + c02 * (c01 * c12 - c11 * c02);
-  T q = det / T(2);
-  q = fmin(T(1), fmax(T(-1), q));
-  T phi = acos(q) / T(3);
-  const T tpi3 = T(2.0943951023931954923);
-  T l2 = m + T(2) * p * cos(phi);
-  T l0 = m + T(2) * p * cos(phi + tpi3);
-  T l1 = T(3) * m - l0 - l2;
-  T t;
+  const double p26 = p2 * (1.0 / 6.0);
+  const double ip = rsqrt(p26), p = p26 * ip;
+  const double c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip, c01 = B[1] * ip, c02 = B[2] * ip, c12 = B[4] * ip;
+  const double det = c00 * (c11 * c22 - c12 * c12) - c01 * (c01 * c22 - c12 * c02) + c02 * (c01 * c12 - c11 * c02);
+  const double q = fmin(1.0, fmax(-1.0, 0.5 * det));
+  const double phi = acos(q) * third;
+  double sphi, cphi;
+  sincos(phi, &sphi, &cphi);
+  const double half_sqrt3 = 0.86602540378443864676;
+  double l2 = m + 2.0 * p * cphi;
+  double l0 = m - p * cphi - 2.0 * half_sqrt3 * p * sphi;
+  double l1 = 3.0 * m - l0 - l2;
+  double t;
   if (l1 < l0) { t = l1; l1 = l0; l0 = t; }
   if (l2 < l1) { t = l2; l2 = l1; l1 = t; }
   if (l1 < l0) { t = l1; l1 = l0; l0 = t; }
-  T v0[3], v1[3], v2[3];
+  double v0[3], v1[3], v2[3];
   if (l1 - l0 >= l2 - l1) {
-    t_null_vector(B, l0, v0);
-    t_plane_vector(B, v0, l1, v1);
-    t_cross(v0, v1, v2);
+    d_null_vector(B, l0, v0);
+    d_plane_vector(B, v0, l1, v1);
+    d_cross(v0, v1, v2);
   } else {
-    t_null_vector(B, l2, v2);
-    t_plane_vector(B, v2, l1, v1);
-    t_cross(v1, v2, v0);
+    d_null_vector(B, l2, v2);
+    d_plane_vector(B, v2, l1, v1);
+    d_cross(v1, v2, v0);
   }
   lam[0] = l0 * amax; lam[1] = l1 * amax; lam[2] = l2 * amax;
   for (int r = 0; r < 3; r++) { U[r * 3 + 0] = v0[r]; U[r * 3 + 1] = v1[r]; U[r * 3 + 2] = v2[r]; }
 }
-__device__ inline void d_eig3(const double *A, double *lam, double *U) { t_eig3<double>(A, lam, U); }
 
 // Solve A x = b for a symmetric 6x6 A given by its lower triangle.
 __device__ inline void d_ldlt_solve6(const double *A, const double *b, double *x) {

@@ -216,11 +216,13 @@ __global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restr
 // Storage policies for the integral image.
 struct MomF64 {
   typedef double T;
+  __device__ static double val(double v) { return v; }
   __device__ static double load(const void *base, size_t i) { return static_cast<const double *>(base)[i]; }
   __device__ static void store(void *base, size_t i, double v) { static_cast<double *>(base)[i] = v; }
 };
 struct MomF32 {
   typedef float T;
+  __device__ static double val(float v) { return (double)v; }
   __device__ static double load(const void *base, size_t i) { return (double)static_cast<const float *>(base)[i]; }
   __device__ static void store(void *base, size_t i, double v) { static_cast<float *>(base)[i] = (float)v; }
 };
@@ -228,6 +230,7 @@ struct MomF32 {
 // bits); values travel as double inside the kernels and are split on store.
 struct MomTwoFloat {
   typedef float2 T;
+  __device__ static double val(float2 v) { return (double)v.x + (double)v.y; }
   __device__ static double load(const void *base, size_t i) {
     float2 v = static_cast<const float2 *>(base)[i];
     return (double)v.x + (double)v.y;
@@ -575,13 +578,17 @@ __global__ void __launch_bounds__(kStatsThreads, 3) k_stats(const FrameDev *__re
     size_t iA = (size_t)yM * cols + xM, iB = (size_t)ym * cols + xm;
     size_t iC = (size_t)yM * cols + xm, iD = (size_t)ym * cols + xM;
     double S[10];
+    // one pointer per corner, advanced plane by plane
+    const typename M::T *pA = static_cast<const typename M::T *>(f.moments) + iA;
+    const typename M::T *pB = pA + ((ptrdiff_t)iB - (ptrdiff_t)iA), *pC = pA + ((ptrdiff_t)iC - (ptrdiff_t)iA),
+                        *pD = pA + ((ptrdiff_t)iD - (ptrdiff_t)iA);
 #pragma unroll
     for (int m = 0; m < 10; m++) {
-      size_t o = (size_t)m * P;
-      double s = M::load(f.moments, o + iA) + M::load(f.moments, o + iB);
-      s = s - M::load(f.moments, o + iC);
-      s = s - M::load(f.moments, o + iD);
+      double s = M::val(pA[0]) + M::val(pB[0]);
+      s = s - M::val(pC[0]);
+      s = s - M::val(pD[0]);
       S[m] = s;
+      pA += P; pB += P; pC += P; pD += P;
     }
     int n = (int)S[0];
     if (n >= f.min_points) {
