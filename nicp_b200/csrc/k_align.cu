@@ -95,22 +95,29 @@ __device__ __forceinline__ int zbuf_index(unsigned long long z, bool drop_no_nor
 }
 
 // z-buffer -> int index image (and optional depth image, FLT_MAX where empty);
-// the z-buffer is left all ones for its next use.
+// the z-buffer is left all ones for its next use.  Thread t handles pixels
+// t, t + 256, ... of its tile: every warp access is one contiguous run.
 __global__ void k_resolve(const PairDev *__restrict__ pairs, int npairs, int to_ref, float *depth_out,
                           int drop_no_normal) {
   int pi = find_pair(pairs, npairs, blockIdx.x, false);
   const PairDev &pd = pairs[pi];
-  int P = pd.rows * pd.cols;
-  int pix0 = (blockIdx.x - pd.tile_base) * kCorrTilePixels + threadIdx.x * 4;
+  const int P = pd.rows * pd.cols;
+  const int pix0 = (blockIdx.x - pd.tile_base) * kCorrTilePixels + threadIdx.x;
   int32_t *dst = to_ref ? pd.ref_index : pd.cur_index;
+  unsigned long long z[kCorrTilePixels / kCorrThreads];
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    int p = pix0 + k;
-    if (p >= P) break;
-    unsigned long long z = pd.zbuf[p];
-    pd.zbuf[p] = ~0ull;
-    dst[p] = zbuf_index(z, drop_no_normal != 0);
-    if (depth_out) depth_out[p] = (z == ~0ull) ? 3.402823466e+38f : key_float((uint32_t)(z >> 32));
+  for (int k = 0; k < kCorrTilePixels / kCorrThreads; k++) {
+    const int p = pix0 + k * kCorrThreads;
+    z[k] = p < P ? pd.zbuf[p] : ~0ull;
+  }
+#pragma unroll
+  for (int k = 0; k < kCorrTilePixels / kCorrThreads; k++) {
+    const int p = pix0 + k * kCorrThreads;
+    if (p < P) {
+      pd.zbuf[p] = ~0ull;
+      dst[p] = zbuf_index(z[k], drop_no_normal != 0);
+      if (depth_out) depth_out[p] = (z[k] == ~0ull) ? 3.402823466e+38f : key_float((uint32_t)(z[k] >> 32));
+    }
   }
 }
 

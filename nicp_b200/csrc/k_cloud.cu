@@ -153,63 +153,73 @@ __device__ __forceinline__ void write_gaussian(const FrameDev &f, float4 *g, flo
   g[2] = make_float4(C[5], C[6], C[7], C[8]);
 }
 
+// Thread t handles pixels t, t + 256, ... of its tile (kUnprojTilePixels /
+// 256 rounds), so that depth loads, index stores and -- after the
+// compaction -- point stores of a warp are consecutive.  The numbering is
+// row-major: within the tile, pixel order is (round, warp, lane) order.
+constexpr int kUnprojRounds = kUnprojTilePixels / 256;
+
 __global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restrict__ frames, int nframes) {
   __shared__ int red[32];
-  __shared__ int wsum[8];
+  __shared__ int rcnt[kUnprojRounds * 8];  // valid pixels per (round, warp), then their exclusive prefix
+  __shared__ int wtot[4];
   int fi = find_frame<0>(frames, nframes, blockIdx.x);
   const FrameDev &f = frames[fi];
-  int tile = blockIdx.x - f.tile_base;
-  int P = f.rows * f.cols;
-  int ntiles = (P + kUnprojTilePixels - 1) / kUnprojTilePixels;
+  const int tile = blockIdx.x - f.tile_base;
+  const int P = f.rows * f.cols;
+  const int ntiles = (P + kUnprojTilePixels - 1) / kUnprojTilePixels;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   // points numbered before this tile
   int before = 0;
-  for (int t = threadIdx.x; t < tile; t += blockDim.x) before += f.tile_counts[t];
+  for (int q = t; q < tile; q += blockDim.x) before += f.tile_counts[q];
   before = block_sum_int(before, red);
-  int pix0 = tile * kUnprojTilePixels + threadIdx.x * 16;
-  float d[16];
-  load16(f, pix0, P, d);
+  const int base = tile * kUnprojTilePixels + t;
+  float d[kUnprojRounds];
   unsigned mask = 0;
 #pragma unroll
-  for (int k = 0; k < 16; k++) mask |= (depth_valid(d[k], f.min_d, f.max_d) ? 1u : 0u) << k;
-  int cnt = __popc(mask);
-  // exclusive block scan of cnt
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int inc = cnt;
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += y;
+  for (int k = 0; k < kUnprojRounds; k++) {
+    const int p = base + k * 256;
+    d[k] = p < P ? depth_of(f, p) : 0.0f;
+    const bool valid = p < P && depth_valid(d[k], f.min_d, f.max_d);
+    mask |= (valid ? 1u : 0u) << k;
+    const unsigned bal = __ballot_sync(0xffffffffu, valid);
+    if (lane == 0) rcnt[k * 8 + wid] = __popc(bal);
   }
-  if (lane == 31) wsum[wid] = inc;
   __syncthreads();
-  int woff = 0, btot = 0;
-  for (int i = 0; i < 8; i++) {
-    if (i < wid) woff += wsum[i];
-    btot += wsum[i];
+  // exclusive prefix of the kUnprojRounds x 8 counts in (round, warp) order
+  if (t < kUnprojRounds * 8) {
+    const int v = rcnt[t];
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) wtot[wid] = inc;
+    __syncwarp();
+    asm volatile("bar.sync 1, %0;" ::"r"(kUnprojRounds * 8));  // the first kUnprojRounds * 8 threads
+    int off = 0;
+    for (int w = 0; w < wid; w++) off += wtot[w];
+    rcnt[t] = off + inc - v;
+    if (t == kUnprojRounds * 8 - 1 && tile == ntiles - 1) *f.count = before + off + inc;
   }
-  int idx = before + woff + inc - cnt;
-  int out[16];
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-  for (int k = 0; k < 16; k++) {
-    out[k] = -1;
-    if (mask & (1u << k)) {
-      int p = pix0 + k;
-      int r = p / f.cols, c = p - r * f.cols;
-      float4 pt = unproject_pixel(f.iKRt, c, r, d[k]);
+  for (int k = 0; k < kUnprojRounds; k++) {
+    const int p = base + k * 256;
+    const bool valid = (mask >> k) & 1u;
+    const unsigned bal = __ballot_sync(0xffffffffu, valid);
+    int out = -1;
+    if (valid) {
+      const int idx = before + rcnt[k * 8 + wid] + __popc(bal & lt);
+      const int r = p / f.cols, c = p - r * f.cols;
+      const float4 pt = unproject_pixel(f.iKRt, c, r, d[k]);
       f.pts[idx] = pt;
       if (f.gauss) write_gaussian(f, f.gauss + 3 * (size_t)idx, pt, c, r, d[k]);
-      out[k] = idx++;
+      out = idx;
     }
+    if (p < P) f.index[p] = out;
   }
-  if (pix0 + 16 <= P && ((reinterpret_cast<uintptr_t>(f.index + pix0) & 15) == 0)) {
-    int4 *dst = reinterpret_cast<int4 *>(f.index + pix0);
-#pragma unroll
-    for (int k = 0; k < 4; k++) dst[k] = make_int4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
-  } else {
-#pragma unroll
-    for (int k = 0; k < 16; k++)
-      if (pix0 + k < P) f.index[pix0 + k] = out[k];
-  }
-  if (tile == ntiles - 1 && threadIdx.x == 0) *f.count = before + btot;
 }
 
 // ------------------------------------------------------------ moments
