@@ -357,7 +357,10 @@ constexpr int kFusedThreads = 128;
 constexpr int kFusedPX = 2;
 constexpr int kSubPix = kFusedThreads * kFusedPX;        // pixels per sub-tile
 constexpr int kSubsPerTile = kCorrTilePixels / kSubPix;  // 4
-constexpr int kCorrStages = 3;
+constexpr int kCorrStages = 3;  // general Omega: gather, gate + Omega gather, linearize
+#ifndef NICP_CORR_S_STAGES
+#define NICP_CORR_S_STAGES 2      // structured Omega: gather, gate + linearize
+#endif
 
 // Structure-of-arrays stage: thread t owns slots t + k kFusedThreads of
 // every array, so a warp's accesses to one field are consecutive 16-byte
@@ -371,12 +374,14 @@ struct GatherStageG : GatherStageS {  // general Omega: gathered for accepted pi
   int ci[kSubPix];
 };
 #ifndef NICP_CORR_S_CTAS
-#define NICP_CORR_S_CTAS 4
+#define NICP_CORR_S_CTAS 5
 #endif
 template <bool kStructured>
 using GatherStage = typename std::conditional<kStructured, GatherStageS, GatherStageG>::type;
 template <bool kStructured>
-constexpr int corr_smem() { return kCorrStages * (int)sizeof(GatherStage<kStructured>); }
+__host__ __device__ constexpr int corr_stages() { return kStructured ? NICP_CORR_S_STAGES : kCorrStages; }
+template <bool kStructured>
+constexpr int corr_smem() { return corr_stages<kStructured>() * (int)sizeof(GatherStage<kStructured>); }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -412,7 +417,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   const int nsub = ntiles * kSubsPerTile;
   const bool drop_no_normal = !cp.demoted;
   auto tile_of = [&](int j) { return (int)blockIdx.x + (j / kSubsPerTile) * (int)gridDim.x; };
-  auto stage_of = [&](int j) -> Stage & { return stages[j % kCorrStages]; };
+  auto stage_of = [&](int j) -> Stage & { return stages[j % corr_stages<kStructured>()]; };
 
   // Tile -> pair lookups, cached per pipeline stage (a stage's tile changes
   // once every kSubsPerTile sub-tiles).
@@ -573,25 +578,9 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   Acc acc;
 #pragma unroll
   for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
-  // prologue: sub-tile 0 through G1 and the gate, sub-tile 1 through G1
-  load_indices(0);
-  tile_constants(0);
-  issue_g1(0);
-  load_indices(1);
-  tile_constants(1);
-  issue_g1(1);
-  load_indices(2);
-  __syncthreads();
-  cp_async_wait<1>();
-  gate_g2(0);
-  for (int j = 0; j < nsub; j++) {
-    tile_constants(j + 2);
-    issue_g1(j + 2);          // uses the indices loaded in the previous iteration
-    load_indices(j + 3);
-    __syncthreads();          // tile constants visible; slots of j-1 fully consumed
-    cp_async_wait<2>();       // G1(j+1) complete (groups after it: G2(j), G1(j+2))
-    gate_g2(j + 1);
-    cp_async_wait<2>();       // G2(j) complete (groups after it: G1(j+2), G2(j+1))
+  // Linearizes sub-tile j (its gather -- and, for general Omega, its gate --
+  // complete); at a tile's last sub-tile the CTA stores the tile's partial.
+  auto consume = [&](int j) {
     const int e = (j / kSubsPerTile) & 1;
     const int sub = j % kSubsPerTile;
     if (sub == 0) {
@@ -633,6 +622,43 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
         const PairDev &pd = pairs[sPair[e]];
         block_reduce_store<kFusedThreads>(acc, pd.partials + (size_t)(tile_of(j) - pd.tile_base) * kPartialWords);
       }
+    }
+  };
+  if constexpr (corr_stages<kStructured>() == 2) {
+    // two stages: sub-tile j+1 is gathered while j is gated and linearized
+    load_indices(0);
+    tile_constants(0);
+    issue_g1(0);
+    load_indices(1);
+    for (int j = 0; j < nsub; j++) {
+      tile_constants(j + 1);
+      issue_g1(j + 1);        // uses the indices loaded in the previous iteration
+      load_indices(j + 2);
+      __syncthreads();        // tile constants visible
+      cp_async_wait<1>();     // G1(j) complete (G1(j+1) may be in flight)
+      consume(j);
+    }
+  } else {
+    // prologue: sub-tile 0 through G1 and the gate, sub-tile 1 through G1
+    load_indices(0);
+    tile_constants(0);
+    issue_g1(0);
+    load_indices(1);
+    tile_constants(1);
+    issue_g1(1);
+    load_indices(2);
+    __syncthreads();
+    cp_async_wait<1>();
+    gate_g2(0);
+    for (int j = 0; j < nsub; j++) {
+      tile_constants(j + 2);
+      issue_g1(j + 2);          // uses the indices loaded in the previous iteration
+      load_indices(j + 3);
+      __syncthreads();          // tile constants visible; slots of j-1 fully consumed
+      cp_async_wait<2>();       // G1(j+1) complete (groups after it: G2(j), G1(j+2))
+      gate_g2(j + 1);
+      cp_async_wait<2>();       // G2(j) complete (groups after it: G1(j+2), G2(j+1))
+      consume(j);
     }
   }
   cp_async_wait<0>();
