@@ -112,6 +112,47 @@ def test_normals_curvature_vs_f64(ctx, pair):
           (np.max(ang), np.max(angle_between(fn2[rb], rn[rb])), np.mean(~stable)))
 
 
+ODD_SIZES = [("640x480", 100, 297, 50, 383), ("640x480", 200, 207, 10, 55), ("640x480", 5, 6, 0, 640),
+             ("640x480", 3, 124, 1, 640), ("1280x720", 100, 581, 7, 1280), ("1280x720", 40, 73, 0, 1281 - 1)]
+
+
+@pytest.mark.parametrize("spec", ODD_SIZES, ids=["%dx%d" % (s[2] - s[1], s[4] - s[3]) for s in ODD_SIZES])
+def test_integral_image_odd_sizes(ctx, spec):
+    """The integral image over 16-row bands and 640-column chunks on frames
+    whose sizes are multiples of neither (one row, fewer rows than a band,
+    widths just under and over a chunk): index image and points bit-exact
+    against REF32; window point counts (moment plane 0) equal to the FP64
+    oracle's; normals and curvature within 1e-5 of the FP64 oracle, with the
+    exclusions of test_normals_curvature_vs_f64."""
+    name, r0, r1, c0, c1 = spec
+    d_full, _, _, cam_full = synth.render_pair(61, name)
+    d = np.ascontiguousarray(d_full[r0:r1, c0:c1])
+    cam = dict(cam_full, rows=d.shape[0], cols=d.shape[1])
+    proj, conv = converter(cam, ctx, keep_stats=True)
+    cloud, gidx = gpu_cloud(ctx, conv, d)
+    pc, oc = cams(cam)
+    r, ridx = O.build_cloud(O.REF32, d, oc)
+    assert np.array_equal(gidx, ridx)
+    g = cloud.download(stats=True)
+    assert np.array_equal(g["points"], r.get("points").astype(np.float32))
+    f, fidx = O.build_cloud(O.F64, d, oc)
+    stable, _, _ = decision_stable_pixels(d, cam, gidx, fidx)
+    gi, fi = match_by_pixel(gidx, fidx, stable)
+    n_gpu = cloud.stats()["n"][gi]
+    assert np.array_equal(n_gpu.astype(np.int64), f.get("stats_n")[fi].astype(np.int64))
+    fn, gn = f.get("normals")[fi, :3], g["normals"][gi, :3].astype(np.float64)
+    fhas, ghas = np.abs(fn).sum(1) > 0, np.abs(gn).sum(1) > 0
+    assert np.mean(fhas != ghas) < 2e-3 if len(fhas) else True
+    lam = f.get("eigenvalues")[fi]
+    ok = fhas & ghas & ((lam[:, 1] - lam[:, 0]) > 1e-3 * lam[:, 2])
+    if ok.any():
+        assert np.max(angle_between(fn[ok], gn[ok])) < 1e-5
+        dk = np.abs(f.get("curvature")[fi] - g["curvature"][gi].astype(np.float64))
+        assert np.max(dk[fhas & ghas]) < 1e-5
+    if d.shape[0] > 40:  # large enough for windows of the minimum radius
+        assert ok.sum() > 1000
+
+
 def test_project_bitexact(ctx, pair):
     """z-buffer projection of identical clouds from a perturbed pose:
     indices and depths equal the serial REF32 z-buffer (smallest depth,
