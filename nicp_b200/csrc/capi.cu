@@ -54,6 +54,9 @@ struct nicp_ctx {
   char *pin_up = nullptr;
   size_t pin_up_cap = 0;
   cudaEvent_t pin_up_ev = nullptr;
+  cudaStream_t copy_stream = nullptr;   // depth staging copies, overlapped with the build kernels
+  std::vector<cudaEvent_t> copy_ev;     // one per build chunk: its frames are staged
+  cudaEvent_t copy_start = nullptr;     // the compute stream's tail when staging begins
   char *pin_down = nullptr;
   size_t pin_down_cap = 0;
   size_t cloud_bytes = 0;
@@ -324,6 +327,10 @@ extern "C" int nicp_ctx_destroy(nicp_ctx *ctx) {
   if (ctx->pin_up) cudaFreeHost(ctx->pin_up);
   if (ctx->pin_down) cudaFreeHost(ctx->pin_down);
   cudaEventDestroy(ctx->pin_up_ev);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  for (cudaEvent_t e : ctx->copy_ev) cudaEventDestroy(e);
+  if (ctx->copy_start) cudaEventDestroy(ctx->copy_start);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return NICP_OK;
@@ -577,12 +584,22 @@ struct FrameIn {
 };
 }  // namespace
 
-// Builds clouds for frames [0, n) in chunks that bound the integral-image scratch.
+// Builds clouds for frames [0, n) in chunks that bound the integral-image
+// scratch.  The descriptors of every chunk are filled first and uploaded in
+// one copy.  Frames that need staging (host frames, or device frames that
+// are not packed and 16-byte aligned) are then copied into one staging
+// region on the copy stream, chunk by chunk, each chunk followed by an
+// event; a chunk's kernels wait for its own event only, so the copies of
+// later chunks overlap the kernels of earlier ones.  (An upload on the
+// compute stream issued after the staging copies would queue behind them in
+// the copy engine and hold up every chunk.)  With host frames, chunks hold at
+// most kStreamChunkFrames frames, so that the first kernels start early.
 static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_camera *cams, const nicp_cloud_params *prm,
                         nicp_cloud *const *clouds, bool unproject_only) {
   cudaStream_t s = ctx->stream;
   const size_t msz = moment_bytes(prm->moments_precision);
   const size_t kChunkMoments = (size_t)3 << 30;  // bytes of integral image per chunk
+  const int kStreamChunkFrames = 32;
   int rc;
   for (int i = 0; i < n; i++) {
     if (!fin[i].depth || fin[i].rows <= 0 || fin[i].cols <= 0 || !clouds[i] || !valid_camera(&cams[i]))
@@ -592,52 +609,81 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
                             prm->keep_gaussians != 0)))
       return rc;
   }
-  int i0 = 0;
-  while (i0 < n) {
+  if (n <= 0) return NICP_OK;
+  // staging needs and chunks
+  std::vector<char> staged(n, 0);
+  bool any_host = false, any_staged = false;
+  for (int i = 0; i < n; i++) {
+    const FrameIn &f = fin[i];
+    const size_t esz = f.u16 ? 2 : 4;
+    const bool packed = f.pitch == 0 || f.pitch == f.cols * esz;
+    const bool aligned = ((uintptr_t)f.depth & 15) == 0;
+    staged[i] = (!f.on_device || !packed || !aligned) ? 1 : 0;
+    any_host |= !f.on_device;
+    any_staged |= staged[i] != 0;
+  }
+  const int max_frames = any_host ? kStreamChunkFrames : n;
+  std::vector<std::pair<int, int>> chunks;
+  for (int i0 = 0; i0 < n;) {
     int i1 = i0;
     size_t mom = 0;
-    while (i1 < n) {
+    while (i1 < n && i1 - i0 < max_frames) {
       size_t m = (size_t)fin[i1].rows * fin[i1].cols * 10 * msz;
       if (i1 > i0 && mom + m > kChunkMoments) break;
       mom += m;
       i1++;
     }
-    int nf = i1 - i0;
-    Layout L;
-    std::vector<size_t> o_stage(nf, 0), o_tiles(nf), o_mom(nf), o_band(nf);
-    const int nb_rows = moment_band_rows();
-    size_t o_frames = L.take(sizeof(FrameDev) * nf);
+    chunks.push_back({i0, i1});
+    i0 = i1;
+  }
+  // one layout for the call: staging region, descriptors, then the scratch
+  // of the largest chunk (reused chunk after chunk, in stream order)
+  const int nb_rows = moment_band_rows();
+  Layout L;
+  std::vector<size_t> o_stage(n, 0);
+  for (int i = 0; i < n; i++)
+    if (staged[i]) o_stage[i] = L.take((size_t)fin[i].rows * fin[i].cols * (fin[i].u16 ? 2 : 4)) + 1;  // +1: "staged"
+  const size_t o_frames_all = L.take(sizeof(FrameDev) * n);
+  const size_t scratch0 = L.off;
+  size_t scratch_max = scratch0;
+  for (auto &c : chunks) {
+    Layout C;
+    C.off = scratch0;
+    for (int i = c.first; i < c.second; i++) {
+      const size_t P = (size_t)fin[i].rows * fin[i].cols;
+      C.take(4 * ((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
+      if (!unproject_only) {
+        C.take(P * 10 * msz);
+        C.take((size_t)((fin[i].rows + nb_rows - 1) / nb_rows) * 10 * fin[i].cols * msz);
+      }
+    }
+    scratch_max = std::max(scratch_max, C.off);
+  }
+  if ((rc = ensure_ws(ctx, scratch_max))) return rc;
+  char *pin;
+  if ((rc = pin_up(ctx, sizeof(FrameDev) * n, &pin))) return rc;
+  struct Grid { int tiles, bands, stiles, carryctas; };
+  std::vector<Grid> grids(chunks.size());
+  for (size_t ci = 0; ci < chunks.size(); ci++) {
+    const int i0 = chunks[ci].first, nf = chunks[ci].second - i0;
+    Layout C;
+    C.off = scratch0;
+    std::vector<size_t> o_tiles(nf), o_mom(nf), o_band(nf);
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
       size_t P = (size_t)f.rows * f.cols;
-      size_t esz = f.u16 ? 2 : 4;
-      bool packed = f.pitch == 0 || f.pitch == f.cols * esz;
-      bool aligned = ((uintptr_t)f.depth & 15) == 0;
-      if (!f.on_device || !packed || !aligned) o_stage[k] = L.take(P * esz) + 1;  // +1: "staged"
-      o_tiles[k] = L.take(4 * ((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
-      o_mom[k] = unproject_only ? 0 : L.take(P * 10 * msz);
-      o_band[k] = unproject_only ? 0 : L.take((size_t)((f.rows + nb_rows - 1) / nb_rows) * 10 * f.cols * msz);
+      o_tiles[k] = C.take(4 * ((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
+      o_mom[k] = unproject_only ? 0 : C.take(P * 10 * msz);
+      o_band[k] = unproject_only ? 0 : C.take((size_t)((f.rows + nb_rows - 1) / nb_rows) * 10 * f.cols * msz);
     }
-    if ((rc = ensure_ws(ctx, L.off))) return rc;
-    char *pin;
-    if ((rc = pin_up(ctx, sizeof(FrameDev) * nf, &pin))) return rc;
-    FrameDev *fd = reinterpret_cast<FrameDev *>(pin);
+    FrameDev *fd = reinterpret_cast<FrameDev *>(pin) + i0;
     int tiles = 0, bands = 0, stiles = 0, carryctas = 0;
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
       const nicp_camera &cam = cams[i0 + k];
       nicp_cloud *cl = clouds[i0 + k];
       size_t P = (size_t)f.rows * f.cols;
-      size_t esz = f.u16 ? 2 : 4;
-      const void *src = f.depth;
-      if (o_stage[k]) {
-        char *dst = ctx->ws + (o_stage[k] - 1);
-        size_t pitch = f.pitch ? f.pitch : f.cols * esz;
-        CK(ctx, cudaMemcpy2DAsync(dst, f.cols * esz, f.depth, pitch, f.cols * esz, f.rows,
-                                  f.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-        if (!f.on_device) ctx->h2d_bytes += (unsigned long long)f.cols * esz * f.rows;
-        src = dst;
-      }
+      const void *src = o_stage[i0 + k] ? (const void *)(ctx->ws + (o_stage[i0 + k] - 1)) : f.depth;
       FrameDev &d = fd[k];
       std::memset(&d, 0, sizeof(d));
       d.depth_u16 = f.u16 ? (const uint16_t *)src : nullptr;
@@ -698,17 +744,51 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.moments = unproject_only ? nullptr : (void *)(ctx->ws + o_mom[k]);
       d.band_tot = unproject_only ? nullptr : (void *)(ctx->ws + o_band[k]);
     }
-    FrameDev *dfr = (FrameDev *)(ctx->ws + o_frames);
-    CK(ctx, cudaMemcpyAsync(dfr, pin, sizeof(FrameDev) * nf, cudaMemcpyHostToDevice, s));
-    ctx->h2d_bytes += sizeof(FrameDev) * nf;
-    CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
-    launch_unproject(dfr, nf, tiles, s, &ctx->prof);
+    grids[ci] = {tiles, bands, stiles, carryctas};
+  }
+  FrameDev *dfr_all = (FrameDev *)(ctx->ws + o_frames_all);
+  CK(ctx, cudaMemcpyAsync(dfr_all, pin, sizeof(FrameDev) * n, cudaMemcpyHostToDevice, s));
+  ctx->h2d_bytes += sizeof(FrameDev) * n;
+  CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
+  if (any_staged) {
+    if (!ctx->copy_stream) CK(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    if (!ctx->copy_start) CK(ctx, cudaEventCreateWithFlags(&ctx->copy_start, cudaEventDisableTiming));
+    while (ctx->copy_ev.size() < chunks.size()) {
+      cudaEvent_t e;
+      CK(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ctx->copy_ev.push_back(e);
+    }
+    // the staging region may still be read by earlier work on the compute stream
+    CK(ctx, cudaEventRecord(ctx->copy_start, s));
+    CK(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_start, 0));
+    for (size_t c = 0; c < chunks.size(); c++) {
+      for (int i = chunks[c].first; i < chunks[c].second; i++) {
+        if (!staged[i]) continue;
+        const FrameIn &f = fin[i];
+        const size_t esz = f.u16 ? 2 : 4;
+        const size_t pitch = f.pitch ? f.pitch : f.cols * esz;
+        const cudaMemcpyKind kind = f.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if (pitch == f.cols * esz)  // packed rows: one linear copy
+          CK(ctx, cudaMemcpyAsync(ctx->ws + (o_stage[i] - 1), f.depth, pitch * f.rows, kind, ctx->copy_stream));
+        else
+          CK(ctx, cudaMemcpy2DAsync(ctx->ws + (o_stage[i] - 1), f.cols * esz, f.depth, pitch, f.cols * esz, f.rows,
+                                    kind, ctx->copy_stream));
+        if (!f.on_device) ctx->h2d_bytes += (unsigned long long)f.cols * esz * f.rows;
+      }
+      CK(ctx, cudaEventRecord(ctx->copy_ev[c], ctx->copy_stream));
+    }
+  }
+  for (size_t ci = 0; ci < chunks.size(); ci++) {
+    const int i0 = chunks[ci].first, nf = chunks[ci].second - i0;
+    const Grid &g = grids[ci];
+    if (any_staged) CK(ctx, cudaStreamWaitEvent(s, ctx->copy_ev[ci], 0));
+    const FrameDev *dfr = dfr_all + i0;
+    launch_unproject(dfr, nf, g.tiles, s, &ctx->prof);
     if (!unproject_only) {
-      launch_moments(prm->moments_precision, dfr, nf, bands, carryctas, s, &ctx->prof);
-      launch_stats(prm->moments_precision, dfr, nf, stiles, s, &ctx->prof);
+      launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, s, &ctx->prof);
+      launch_stats(prm->moments_precision, dfr, nf, g.stiles, s, &ctx->prof);
     }
     CK(ctx, cudaGetLastError());
-    i0 = i1;
   }
   return NICP_OK;
 }
