@@ -287,17 +287,29 @@ __device__ __forceinline__ void lin_terms_structured_xf(const LinParams &lp, con
   // Htr += ks Omega_p S, S = [[0, c, -b], [-c, 0, a], [b, -a, 0]]
   const float wp0 = -c * uy + b * uz, wp1 = c * ux - a * uz, wp2 = -b * ux + a * uy;
   const float wn0 = -cn2 * uy + bn * uz, wn1 = cn2 * ux - an * uz, wn2 = -bn * ux + an * uy;
-  acc.v[6] += t0 * wp0;          acc.v[7] += ka * c + t0 * wp1;  acc.v[8] += -ka * b + t0 * wp2;
-  acc.v[9] += -ka * c + t1 * wp0; acc.v[10] += t1 * wp1;         acc.v[11] += ka * a + t1 * wp2;
-  acc.v[12] += ka * b + t2 * wp0; acc.v[13] += -ka * a + t2 * wp1; acc.v[14] += t2 * wp2;
+  // (ka S = [[0, qc, -qb], [-qc, 0, qa], [qb, -qa, 0]] with q = ka (a, b, c))
+  const float qa = ka * a, qb = ka * b, qc = ka * c;
+  acc.v[6] = fmaf(t0, wp0, acc.v[6]);
+  acc.v[7] = fmaf(t0, wp1, acc.v[7] + qc);
+  acc.v[8] = fmaf(t0, wp2, acc.v[8] - qb);
+  acc.v[9] = fmaf(t1, wp0, acc.v[9] - qc);
+  acc.v[10] = fmaf(t1, wp1, acc.v[10]);
+  acc.v[11] = fmaf(t1, wp2, acc.v[11] + qa);
+  acc.v[12] = fmaf(t2, wp0, acc.v[12] + qb);
+  acc.v[13] = fmaf(t2, wp1, acc.v[13] - qa);
+  acc.v[14] = fmaf(t2, wp2, acc.v[14]);
   // Hrr += ks (S^T Omega_p S + Sn^T Omega_n Sn)
-  const float ss = a * a + b * b + c * c, sn = an * an + bn * bn + cn2 * cn2;
-  acc.v[15] += ka * (ss - a * a) + kb * wp0 * wp0 + kan * (sn - an * an) + kbn * wn0 * wn0;
-  acc.v[16] += -ka * (b * a) + kb * wp1 * wp0 - kan * (bn * an) + kbn * wn1 * wn0;
-  acc.v[17] += ka * (ss - b * b) + kb * wp1 * wp1 + kan * (sn - bn * bn) + kbn * wn1 * wn1;
-  acc.v[18] += -ka * (c * a) + kb * wp2 * wp0 - kan * (cn2 * an) + kbn * wn2 * wn0;
-  acc.v[19] += -ka * (c * b) + kb * wp2 * wp1 - kan * (cn2 * bn) + kbn * wn2 * wn1;
-  acc.v[20] += ka * (ss - c * c) + kb * wp2 * wp2 + kan * (sn - cn2 * cn2) + kbn * wn2 * wn2;
+  //      = ka (|v|^2 I - v v^T) + kan (|vn|^2 I - vn vn^T) + kb wp wp^T + kbn wn wn^T
+  const float qan = kan * an, qbn = kan * bn, qcn = kan * cn2;
+  const float D = fmaf(ka, a * a + b * b + c * c, kan * (an * an + bn * bn + cn2 * cn2));
+  const float pw0 = kb * wp0, pw1 = kb * wp1, pw2 = kb * wp2;
+  const float nw0 = kbn * wn0, nw1 = kbn * wn1, nw2 = kbn * wn2;
+  acc.v[15] = fmaf(nw0, wn0, fmaf(pw0, wp0, fmaf(-qan, an, fmaf(-qa, a, acc.v[15] + D))));
+  acc.v[16] = fmaf(nw1, wn0, fmaf(pw1, wp0, fmaf(-qbn, an, fmaf(-qb, a, acc.v[16]))));
+  acc.v[17] = fmaf(nw1, wn1, fmaf(pw1, wp1, fmaf(-qbn, bn, fmaf(-qb, b, acc.v[17] + D))));
+  acc.v[18] = fmaf(nw2, wn0, fmaf(pw2, wp0, fmaf(-qcn, an, fmaf(-qc, a, acc.v[18]))));
+  acc.v[19] = fmaf(nw2, wn1, fmaf(pw2, wp1, fmaf(-qcn, bn, fmaf(-qc, b, acc.v[19]))));
+  acc.v[20] = fmaf(nw2, wn2, fmaf(pw2, wp2, fmaf(-qcn, cn2, fmaf(-qc, c, acc.v[20] + D))));
   // bt += ks ep; br += ks (S^T ep + Sn^T en)
   acc.v[21] += ks * ep[0]; acc.v[22] += ks * ep[1]; acc.v[23] += ks * ep[2];
   float u0 = b * ep[2] - c * ep[1], u1 = c * ep[0] - a * ep[2], u2 = a * ep[1] - b * ep[0];
