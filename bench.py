@@ -74,7 +74,10 @@ def replica_value(world, units_per_rank, steps, ms_max):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples nvidia-smi clocks and throttle reasons during the timed region.
+    Started before the warm-up (so that nvidia-smi's own start-up is not
+    inside the timed region); mark() brackets the timed region and stop()
+    keeps the samples that arrived inside it (all of them if none did)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -85,6 +88,7 @@ class ClockSampler:
         self.proc = None
         self.lines = []
         self.reader = None
+        self.window = [None, None]
 
     def start(self):
         try:
@@ -98,7 +102,10 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def mark(self, which):
+        self.window[which] = time.monotonic()
 
     def stop(self):
         if self.proc is None:
@@ -111,7 +118,11 @@ class ClockSampler:
         self.reader.join(timeout=2)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0, t1 = self.window
+        lines = [ln for t, ln in self.lines if t0 is not None and t1 is not None and t0 <= t <= t1 + 0.25]
+        if not lines:
+            lines = [ln for _, ln in self.lines]
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -619,7 +630,7 @@ def workload_config(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--frames", type=int, default=200)
@@ -688,16 +699,19 @@ def main():
     def max_over_ranks(x):
         return max_over_ranks_of(dist, x)
 
+    # the clock sampler starts before the warm-up: nvidia-smi's start-up is
+    # not inside the timed region
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         step_dev()
     torch.cuda.synchronize()
 
     # ---- value: device-resident inputs
-    clocks = ClockSampler(local)
-    clocks.start()
     l0 = ctx.kernel_launches()
     barrier()
     torch.cuda.synchronize()
+    clocks.mark(0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
@@ -705,6 +719,7 @@ def main():
             res = step_dev()
         e1.record(stream)
     torch.cuda.synchronize()
+    clocks.mark(1)
     barrier()
     launches = ctx.kernel_launches() - l0
     ms = e0.elapsed_time(e1)
