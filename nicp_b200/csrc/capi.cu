@@ -1859,7 +1859,9 @@ extern "C" int nicp_align(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud
                           const float guess16[16], const float ref_offset16[16], const float cur_offset16[16],
                           const nicp_corr_params *corr, const nicp_lin_params *lin, const nicp_align_params *prm,
                           nicp_align_result *out) {
-  AlignCall a{1, &ref, &cur, cam, guess16, ref_offset16, cur_offset16, corr, lin, prm, false};
+  // replayed from a cached CUDA graph like a batch: the pair descriptors are
+  // uploaded per call, so one graph serves every pair of the same shape
+  AlignCall a{1, &ref, &cur, cam, guess16, ref_offset16, cur_offset16, corr, lin, prm, true};
   return align_impl(ctx, a, out);
 }
 
