@@ -649,12 +649,14 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   for (auto &c : chunks) {
     Layout C;
     C.off = scratch0;
+    const bool rowpath = moments_row_path(c.second - c.first);
     for (int i = c.first; i < c.second; i++) {
       const size_t P = (size_t)fin[i].rows * fin[i].cols;
       C.take(4 * ((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
       if (!unproject_only) {
         C.take(P * 10 * msz);
         C.take((size_t)((fin[i].rows + nb_rows - 1) / nb_rows) * 10 * fin[i].cols * msz);
+        if (rowpath) C.take(P * 10 * moment_acc_bytes(prm->moments_precision));
       }
     }
     scratch_max = std::max(scratch_max, C.off);
@@ -662,22 +664,24 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   if ((rc = ensure_ws(ctx, scratch_max))) return rc;
   char *pin;
   if ((rc = pin_up(ctx, sizeof(FrameDev) * n, &pin))) return rc;
-  struct Grid { int tiles, bands, stiles, carryctas; };
+  struct Grid { int tiles, bands, stiles, carryctas, max_bands; };
   std::vector<Grid> grids(chunks.size());
   for (size_t ci = 0; ci < chunks.size(); ci++) {
     const int i0 = chunks[ci].first, nf = chunks[ci].second - i0;
     Layout C;
     C.off = scratch0;
-    std::vector<size_t> o_tiles(nf), o_mom(nf), o_band(nf);
+    std::vector<size_t> o_tiles(nf), o_mom(nf), o_band(nf), o_rowpre(nf, 0);
+    const bool rowpath = moments_row_path(nf);
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
       size_t P = (size_t)f.rows * f.cols;
       o_tiles[k] = C.take(4 * ((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
       o_mom[k] = unproject_only ? 0 : C.take(P * 10 * msz);
       o_band[k] = unproject_only ? 0 : C.take((size_t)((f.rows + nb_rows - 1) / nb_rows) * 10 * f.cols * msz);
+      if (!unproject_only && rowpath) o_rowpre[k] = C.take(P * 10 * moment_acc_bytes(prm->moments_precision));
     }
     FrameDev *fd = reinterpret_cast<FrameDev *>(pin) + i0;
-    int tiles = 0, bands = 0, stiles = 0, carryctas = 0;
+    int tiles = 0, bands = 0, stiles = 0, carryctas = 0, max_bands = 0;
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
       const nicp_camera &cam = cams[i0 + k];
@@ -696,6 +700,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.col_base = carryctas;
       tiles += (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels);
       bands += (f.rows + nb_rows - 1) / nb_rows;
+      max_bands = std::max(max_bands, (f.rows + nb_rows - 1) / nb_rows);
       stiles += (int)((P + kStatsThreads - 1) / kStatsThreads);
       carryctas += (10 * f.cols + 127) / 128;
       d.depth_scale = prm->depth_scale;
@@ -743,8 +748,9 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.tile_counts = (int *)(ctx->ws + o_tiles[k]);
       d.moments = unproject_only ? nullptr : (void *)(ctx->ws + o_mom[k]);
       d.band_tot = unproject_only ? nullptr : (void *)(ctx->ws + o_band[k]);
+      d.rowpre = o_rowpre[k] ? (void *)(ctx->ws + o_rowpre[k]) : nullptr;
     }
-    grids[ci] = {tiles, bands, stiles, carryctas};
+    grids[ci] = {tiles, bands, stiles, carryctas, max_bands};
   }
   FrameDev *dfr_all = (FrameDev *)(ctx->ws + o_frames_all);
   CK(ctx, cudaMemcpyAsync(dfr_all, pin, sizeof(FrameDev) * n, cudaMemcpyHostToDevice, s));
@@ -785,7 +791,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     const FrameDev *dfr = dfr_all + i0;
     launch_unproject(dfr, nf, g.tiles, s, &ctx->prof);
     if (!unproject_only) {
-      launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, s, &ctx->prof);
+      launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, g.max_bands, s, &ctx->prof);
       launch_stats(prm->moments_precision, dfr, nf, g.stiles, s, &ctx->prof);
     }
     CK(ctx, cudaGetLastError());

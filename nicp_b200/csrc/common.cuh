@@ -78,6 +78,7 @@ struct FrameDev {
   int *tile_counts;           // per unprojection tile
   void *moments;              // 10 planes of rows*cols values (double / float / float2)
   void *band_tot;             // per 16-row band: 10 x cols totals, then carries (double / float)
+  void *rowpre;               // few-frame builds: 10 planes of row prefixes (double / float), else null
 };
 
 // ---- per-pair device state of the Gauss-Newton loop

@@ -818,9 +818,74 @@ void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cu
   prof->end(NICP_K_UNPROJECT, s, 2);
 }
 
+// ---- few-frame path (no more than kRowPathFrames frames per launch).  The
+// sweep walks a band's 16 rows in sequence, which on a single frame leaves
+// the GPU nearly idle.  Here the row prefixes R of every row are computed in
+// parallel (one CTA per image row, row_chunk_scan) into `rowpre`, then one
+// thread per (band, plane, column) adds them down the band onto the band's
+// carry: the sweep's additions in the sweep's order, so the planes are
+// bitwise those of the sweep and results do not depend on how frames are
+// batched.
+constexpr int kRowPathFrames = 2;
+
 template <class M>
-static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas, cudaStream_t s,
-                         Profiler *prof) {
+__global__ void __launch_bounds__(kRowThreads) k_moments_rowpre(const FrameDev *__restrict__ frames, int nframes) {
+  typedef typename MomAcc<M>::T A;
+  __shared__ A wtot[kRowThreads / 32][10];
+  const int fi = find_frame<1>(frames, nframes, blockIdx.x);
+  const FrameDev &f = frames[fi];
+  const int r = ((int)blockIdx.x - f.band_base) * kBandRows + (int)blockIdx.y;
+  if (r >= f.rows) return;  // the whole CTA
+  const int cols = f.cols;
+  const size_t P = (size_t)f.rows * cols;
+  A *Rp = static_cast<A *>(f.rowpre) + (size_t)r * cols;
+  A carry[10];
+#pragma unroll
+  for (int m = 0; m < 10; m++) carry[m] = A(0);
+  for (int x0 = 0; x0 < cols; x0 += kChunkPix) {
+    unsigned w[kRowPix];
+    load_row_raw(f, r, x0 + threadIdx.x * kRowPix, w);
+    float d[kRowPix];
+#pragma unroll
+    for (int k = 0; k < kRowPix; k++) d[k] = depth_from_raw(f, w[k]);
+    row_chunk_scan<M>(f, r, x0, d, carry, wtot, [&](int, int c, const A *acc) {
+      if (c < cols) {
+#pragma unroll
+        for (int m = 0; m < 10; m++) Rp[m * P + c] = acc[m];
+      }
+    });
+  }
+}
+
+template <class M>
+__global__ void __launch_bounds__(128) k_moments_colsum(const FrameDev *__restrict__ frames, int nframes) {
+  typedef typename MomAcc<M>::T A;
+  const int fi = find_frame<3>(frames, nframes, blockIdx.x);
+  const FrameDev &f = frames[fi];
+  const int cols = f.cols;
+  const int q = ((int)blockIdx.x - f.col_base) * 128 + (int)threadIdx.x;  // plane * cols + column
+  const int b = blockIdx.y, r0 = b * kBandRows;
+  if (q >= 10 * cols || r0 >= f.rows) return;
+  const int r1 = min(f.rows, r0 + kBandRows);
+  const int m = q / cols, c = q - m * cols;
+  const size_t P = (size_t)f.rows * cols;
+  A s = static_cast<const A *>(f.band_tot)[(size_t)b * 10 * cols + q];
+  const A *Rp = static_cast<const A *>(f.rowpre) + m * P + c;
+  A v[kBandRows];
+#pragma unroll
+  for (int k = 0; k < kBandRows; k++) v[k] = r0 + k < r1 ? Rp[(size_t)(r0 + k) * cols] : A(0);
+#pragma unroll
+  for (int k = 0; k < kBandRows; k++) {
+    if (r0 + k < r1) {
+      s = s + v[k];
+      M::store(f.moments, m * P + (size_t)(r0 + k) * cols + c, (double)s);
+    }
+  }
+}
+
+template <class M>
+static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas, int max_bands,
+                         cudaStream_t s, Profiler *prof) {
   static bool configured = false;  // one attribute call per instantiation
   if (!configured) {
     cudaFuncSetAttribute(k_moments_band_totals<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes<M>());
@@ -832,18 +897,27 @@ static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands,
   k_moments_band_carry<M><<<total_carry_ctas, 128, 0, s>>>(d_frames, nframes);
   prof->end(NICP_K_MOMENTS_BANDS, s, 2);
   prof->begin(NICP_K_MOMENTS_SWEEP, s);
-  k_moments_band_sweep<M><<<total_bands, kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, nframes);
-  prof->end(NICP_K_MOMENTS_SWEEP, s);
+  if (nframes <= kRowPathFrames) {
+    k_moments_rowpre<M><<<dim3(total_bands, kBandRows), kRowThreads, 0, s>>>(d_frames, nframes);
+    k_moments_colsum<M><<<dim3(total_carry_ctas, max_bands), 128, 0, s>>>(d_frames, nframes);
+    prof->end(NICP_K_MOMENTS_SWEEP, s, 2);
+  } else {
+    k_moments_band_sweep<M><<<total_bands, kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, nframes);
+    prof->end(NICP_K_MOMENTS_SWEEP, s);
+  }
 }
 
 int moment_band_rows() { return kBandRows; }
+bool moments_row_path(int nframes) { return nframes <= kRowPathFrames; }
+size_t moment_acc_bytes(int precision) { return precision == NICP_MOMENTS_F32 ? 4 : 8; }
 
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
-                    cudaStream_t s, Profiler *prof) {
-  if (precision == NICP_MOMENTS_F32) launch_bands<MomF32>(d_frames, nframes, total_bands, total_carry_ctas, s, prof);
+                    int max_bands, cudaStream_t s, Profiler *prof) {
+  if (precision == NICP_MOMENTS_F32)
+    launch_bands<MomF32>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, s, prof);
   else if (precision == NICP_MOMENTS_TWOFLOAT)
-    launch_bands<MomTwoFloat>(d_frames, nframes, total_bands, total_carry_ctas, s, prof);
-  else launch_bands<MomF64>(d_frames, nframes, total_bands, total_carry_ctas, s, prof);
+    launch_bands<MomTwoFloat>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, s, prof);
+  else launch_bands<MomF64>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, s, prof);
 }
 
 void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof) {

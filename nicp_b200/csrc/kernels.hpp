@@ -66,8 +66,13 @@ void launch_depth_scale(const uint16_t *u16, const float *f32, size_t pitch_elem
 // Integral image over 16-row bands (moment_band_rows()): total_bands band
 // CTAs, total_carry_ctas = sum over frames of ceil(10 cols / 128).
 int moment_band_rows();
+// Few-frame launches (moments_row_path) compute every row prefix in parallel
+// into FrameDev::rowpre (10 planes of moment_acc_bytes per pixel) instead of
+// sweeping the bands; the planes are bitwise the same.
+bool moments_row_path(int nframes);
+size_t moment_acc_bytes(int precision);
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
-                    cudaStream_t s, Profiler *prof);
+                    int max_bands, cudaStream_t s, Profiler *prof);
 void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s,
                   Profiler *prof);
 void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,

@@ -351,6 +351,47 @@ def test_build_batch_equals_single(ctx):
             assert np.array_equal(s[k], d[k]), k
 
 
+@pytest.mark.parametrize("precision", [L.NICP_MOMENTS_F64, L.NICP_MOMENTS_TWOFLOAT, L.NICP_MOMENTS_F32],
+                         ids=["fp64", "twofloat", "fp32"])
+def test_integral_image_paths_agree(ctx, precision):
+    """Builds of a few frames compute every row prefix in parallel and add
+    them down each band; larger batches sweep the bands.  Both must give
+    bitwise the same planes, so that results do not depend on batching: a
+    9-frame batch (sweep) against the same frames built one at a time,
+    compared through everything derived from the planes, kept Stats
+    included.  Sizes cover odd widths, fewer rows than a band, one row and
+    frames wider than a 640-column chunk."""
+    d0, _, _, cam0 = synth.render_pair(51, "640x480")
+    d1, _, _, cam1 = synth.render_pair(52, "320x240")
+    d2, _, _, cam2 = synth.render_pair(53, "1280x720")
+    specs = [(d0, cam0), (d1, cam1), (d2[100:581, 7:1280], cam2), (d0[100:297, 50:383], cam0),
+             (d0[200:207, 10:55], cam0), (d0[3:124, 1:640], cam0), (d1[5:6, :], cam1), (d2[40:73, :], cam2),
+             (d0[::-1].copy(), cam0)]
+    frames, cam_list, singles = [], [], []
+    for d, cam in specs:
+        d = np.ascontiguousarray(d)
+        proj, conv = converter(cam, ctx, keep_stats=True, precision=precision)
+        c = proj.camera(d.shape[0], d.shape[1])
+        frames.append(d)
+        cam_list.append(c)
+        one = api.Cloud(ctx)
+        api.build_batch(ctx, [d], [c], conv.params(), [one])
+        singles.append(one)
+        prm = conv.params()
+    assert len(frames) > 4
+    outs = [api.Cloud(ctx) for _ in frames]
+    api.build_batch(ctx, frames, cam_list, prm, outs)
+    for i, (s1, o) in enumerate(zip(singles, outs)):
+        a, b = s1.download(stats=True), o.download(stats=True)
+        assert len(a["points"]) == len(b["points"]), i
+        for k in ("points", "normals", "curvature", "omega_p", "omega_n", "eigenvalues", "eigenvectors"):
+            assert np.array_equal(a[k], b[k]), (i, k)
+        sa, sb = s1.stats(), o.stats()
+        for k in ("mean", "n"):
+            assert np.array_equal(sa[k], sb[k]), (i, k)
+    assert np.count_nonzero(np.any(outs[0].download()["normals"] != 0, axis=1)) > 100000
+
+
 @pytest.mark.parametrize("offset", [False, True], ids=["identity", "sensor_offset"])
 def test_gaussians(ctx, pair, offset):
     """unProject's Gaussian3f per point (pinholepointprojector.cpp:93-134),
