@@ -593,13 +593,14 @@ struct FrameIn {
 // later chunks overlap the kernels of earlier ones.  (An upload on the
 // compute stream issued after the staging copies would queue behind them in
 // the copy engine and hold up every chunk.)  With host frames, chunks hold at
-// most kStreamChunkFrames frames, so that the first kernels start early.
+// most kStreamChunkFrames frames (the first kStreamFirstChunkFrames), so
+// that the first kernels start early.
 static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_camera *cams, const nicp_cloud_params *prm,
                         nicp_cloud *const *clouds, bool unproject_only) {
   cudaStream_t s = ctx->stream;
   const size_t msz = moment_bytes(prm->moments_precision);
   const size_t kChunkMoments = (size_t)3 << 30;  // bytes of integral image per chunk
-  const int kStreamChunkFrames = 32;
+  const int kStreamChunkFrames = 32, kStreamFirstChunkFrames = 8;
   int rc;
   for (int i = 0; i < n; i++) {
     if (!fin[i].depth || fin[i].rows <= 0 || fin[i].cols <= 0 || !clouds[i] || !valid_camera(&cams[i]))
@@ -622,9 +623,11 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     any_host |= !f.on_device;
     any_staged |= staged[i] != 0;
   }
-  const int max_frames = any_host ? kStreamChunkFrames : n;
   std::vector<std::pair<int, int>> chunks;
   for (int i0 = 0; i0 < n;) {
+    // with host frames the first chunk is short, so the kernels start after
+    // a few frames' copies
+    const int max_frames = !any_host ? n : (i0 == 0 ? kStreamFirstChunkFrames : kStreamChunkFrames);
     int i1 = i0;
     size_t mom = 0;
     while (i1 < n && i1 - i0 < max_frames) {
