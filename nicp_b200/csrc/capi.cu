@@ -777,27 +777,44 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
         const size_t esz = f.u16 ? 2 : 4;
         const size_t pitch = f.pitch ? f.pitch : f.cols * esz;
         const cudaMemcpyKind kind = f.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        cudaError_t e;
         if (pitch == f.cols * esz)  // packed rows: one linear copy
-          CK(ctx, cudaMemcpyAsync(ctx->ws + (o_stage[i] - 1), f.depth, pitch * f.rows, kind, ctx->copy_stream));
+          e = cudaMemcpyAsync(ctx->ws + (o_stage[i] - 1), f.depth, pitch * f.rows, kind, ctx->copy_stream);
         else
-          CK(ctx, cudaMemcpy2DAsync(ctx->ws + (o_stage[i] - 1), f.cols * esz, f.depth, pitch, f.cols * esz, f.rows,
-                                    kind, ctx->copy_stream));
+          e = cudaMemcpy2DAsync(ctx->ws + (o_stage[i] - 1), f.cols * esz, f.depth, pitch, f.cols * esz, f.rows, kind,
+                                ctx->copy_stream);
+        if (e != cudaSuccess) {
+          cudaStreamSynchronize(ctx->copy_stream);  // copies already queued may read the caller's frames
+          return fail(ctx, NICP_ECUDA, std::string("depth staging copy: ") + cudaGetErrorString(e));
+        }
         if (!f.on_device) ctx->h2d_bytes += (unsigned long long)f.cols * esz * f.rows;
       }
-      CK(ctx, cudaEventRecord(ctx->copy_ev[c], ctx->copy_stream));
+      cudaError_t e = cudaEventRecord(ctx->copy_ev[c], ctx->copy_stream);
+      if (e != cudaSuccess) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        return fail(ctx, NICP_ECUDA, std::string("staging event: ") + cudaGetErrorString(e));
+      }
     }
   }
+  // From here on an error return first waits for the staging copies: they
+  // may read the caller's host frames, which the caller may free on error.
+  auto fail_staged = [&](cudaError_t e, const char *what) {
+    if (any_staged) cudaStreamSynchronize(ctx->copy_stream);
+    return fail(ctx, NICP_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
   for (size_t ci = 0; ci < chunks.size(); ci++) {
     const int i0 = chunks[ci].first, nf = chunks[ci].second - i0;
     const Grid &g = grids[ci];
-    if (any_staged) CK(ctx, cudaStreamWaitEvent(s, ctx->copy_ev[ci], 0));
+    cudaError_t e;
+    if (any_staged && (e = cudaStreamWaitEvent(s, ctx->copy_ev[ci], 0)) != cudaSuccess)
+      return fail_staged(e, "cudaStreamWaitEvent");
     const FrameDev *dfr = dfr_all + i0;
     launch_unproject(dfr, nf, g.tiles, s, &ctx->prof);
     if (!unproject_only) {
       launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, g.max_bands, s, &ctx->prof);
       launch_stats(prm->moments_precision, dfr, nf, g.stiles, s, &ctx->prof);
     }
-    CK(ctx, cudaGetLastError());
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail_staged(e, "build launch");
   }
   return NICP_OK;
 }
