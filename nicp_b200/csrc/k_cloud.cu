@@ -883,6 +883,8 @@ __global__ void __launch_bounds__(128) k_moments_colsum(const FrameDev *__restri
   }
 }
 
+bool moments_row_path(int nframes) { return nframes <= kRowPathFrames; }
+
 template <class M>
 static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas, int max_bands,
                          cudaStream_t s, Profiler *prof) {
@@ -897,7 +899,7 @@ static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands,
   k_moments_band_carry<M><<<total_carry_ctas, 128, 0, s>>>(d_frames, nframes);
   prof->end(NICP_K_MOMENTS_BANDS, s, 2);
   prof->begin(NICP_K_MOMENTS_SWEEP, s);
-  if (nframes <= kRowPathFrames) {
+  if (moments_row_path(nframes) && max_bands <= 65535) {  // (grid y of the column sums)
     k_moments_rowpre<M><<<dim3(total_bands, kBandRows), kRowThreads, 0, s>>>(d_frames, nframes);
     k_moments_colsum<M><<<dim3(total_carry_ctas, max_bands), 128, 0, s>>>(d_frames, nframes);
     prof->end(NICP_K_MOMENTS_SWEEP, s, 2);
@@ -908,7 +910,6 @@ static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands,
 }
 
 int moment_band_rows() { return kBandRows; }
-bool moments_row_path(int nframes) { return nframes <= kRowPathFrames; }
 size_t moment_acc_bytes(int precision) { return precision == NICP_MOMENTS_F32 ? 4 : 8; }
 
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
