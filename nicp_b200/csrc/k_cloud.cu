@@ -174,12 +174,23 @@ __global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restr
   for (int q = t; q < tile; q += blockDim.x) before += f.tile_counts[q];
   before = block_sum_int(before, red);
   const int base = tile * kUnprojTilePixels + t;
+  // every round's depth is loaded before the first ballot (one branch on the
+  // depth type for all of them), so the loads are in flight together
   float d[kUnprojRounds];
+  if (f.depth_u16) {
+    unsigned short u[kUnprojRounds];
+#pragma unroll
+    for (int k = 0; k < kUnprojRounds; k++) u[k] = base + k * 256 < P ? f.depth_u16[base + k * 256] : 0;
+#pragma unroll
+    for (int k = 0; k < kUnprojRounds; k++) d[k] = u[k] ? fm(f.depth_scale, (float)(int)u[k]) : 0.0f;
+  } else {
+#pragma unroll
+    for (int k = 0; k < kUnprojRounds; k++) d[k] = base + k * 256 < P ? f.depth_f32[base + k * 256] : 0.0f;
+  }
   unsigned mask = 0;
 #pragma unroll
   for (int k = 0; k < kUnprojRounds; k++) {
     const int p = base + k * 256;
-    d[k] = p < P ? depth_of(f, p) : 0.0f;
     const bool valid = p < P && depth_valid(d[k], f.min_d, f.max_d);
     mask |= (valid ? 1u : 0u) << k;
     const unsigned bal = __ballot_sync(0xffffffffu, valid);
@@ -565,10 +576,11 @@ __global__ void __launch_bounds__(kStatsThreads, 3) k_stats(const FrameDev *__re
   int rows = f.rows, cols = f.cols;
   int P = rows * cols;
   if (pix >= P) return;
-  int idx = f.index[pix];
+  // index and depth loaded together (the depth is not needed when the index is negative)
+  const int idx = f.index[pix];
+  const float d = depth_of(f, pix);
   if (idx < 0) return;
   int r = pix / cols, c = pix - r * cols;
-  float d = depth_of(f, pix);
   float4 nout = make_float4(0.f, 0.f, 0.f, 0.f);
   float om[12];
 #pragma unroll
