@@ -39,6 +39,13 @@
  *   - Host buffers are caller-owned; device buffers (clouds, scratch) are
  *     owned by the library.  Calls on one context are ordered on its CUDA
  *     stream; functions that return data in host memory synchronize it.
+ *   - Cloud builds from host depth (nicp_cloud_from_depth_*, nicp_build_batch
+ *     with on_device 0) return before the frames are copied when nothing is
+ *     returned in host memory: keep pinned host frames valid until the
+ *     context's stream has passed the call (pageable frames are copied
+ *     before the call returns).  The copies run on a second, library-owned
+ *     stream that is ordered after earlier work on the context's stream and
+ *     before the build kernels that read them.
  *   - There is no CPU fallback: creating a context fails on a host without
  *     an sm_100 GPU.
  *   - A context is not thread-safe: use one per host thread.
