@@ -917,7 +917,7 @@ struct PairPlan {
   size_t o_extra = 0;
   bool keep_ref = false, list_mode = false;
   bool structured = false;  // every current cloud has structured Omegas (k_corr_lin<true>)
-  int total_tiles = 0, total_pt_tiles = 0;
+  int total_tiles = 0, max_pt_tiles = 0;  // max_pt_tiles: 1024-point tiles of the largest projected cloud
   size_t o_pairs = 0, o_states = 0, o_krt = 0, o_guess = 0, o_roff = 0, o_zbuf = 0, zbuf_bytes = 0;
   std::vector<size_t> o_cur, o_ref, o_part, o_list, o_ltc, o_np;
   std::vector<int> P, tiles;
@@ -952,7 +952,7 @@ static int plan_pairs(nicp_ctx *ctx, int n, const nicp_camera *cams, const nicp_
   pl.o_cur.resize(n); pl.o_ref.resize(n); pl.o_part.resize(n);
   pl.o_list.resize(n); pl.o_ltc.resize(n); pl.o_np.resize(n);
   pl.total_tiles = 0;
-  pl.total_pt_tiles = 0;
+  pl.max_pt_tiles = 0;
   for (int i = 0; i < n; i++) {
     size_t P = pl.P[i];
     pl.o_cur[i] = L.take(4 * P);
@@ -963,7 +963,7 @@ static int plan_pairs(nicp_ctx *ctx, int n, const nicp_camera *cams, const nicp_
     pl.o_np[i] = L.take(4);
     pl.total_tiles += pl.tiles[i];
     int cap = std::max(refs[i] ? refs[i]->capacity : 0, 1);
-    pl.total_pt_tiles += (cap + kPointsPerCta - 1) / kPointsPerCta;
+    pl.max_pt_tiles = std::max(pl.max_pt_tiles, (cap + kPointsPerCta - 1) / kPointsPerCta);
   }
   pl.o_extra = L.take(std::max<size_t>(extra_bytes, 1));
   return ensure_ws(ctx, L.off);
@@ -973,7 +973,7 @@ static int plan_pairs(nicp_ctx *ctx, int n, const nicp_camera *cams, const nicp_
 static void fill_pairs(nicp_ctx *ctx, const PairPlan &pl, const nicp_camera *cams, const nicp_cloud *const *refs,
                        const nicp_cloud *const *curs, PairDev *pd) {
   char *ws = ctx->ws;
-  int tb = 0, pb = 0;
+  int tb = 0;
   size_t zoff = pl.o_zbuf;
   for (int i = 0; i < pl.n; i++) {
     PairDev &d = pd[i];
@@ -991,10 +991,8 @@ static void fill_pairs(nicp_ctx *ctx, const PairPlan &pl, const nicp_camera *cam
     d.rows = cam_rows(cams[i]);
     d.cols = cam_cols(cams[i]);
     d.tile_base = tb;
-    d.pt_tile_base = pb;
     d.ref_capacity = std::max(r ? r->capacity : 0, 1);
     tb += pl.tiles[i];
-    pb += (d.ref_capacity + kPointsPerCta - 1) / kPointsPerCta;
     d.min_d = cams[i].min_distance;
     d.max_d = cams[i].max_distance;
     cam_K(cams[i], d.K);
@@ -1143,7 +1141,7 @@ extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_c
   CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
   CK(ctx, cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s));
   const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
-  launch_zbuffer(dpd, 1, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), kZbufDefaultPPT, s, &ctx->prof);
+  launch_zbuffer(dpd, 1, pl.max_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), kZbufDefaultPPT, s, &ctx->prof);
   launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ctx->ws + o_depth), 0, s, &ctx->prof);
   CK(ctx, cudaGetLastError());
   if (index_out) CK(ctx, cudaMemcpyAsync(index_out, ctx->ws + pl.o_cur[0], 4 * P, cudaMemcpyDeviceToHost, s));
@@ -1557,7 +1555,7 @@ extern "C" int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *c
   CK(ctx, cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s));
   const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
   // the serial z-buffer of PinholePointProjector::project, all points kept
-  launch_zbuffer(dpd, 1, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), kZbufDefaultPPT, s, &ctx->prof);
+  launch_zbuffer(dpd, 1, pl.max_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), kZbufDefaultPPT, s, &ctx->prof);
   launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ex + o_depth), 0, s, &ctx->prof);
   MergeArgs a{};
   a.n = n;
@@ -1638,12 +1636,12 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
                     &ctx->prof);
   // current cloud, seen from its sensor offset, projected once (alignerprojective.cpp:36-39)
   const nicp_ctx::Launch &L = ctx->launch;
-  launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), L.zb_ppt, s, &ctx->prof);
+  launch_zbuffer(dpd, pl.n, pl.max_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), L.zb_ppt, s, &ctx->prof);
   // outside list (parity) mode, current pixels whose point has no normal are
   // dropped from the index image: the gates would reject them anyway
   launch_resolve(dpd, pl.n, pl.total_tiles, 0, nullptr, (pl.list_mode || cp.demoted) ? 0 : 1, s, &ctx->prof);
   for (int i = 0; i < outer; i++) {
-    launch_zbuffer(dpd, pl.n, pl.total_pt_tiles, 1, nullptr, L.zb_ppt, s, &ctx->prof);
+    launch_zbuffer(dpd, pl.n, pl.max_pt_tiles, 1, nullptr, L.zb_ppt, s, &ctx->prof);
     if (pl.list_mode) {
       launch_resolve(dpd, pl.n, pl.total_tiles, 1, nullptr, 0, s, &ctx->prof);
       launch_corr_list(dpd, pl.n, pl.total_tiles, cp, 1, nullptr, s, &ctx->prof);
@@ -1679,7 +1677,7 @@ static std::string graph_key(nicp_ctx *ctx, const PairPlan &pl, const AlignCall 
   put(&pl.list_mode, 1);
   put(&pl.structured, 1);
   put(&pl.total_tiles, sizeof(int));
-  put(&pl.total_pt_tiles, sizeof(int));
+  put(&pl.max_pt_tiles, sizeof(int));
   put(&pl.zbuf_bytes, sizeof(size_t));
   put(a.corr, sizeof(*a.corr));
   put(a.lin, sizeof(*a.lin));

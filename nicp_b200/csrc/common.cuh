@@ -117,7 +117,6 @@ struct PairDev {
   float cur_omd[8];
   int rows, cols;       // projection image (scaled)
   int tile_base;        // first pixel tile of this pair in the grid
-  int pt_tile_base;     // first point tile (reference cloud) in the grid
   int ref_capacity;     // upper bound on reference points
   float min_d, max_d;
   float K[9];

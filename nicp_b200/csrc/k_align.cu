@@ -32,11 +32,12 @@
 
 namespace nicp {
 
-__device__ __forceinline__ int find_pair(const PairDev *pairs, int n, int key, bool points) {
+// The pair whose pixel tiles hold tile `key` (largest i with tile_base <= key).
+__device__ __forceinline__ int find_pair(const PairDev *pairs, int n, int key) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
-    int b = points ? pairs[mid].pt_tile_base : pairs[mid].tile_base;
+    int b = pairs[mid].tile_base;
     if (b <= key) lo = mid;
     else hi = mid - 1;
   }
@@ -49,16 +50,20 @@ __device__ __forceinline__ int find_pair(const PairDev *pairs, int n, int key, b
 // the pair state's KRt.
 // A CTA covers kPointsPerCta points with kPointsPerCta / PPT threads, PPT
 // independent points per thread (their loads and atomics overlap); the
-// result does not depend on PPT (atomicMin is order-free).
+// result does not depend on PPT (atomicMin is order-free).  Grid: (point
+// tile, pair) -- the pair comes from blockIdx.y, with no search, so a CTA's
+// first loads are its pose and its points.
 template <int PPT>
 __global__ void __launch_bounds__(kPointsPerCta / PPT)
-    k_zbuffer(const PairDev *__restrict__ pairs, int npairs, int mode, const float *__restrict__ explicit_KRt) {
+    k_zbuffer(const PairDev *__restrict__ pairs, int npairs, int mode, const float *__restrict__ explicit_KRt,
+              int pair0) {
   constexpr int kThreads = kPointsPerCta / PPT;
-  int pi = find_pair(pairs, npairs, blockIdx.x, true);
+  const int pi = pair0 + (int)blockIdx.y;
+  if (pi >= npairs) return;
   const PairDev &pd = pairs[pi];
   const PairState *st = pd.state;
   if (mode == 1 && st->done) return;
-  const int i0 = (blockIdx.x - pd.pt_tile_base) * kPointsPerCta + threadIdx.x;
+  const int i0 = blockIdx.x * kPointsPerCta + threadIdx.x;
   const float4 *pts = mode ? pd.ref_pts : pd.cur_pts;
   const int n = mode ? *pd.ref_count : *pd.cur_count;
   if (i0 >= n) return;
@@ -99,7 +104,7 @@ __device__ __forceinline__ int zbuf_index(unsigned long long z, bool drop_no_nor
 // t, t + 256, ... of its tile: every warp access is one contiguous run.
 __global__ void k_resolve(const PairDev *__restrict__ pairs, int npairs, int to_ref, float *depth_out,
                           int drop_no_normal) {
-  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  int pi = find_pair(pairs, npairs, blockIdx.x);
   const PairDev &pd = pairs[pi];
   const int P = pd.rows * pd.cols;
   const int pix0 = (blockIdx.x - pd.tile_base) * kCorrTilePixels + threadIdx.x;
@@ -438,7 +443,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   auto lookup = [&](int tile, int &ctile, int &cpi, bool &cskip) {
     if (tile != ctile) {
       ctile = tile;
-      cpi = find_pair(pairs, npairs, tile, false);
+      cpi = find_pair(pairs, npairs, tile);
       cskip = !stats_pass && pairs[cpi].state->done;
     }
   };
@@ -695,7 +700,7 @@ __device__ __forceinline__ unsigned list_mask(const PairDev &pd, const CorrParam
 __global__ void __launch_bounds__(kCorrThreads) k_corr_count(const PairDev *__restrict__ pairs, int npairs, CorrParams cp,
                                                              int use_state_T, const float *__restrict__ explicit_T) {
   __shared__ int red[32];
-  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  int pi = find_pair(pairs, npairs, blockIdx.x);
   const PairDev &pd = pairs[pi];
   if (use_state_T && pd.state->done) return;
   int tile = blockIdx.x - pd.tile_base;
@@ -722,7 +727,7 @@ __global__ void __launch_bounds__(kCorrThreads) k_corr_write(const PairDev *__re
                                                              int use_state_T, const float *__restrict__ explicit_T) {
   __shared__ int red[32];
   __shared__ int wsum[kCorrThreads / 32];
-  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  int pi = find_pair(pairs, npairs, blockIdx.x);
   const PairDev &pd = pairs[pi];
   if (use_state_T && pd.state->done) return;
   int tile = blockIdx.x - pd.tile_base;
@@ -775,7 +780,7 @@ __global__ void __launch_bounds__(kCorrThreads) k_corr_write(const PairDev *__re
 __global__ void __launch_bounds__(kCorrThreads) k_lin_list(const PairDev *__restrict__ pairs, int npairs, LinParams lp,
                                                            int parity_threads, int use_state_T,
                                                            const float *__restrict__ explicit_T) {
-  int pi = find_pair(pairs, npairs, blockIdx.x, false);
+  int pi = find_pair(pairs, npairs, blockIdx.x);
   const PairDev &pd = pairs[pi];
   if (use_state_T == 1 && pd.state->done) return;
   int tile = blockIdx.x - pd.tile_base;
@@ -938,15 +943,19 @@ __global__ void __launch_bounds__(128) k_solve(const PairDev *__restrict__ pairs
 }
 
 // ------------------------------------------------------------ launchers
-void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int mode, const float *explicit_KRt,
+void launch_zbuffer(const PairDev *d_pairs, int npairs, int max_pt_tiles, int mode, const float *explicit_KRt,
                     int ppt, cudaStream_t s, Profiler *prof) {
-  if (total_pt_tiles <= 0) return;
+  if (max_pt_tiles <= 0 || npairs <= 0) return;
   prof->begin(NICP_K_ZBUFFER, s);
-  switch (ppt) {
-    case 1: k_zbuffer<1><<<total_pt_tiles, kPointsPerCta, 0, s>>>(d_pairs, npairs, mode, explicit_KRt); break;
-    case 2: k_zbuffer<2><<<total_pt_tiles, kPointsPerCta / 2, 0, s>>>(d_pairs, npairs, mode, explicit_KRt); break;
-    case 8: k_zbuffer<8><<<total_pt_tiles, kPointsPerCta / 8, 0, s>>>(d_pairs, npairs, mode, explicit_KRt); break;
-    default: k_zbuffer<4><<<total_pt_tiles, kPointsPerCta / 4, 0, s>>>(d_pairs, npairs, mode, explicit_KRt); break;
+  const int kMaxGridY = 65535;
+  for (int p0 = 0; p0 < npairs; p0 += kMaxGridY) {
+    const dim3 g(max_pt_tiles, std::min(kMaxGridY, npairs - p0));
+    switch (ppt) {
+      case 1: k_zbuffer<1><<<g, kPointsPerCta, 0, s>>>(d_pairs, npairs, mode, explicit_KRt, p0); break;
+      case 2: k_zbuffer<2><<<g, kPointsPerCta / 2, 0, s>>>(d_pairs, npairs, mode, explicit_KRt, p0); break;
+      case 8: k_zbuffer<8><<<g, kPointsPerCta / 8, 0, s>>>(d_pairs, npairs, mode, explicit_KRt, p0); break;
+      default: k_zbuffer<4><<<g, kPointsPerCta / 4, 0, s>>>(d_pairs, npairs, mode, explicit_KRt, p0); break;
+    }
   }
   prof->end(NICP_K_ZBUFFER, s);
 }

@@ -86,7 +86,9 @@ void launch_intervals(const float *d_depth, int P, const float *d_K9, float min_
 void solution_statistics(const double H36[36], const double T16[16], double *translational_ratio,
                          double *rotational_ratio);
 
-void launch_zbuffer(const PairDev *d_pairs, int npairs, int total_pt_tiles, int mode, const float *explicit_KRt,
+// Grid (max_pt_tiles, npairs): max_pt_tiles = the largest number of
+// 1024-point tiles of any pair's projected cloud.
+void launch_zbuffer(const PairDev *d_pairs, int npairs, int max_pt_tiles, int mode, const float *explicit_KRt,
                     int ppt, cudaStream_t s, Profiler *prof);
 void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out,
                     int drop_no_normal, cudaStream_t s, Profiler *prof);
