@@ -627,7 +627,9 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   for (int i0 = 0; i0 < n;) {
     // with host frames the first chunk is short, so the kernels start after
     // a few frames' copies
-    const int max_frames = !any_host ? n : (i0 == 0 ? kStreamFirstChunkFrames : kStreamChunkFrames);
+    // (frames per launch are the grids' y dimension: at most 65535)
+    const int max_frames =
+        std::min(65535, !any_host ? n : (i0 == 0 ? kStreamFirstChunkFrames : kStreamChunkFrames));
     int i1 = i0;
     size_t mom = 0;
     while (i1 < n && i1 - i0 < max_frames) {
@@ -667,7 +669,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   if ((rc = ensure_ws(ctx, scratch_max))) return rc;
   char *pin;
   if ((rc = pin_up(ctx, sizeof(FrameDev) * n, &pin))) return rc;
-  struct Grid { int tiles, bands, stiles, carryctas, max_bands; };
+  struct Grid { int tiles, bands, stiles, carryctas, max_bands, max_tiles, max_stiles; };
   std::vector<Grid> grids(chunks.size());
   for (size_t ci = 0; ci < chunks.size(); ci++) {
     const int i0 = chunks[ci].first, nf = chunks[ci].second - i0;
@@ -684,7 +686,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       if (!unproject_only && rowpath) o_rowpre[k] = C.take(P * 10 * moment_acc_bytes(prm->moments_precision));
     }
     FrameDev *fd = reinterpret_cast<FrameDev *>(pin) + i0;
-    int tiles = 0, bands = 0, stiles = 0, carryctas = 0, max_bands = 0;
+    int tiles = 0, bands = 0, stiles = 0, carryctas = 0, max_bands = 0, max_tiles = 0, max_stiles = 0;
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
       const nicp_camera &cam = cams[i0 + k];
@@ -704,6 +706,8 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       tiles += (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels);
       bands += (f.rows + nb_rows - 1) / nb_rows;
       max_bands = std::max(max_bands, (f.rows + nb_rows - 1) / nb_rows);
+      max_tiles = std::max(max_tiles, (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
+      max_stiles = std::max(max_stiles, (int)((P + kStatsThreads - 1) / kStatsThreads));
       stiles += (int)((P + kStatsThreads - 1) / kStatsThreads);
       carryctas += (10 * f.cols + 127) / 128;
       d.depth_scale = prm->depth_scale;
@@ -753,7 +757,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.band_tot = unproject_only ? nullptr : (void *)(ctx->ws + o_band[k]);
       d.rowpre = o_rowpre[k] ? (void *)(ctx->ws + o_rowpre[k]) : nullptr;
     }
-    grids[ci] = {tiles, bands, stiles, carryctas, max_bands};
+    grids[ci] = {tiles, bands, stiles, carryctas, max_bands, max_tiles, max_stiles};
   }
   FrameDev *dfr_all = (FrameDev *)(ctx->ws + o_frames_all);
   CK(ctx, cudaMemcpyAsync(dfr_all, pin, sizeof(FrameDev) * n, cudaMemcpyHostToDevice, s));
@@ -812,7 +816,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     launch_unproject(dfr, nf, g.tiles, s, &ctx->prof);
     if (!unproject_only) {
       launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, g.max_bands, s, &ctx->prof);
-      launch_stats(prm->moments_precision, dfr, nf, g.stiles, s, &ctx->prof);
+      launch_stats(prm->moments_precision, dfr, nf, g.max_stiles, s, &ctx->prof);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail_staged(e, "build launch");
   }

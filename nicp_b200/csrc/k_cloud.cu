@@ -503,6 +503,8 @@ __global__ void __launch_bounds__(128) k_moments_band_carry(const FrameDev *__re
   }
 }
 
+// Grid (band, frame): the frame is blockIdx.y, no search over the frame
+// descriptors; CTAs past a smaller frame's last band return at once.
 template <class M>
 __global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const FrameDev *__restrict__ frames, int nframes) {
   typedef typename MomAcc<M>::T A;
@@ -510,11 +512,11 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const Fra
   A *state = reinterpret_cast<A *>(band_raw);  // [10][kChunkPix]: I(r, c) of the current row
   __shared__ A wtot[kRowThreads / 32][10];
   __shared__ A rowc[kBandRows][10];  // row carries across chunks (frames wider than a chunk)
-  const int fi = find_frame<1>(frames, nframes, blockIdx.x);
-  const FrameDev &f = frames[fi];
-  const int b = blockIdx.x - f.band_base;
+  const FrameDev &f = frames[blockIdx.y];
+  const int b = blockIdx.x;
   const int cols = f.cols;
   const size_t P = (size_t)f.rows * cols;
+  if (b * kBandRows >= f.rows) return;
   const int r0 = b * kBandRows, r1 = min(f.rows, r0 + kBandRows);
   const A *carry_b = static_cast<const A *>(f.band_tot) + (size_t)b * 10 * cols;
   const int t = threadIdx.x;
@@ -568,11 +570,12 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const Fra
 }
 
 // ------------------------------------------------------------ stats + omegas
+// Grid (pixel tile, frame): the frame is blockIdx.y, no search over the frame
+// descriptors.
 template <class M>
 __global__ void __launch_bounds__(kStatsThreads, 3) k_stats(const FrameDev *__restrict__ frames, int nframes) {
-  int fi = find_frame<2>(frames, nframes, blockIdx.x);
-  const FrameDev &f = frames[fi];
-  int pix = (blockIdx.x - f.stat_tile_base) * kStatsThreads + threadIdx.x;
+  const FrameDev &f = frames[blockIdx.y];
+  int pix = blockIdx.x * kStatsThreads + threadIdx.x;
   int rows = f.rows, cols = f.cols;
   int P = rows * cols;
   if (pix >= P) return;
@@ -916,7 +919,7 @@ static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands,
     k_moments_colsum<M><<<dim3(total_carry_ctas, max_bands), 128, 0, s>>>(d_frames, nframes);
     prof->end(NICP_K_MOMENTS_SWEEP, s, 2);
   } else {
-    k_moments_band_sweep<M><<<total_bands, kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, nframes);
+    k_moments_band_sweep<M><<<dim3(max_bands, nframes), kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, nframes);
     prof->end(NICP_K_MOMENTS_SWEEP, s);
   }
 }
@@ -933,11 +936,12 @@ void launch_moments(int precision, const FrameDev *d_frames, int nframes, int to
   else launch_bands<MomF64>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, s, prof);
 }
 
-void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof) {
+void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_tiles, cudaStream_t s, Profiler *prof) {
   prof->begin(NICP_K_STATS, s);
-  if (precision == NICP_MOMENTS_F32) k_stats<MomF32><<<total_tiles, kStatsThreads, 0, s>>>(d_frames, nframes);
-  else if (precision == NICP_MOMENTS_TWOFLOAT) k_stats<MomTwoFloat><<<total_tiles, kStatsThreads, 0, s>>>(d_frames, nframes);
-  else k_stats<MomF64><<<total_tiles, kStatsThreads, 0, s>>>(d_frames, nframes);
+  const dim3 g(max_tiles, nframes);
+  if (precision == NICP_MOMENTS_F32) k_stats<MomF32><<<g, kStatsThreads, 0, s>>>(d_frames, nframes);
+  else if (precision == NICP_MOMENTS_TWOFLOAT) k_stats<MomTwoFloat><<<g, kStatsThreads, 0, s>>>(d_frames, nframes);
+  else k_stats<MomF64><<<g, kStatsThreads, 0, s>>>(d_frames, nframes);
   prof->end(NICP_K_STATS, s);
 }
 

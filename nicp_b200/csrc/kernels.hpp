@@ -73,7 +73,9 @@ bool moments_row_path(int nframes);
 size_t moment_acc_bytes(int precision);
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
                     int max_bands, cudaStream_t s, Profiler *prof);
-void launch_stats(int precision, const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s,
+// (tile, frame) grid: max_tiles = the largest number of kStatsThreads-pixel
+// tiles of any frame of the launch; nframes <= 65535.
+void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_tiles, cudaStream_t s,
                   Profiler *prof);
 void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,
                             int capacity, const float *d_m12, cudaStream_t s, Profiler *prof);
