@@ -922,6 +922,7 @@ struct PairPlan {
   bool keep_ref = false, list_mode = false;
   bool structured = false;  // every current cloud has structured Omegas (k_corr_lin<true>)
   int total_tiles = 0, max_pt_tiles = 0;  // max_pt_tiles: 1024-point tiles of the largest projected cloud
+  int max_tiles = 0;                      // pixel tiles of the largest pair image
   size_t o_pairs = 0, o_states = 0, o_krt = 0, o_guess = 0, o_roff = 0, o_zbuf = 0, zbuf_bytes = 0;
   std::vector<size_t> o_cur, o_ref, o_part, o_list, o_ltc, o_np;
   std::vector<int> P, tiles;
@@ -949,6 +950,7 @@ static int plan_pairs(nicp_ctx *ctx, int n, const nicp_camera *cams, const nicp_
     if (P > (1u << 30)) return fail(ctx, NICP_EINVAL, "projection image too large");
     pl.P[i] = (int)P;
     pl.tiles[i] = (int)((P + kCorrTilePixels - 1) / kCorrTilePixels);
+    pl.max_tiles = std::max(pl.max_tiles, pl.tiles[i]);
     ztot += align_up(8 * P, 256);
   }
   pl.o_zbuf = L.take(ztot);
@@ -1146,7 +1148,7 @@ extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_c
   CK(ctx, cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s));
   const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
   launch_zbuffer(dpd, 1, pl.max_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), kZbufDefaultPPT, s, &ctx->prof);
-  launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ctx->ws + o_depth), 0, s, &ctx->prof);
+  launch_resolve(dpd, 1, pl.max_tiles, 0, (float *)(ctx->ws + o_depth), 0, s, &ctx->prof);
   CK(ctx, cudaGetLastError());
   if (index_out) CK(ctx, cudaMemcpyAsync(index_out, ctx->ws + pl.o_cur[0], 4 * P, cudaMemcpyDeviceToHost, s));
   if (depth_out) CK(ctx, cudaMemcpyAsync(depth_out, ctx->ws + o_depth, 4 * P, cudaMemcpyDeviceToHost, s));
@@ -1560,7 +1562,7 @@ extern "C" int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *c
   const PairDev *dpd = (const PairDev *)(ctx->ws + pl.o_pairs);
   // the serial z-buffer of PinholePointProjector::project, all points kept
   launch_zbuffer(dpd, 1, pl.max_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), kZbufDefaultPPT, s, &ctx->prof);
-  launch_resolve(dpd, 1, pl.total_tiles, 0, (float *)(ex + o_depth), 0, s, &ctx->prof);
+  launch_resolve(dpd, 1, pl.max_tiles, 0, (float *)(ex + o_depth), 0, s, &ctx->prof);
   MergeArgs a{};
   a.n = n;
   a.count = cloud->count;
@@ -1643,11 +1645,11 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
   launch_zbuffer(dpd, pl.n, pl.max_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), L.zb_ppt, s, &ctx->prof);
   // outside list (parity) mode, current pixels whose point has no normal are
   // dropped from the index image: the gates would reject them anyway
-  launch_resolve(dpd, pl.n, pl.total_tiles, 0, nullptr, (pl.list_mode || cp.demoted) ? 0 : 1, s, &ctx->prof);
+  launch_resolve(dpd, pl.n, pl.max_tiles, 0, nullptr, (pl.list_mode || cp.demoted) ? 0 : 1, s, &ctx->prof);
   for (int i = 0; i < outer; i++) {
     launch_zbuffer(dpd, pl.n, pl.max_pt_tiles, 1, nullptr, L.zb_ppt, s, &ctx->prof);
     if (pl.list_mode) {
-      launch_resolve(dpd, pl.n, pl.total_tiles, 1, nullptr, 0, s, &ctx->prof);
+      launch_resolve(dpd, pl.n, pl.max_tiles, 1, nullptr, 0, s, &ctx->prof);
       launch_corr_list(dpd, pl.n, pl.total_tiles, cp, 1, nullptr, s, &ctx->prof);
       for (int k = 0; k < inner; k++) {
         launch_lin_list(dpd, pl.n, pl.total_tiles, lp, std::max(1, a.corr->parity_threads), 1, nullptr, s, &ctx->prof);
@@ -1682,6 +1684,7 @@ static std::string graph_key(nicp_ctx *ctx, const PairPlan &pl, const AlignCall 
   put(&pl.structured, 1);
   put(&pl.total_tiles, sizeof(int));
   put(&pl.max_pt_tiles, sizeof(int));
+  put(&pl.max_tiles, sizeof(int));
   put(&pl.zbuf_bytes, sizeof(size_t));
   put(a.corr, sizeof(*a.corr));
   put(a.lin, sizeof(*a.lin));

@@ -102,12 +102,14 @@ __device__ __forceinline__ int zbuf_index(unsigned long long z, bool drop_no_nor
 // z-buffer -> int index image (and optional depth image, FLT_MAX where empty);
 // the z-buffer is left all ones for its next use.  Thread t handles pixels
 // t, t + 256, ... of its tile: every warp access is one contiguous run.
+// Grid (pixel tile, pair): the pair is pair0 + blockIdx.y, no search.
 __global__ void k_resolve(const PairDev *__restrict__ pairs, int npairs, int to_ref, float *depth_out,
-                          int drop_no_normal) {
-  int pi = find_pair(pairs, npairs, blockIdx.x);
+                          int drop_no_normal, int pair0) {
+  const int pi = pair0 + (int)blockIdx.y;
+  if (pi >= npairs) return;
   const PairDev &pd = pairs[pi];
   const int P = pd.rows * pd.cols;
-  const int pix0 = (blockIdx.x - pd.tile_base) * kCorrTilePixels + threadIdx.x;
+  const int pix0 = blockIdx.x * kCorrTilePixels + threadIdx.x;
   int32_t *dst = to_ref ? pd.ref_index : pd.cur_index;
   unsigned long long z[kCorrTilePixels / kCorrThreads];
 #pragma unroll
@@ -960,10 +962,14 @@ void launch_zbuffer(const PairDev *d_pairs, int npairs, int max_pt_tiles, int mo
   prof->end(NICP_K_ZBUFFER, s);
 }
 
-void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out,
+void launch_resolve(const PairDev *d_pairs, int npairs, int max_tiles, int to_ref, float *depth_out,
                     int drop_no_normal, cudaStream_t s, Profiler *prof) {
+  if (max_tiles <= 0 || npairs <= 0) return;
   prof->begin(NICP_K_RESOLVE, s);
-  k_resolve<<<total_tiles, kCorrThreads, 0, s>>>(d_pairs, npairs, to_ref, depth_out, drop_no_normal);
+  const int kMaxGridY = 65535;
+  for (int p0 = 0; p0 < npairs; p0 += kMaxGridY)
+    k_resolve<<<dim3(max_tiles, std::min(kMaxGridY, npairs - p0)), kCorrThreads, 0, s>>>(d_pairs, npairs, to_ref,
+                                                                                        depth_out, drop_no_normal, p0);
   prof->end(NICP_K_RESOLVE, s);
 }
 

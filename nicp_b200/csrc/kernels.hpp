@@ -92,7 +92,9 @@ void solution_statistics(const double H36[36], const double T16[16], double *tra
 // 1024-point tiles of any pair's projected cloud.
 void launch_zbuffer(const PairDev *d_pairs, int npairs, int max_pt_tiles, int mode, const float *explicit_KRt,
                     int ppt, cudaStream_t s, Profiler *prof);
-void launch_resolve(const PairDev *d_pairs, int npairs, int total_tiles, int to_ref, float *depth_out,
+// Grid (max_tiles, npairs): max_tiles = the largest number of 1024-pixel
+// tiles of any pair's image.
+void launch_resolve(const PairDev *d_pairs, int npairs, int max_tiles, int to_ref, float *depth_out,
                     int drop_no_normal, cudaStream_t s, Profiler *prof);
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
                      int flags, bool structured, int ctas_per_sm, cudaStream_t s, Profiler *prof);
