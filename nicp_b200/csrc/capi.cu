@@ -924,6 +924,7 @@ struct PairPlan {
   int total_tiles = 0, max_pt_tiles = 0;  // max_pt_tiles: 1024-point tiles of the largest projected cloud
   int max_tiles = 0;                      // pixel tiles of the largest pair image
   size_t o_pairs = 0, o_states = 0, o_krt = 0, o_guess = 0, o_roff = 0, o_zbuf = 0, zbuf_bytes = 0;
+  size_t o_tile_pair = 0;  // int per pixel tile: its pair
   std::vector<size_t> o_cur, o_ref, o_part, o_list, o_ltc, o_np;
   std::vector<int> P, tiles;
 };
@@ -971,6 +972,7 @@ static int plan_pairs(nicp_ctx *ctx, int n, const nicp_camera *cams, const nicp_
     int cap = std::max(refs[i] ? refs[i]->capacity : 0, 1);
     pl.max_pt_tiles = std::max(pl.max_pt_tiles, (cap + kPointsPerCta - 1) / kPointsPerCta);
   }
+  pl.o_tile_pair = L.take(4 * (size_t)std::max(pl.total_tiles, 1));
   pl.o_extra = L.take(std::max<size_t>(extra_bytes, 1));
   return ensure_ws(ctx, L.off);
 }
@@ -1385,8 +1387,8 @@ extern "C" int nicp_align_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cl
   const PairDev *dpd = (const PairDev *)(ws + pl.o_pd);
   LinParams lp = lin_params(*lin);
   const int xb = lin->cross_block_f32 ? kSolveCrossF32 : 0;
-  launch_init_pairs(dpd, 1, (const double *)(ws + pl.o_guess), (const double *)(ws + pl.o_guess + 128), s,
-                    &ctx->prof);
+  launch_init_pairs(dpd, 1, (const double *)(ws + pl.o_guess), (const double *)(ws + pl.o_guess + 128), nullptr, 0,
+                    s, &ctx->prof);
   NNQuery q = nn_query(ctx, pl, ref, cur, normal_scaling, *corr, nullptr, (const PairState *)(ws + pl.o_st));
   for (int i = 0; i < prm->outer_iterations; i++) {
     // correspondences with the state's T^-1 (alignernn.cpp:40-45)
@@ -1638,8 +1640,9 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
   bool stats = p.compute_statistics != 0;
   const int xb = a.lin->cross_block_f32 ? kSolveCrossF32 : 0;
   cudaMemsetAsync(ctx->ws + pl.o_zbuf, 0xff, pl.zbuf_bytes, s);
-  launch_init_pairs(dpd, pl.n, (const double *)(ctx->ws + pl.o_guess), (const double *)(ctx->ws + pl.o_roff), s,
-                    &ctx->prof);
+  int *tile_pair = (int *)(ctx->ws + pl.o_tile_pair);
+  launch_init_pairs(dpd, pl.n, (const double *)(ctx->ws + pl.o_guess), (const double *)(ctx->ws + pl.o_roff),
+                    tile_pair, pl.max_tiles, s, &ctx->prof);
   // current cloud, seen from its sensor offset, projected once (alignerprojective.cpp:36-39)
   const nicp_ctx::Launch &L = ctx->launch;
   launch_zbuffer(dpd, pl.n, pl.max_pt_tiles, 0, (const float *)(ctx->ws + pl.o_krt), L.zb_ppt, s, &ctx->prof);
@@ -1658,7 +1661,8 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
     } else {
       for (int k = 0; k < inner; k++) {
         int flags = (k == 0) ? (1 | 2 | (pl.keep_ref ? 4 : 0)) : 0;
-        launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, flags, pl.structured, L.corr_ctas, s, &ctx->prof);
+        launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, flags, pl.structured, L.corr_ctas, tile_pair, s,
+                        &ctx->prof);
         launch_solve(dpd, pl.n, p.lambda, ((k == inner - 1) ? 1 : 0) | xb, p.early_exit_eps, 0, s, &ctx->prof);
       }
     }
@@ -1669,7 +1673,7 @@ static void enqueue_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a) 
     if (pl.list_mode)
       launch_lin_list(dpd, pl.n, pl.total_tiles, lp, std::max(1, a.corr->parity_threads), 2, nullptr, s, &ctx->prof);
     else
-      launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, 8, pl.structured, L.corr_ctas, s, &ctx->prof);
+      launch_corr_lin(dpd, pl.n, pl.total_tiles, cp, lp, 8, pl.structured, L.corr_ctas, tile_pair, s, &ctx->prof);
     launch_solve(dpd, pl.n, 0.0f, 4 | xb, 0.0, 1, s, &ctx->prof);
   }
 }

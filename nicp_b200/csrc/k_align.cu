@@ -419,8 +419,8 @@ __device__ __forceinline__ void cp_async_wait() {
 // matrices (no Omega gathers, smaller stages).
 template <bool kStructured>
 __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS : 3)
-    k_corr_lin(const PairDev *__restrict__ pairs, int npairs, int total_tiles, CorrParams cp, LinParams lp,
-               int flags) {
+    k_corr_lin(const PairDev *__restrict__ pairs, int npairs, const int *__restrict__ tile_pair, int total_tiles,
+               CorrParams cp, LinParams lp, int flags) {
   extern __shared__ __align__(16) unsigned char corr_smem_raw[];
   using Stage = GatherStage<kStructured>;
   Stage *stages = reinterpret_cast<Stage *>(corr_smem_raw);
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   auto lookup = [&](int tile, int &ctile, int &cpi, bool &cskip) {
     if (tile != ctile) {
       ctile = tile;
-      cpi = find_pair(pairs, npairs, tile);
+      cpi = tile_pair[tile];  // filled once per alignment by k_tile_pairs
       cskip = !stats_pass && pairs[cpi].state->done;
     }
   };
@@ -995,15 +995,18 @@ static int corr_lin_grid(int total_tiles, int ctas_per_sm) {
 }
 
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
-                     int flags, bool structured, int ctas_per_sm, cudaStream_t s, Profiler *prof) {
+                     int flags, bool structured, int ctas_per_sm, const int *tile_pair, cudaStream_t s,
+                     Profiler *prof) {
   if (total_tiles <= 0) return;
   prof->begin(NICP_K_CORR_LIN, s);
   if (structured) {
     int grid = corr_lin_grid<true>(total_tiles, ctas_per_sm);
-    k_corr_lin<true><<<grid, kFusedThreads, corr_smem<true>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
+    k_corr_lin<true><<<grid, kFusedThreads, corr_smem<true>(), s>>>(d_pairs, npairs, tile_pair, total_tiles, cp,
+                                                                    lp, flags);
   } else {
     int grid = corr_lin_grid<false>(total_tiles, ctas_per_sm);
-    k_corr_lin<false><<<grid, kFusedThreads, corr_smem<false>(), s>>>(d_pairs, npairs, total_tiles, cp, lp, flags);
+    k_corr_lin<false><<<grid, kFusedThreads, corr_smem<false>(), s>>>(d_pairs, npairs, tile_pair, total_tiles,
+                                                                      cp, lp, flags);
   }
   prof->end(NICP_K_CORR_LIN, s);
 }
@@ -1023,11 +1026,28 @@ void launch_lin_list(const PairDev *d_pairs, int npairs, int total_tiles, const 
   prof->end(NICP_K_LIN_LIST, s);
 }
 
+// tile_pair[tile] = the pair whose pixel image holds the tile (grid: tiles
+// of a pair, pair), so that the persistent fused kernel finds a tile's pair
+// with one load instead of a search.
+__global__ void k_tile_pairs(const PairDev *__restrict__ pairs, int npairs, int *__restrict__ tile_pair, int pair0) {
+  const int pi = pair0 + (int)blockIdx.y;
+  if (pi >= npairs) return;
+  const PairDev &pd = pairs[pi];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ntiles = (pd.rows * pd.cols + kCorrTilePixels - 1) / kCorrTilePixels;
+  if (t < ntiles) tile_pair[pd.tile_base + t] = pi;
+}
+
 void launch_init_pairs(const PairDev *d_pairs, int npairs, const double *d_guesses, const double *d_ref_offsets,
-                       cudaStream_t s, Profiler *prof) {
+                       int *tile_pair, int max_tiles, cudaStream_t s, Profiler *prof) {
   prof->begin(NICP_K_SOLVE, s);
   k_init_pairs<<<(npairs + 63) / 64, 64, 0, s>>>(d_pairs, npairs, d_guesses, d_ref_offsets);
-  prof->end(NICP_K_SOLVE, s);
+  const int kMaxGridY = 65535;
+  if (tile_pair && max_tiles > 0)
+    for (int p0 = 0; p0 < npairs; p0 += kMaxGridY)
+      k_tile_pairs<<<dim3((max_tiles + 255) / 256, std::min(kMaxGridY, npairs - p0)), 256, 0, s>>>(d_pairs, npairs,
+                                                                                                  tile_pair, p0);
+  prof->end(NICP_K_SOLVE, s, tile_pair && max_tiles > 0 ? 2 : 1);
 }
 
 void launch_solve(const PairDev *d_pairs, int npairs, float lambda, int mode, double early_eps, int ignore_done,

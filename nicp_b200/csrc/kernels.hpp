@@ -97,13 +97,16 @@ void launch_zbuffer(const PairDev *d_pairs, int npairs, int max_pt_tiles, int mo
 void launch_resolve(const PairDev *d_pairs, int npairs, int max_tiles, int to_ref, float *depth_out,
                     int drop_no_normal, cudaStream_t s, Profiler *prof);
 void launch_corr_lin(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, const LinParams &lp,
-                     int flags, bool structured, int ctas_per_sm, cudaStream_t s, Profiler *prof);
+                     int flags, bool structured, int ctas_per_sm, const int *tile_pair, cudaStream_t s,
+                     Profiler *prof);
 void launch_corr_list(const PairDev *d_pairs, int npairs, int total_tiles, const CorrParams &cp, int use_state_T,
                       const float *explicit_T, cudaStream_t s, Profiler *prof);
 void launch_lin_list(const PairDev *d_pairs, int npairs, int total_tiles, const LinParams &lp, int parity_threads,
                      int use_state_T, const float *explicit_T, cudaStream_t s, Profiler *prof);
+// Initialises the pair states and, when tile_pair is given, the tile -> pair
+// table of the fused kernel (total pixel tiles entries).
 void launch_init_pairs(const PairDev *d_pairs, int npairs, const double *d_guesses, const double *d_ref_offsets,
-                       cudaStream_t s, Profiler *prof);
+                       int *tile_pair, int max_tiles, cudaStream_t s, Profiler *prof);
 void launch_solve(const PairDev *d_pairs, int npairs, float lambda, int mode, double early_eps, int ignore_done,
                   cudaStream_t s, Profiler *prof);
 
