@@ -648,7 +648,24 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   std::vector<size_t> o_stage(n, 0);
   for (int i = 0; i < n; i++)
     if (staged[i]) o_stage[i] = L.take((size_t)fin[i].rows * fin[i].cols * (fin[i].u16 ? 2 : 4)) + 1;  // +1: "staged"
-  const size_t o_frames_all = L.take(sizeof(FrameDev) * n);
+  // descriptors of every frame, then per chunk the frame of each CTA of the
+  // 1-D build grids: unprojection tiles, 16-row bands, band-carry CTAs
+  std::vector<size_t> tab_off(chunks.size() + 1, 0);
+  std::vector<int> tab_tiles(chunks.size(), 0), tab_bands(chunks.size(), 0);
+  for (size_t ci = 0; ci < chunks.size(); ci++) {
+    size_t t = 0, b = 0, k = 0;
+    for (int i = chunks[ci].first; i < chunks[ci].second; i++) {
+      const size_t P = (size_t)fin[i].rows * fin[i].cols;
+      t += (P + kUnprojTilePixels - 1) / kUnprojTilePixels;
+      b += (fin[i].rows + nb_rows - 1) / nb_rows;
+      k += (10 * (size_t)fin[i].cols + 127) / 128;
+    }
+    tab_tiles[ci] = (int)t;
+    tab_bands[ci] = (int)b;
+    tab_off[ci + 1] = tab_off[ci] + t + b + k;
+  }
+  const size_t frames_bytes = sizeof(FrameDev) * n + 4 * tab_off[chunks.size()];
+  const size_t o_frames_all = L.take(frames_bytes);
   const size_t scratch0 = L.off;
   size_t scratch_max = scratch0;
   for (auto &c : chunks) {
@@ -668,7 +685,8 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   }
   if ((rc = ensure_ws(ctx, scratch_max))) return rc;
   char *pin;
-  if ((rc = pin_up(ctx, sizeof(FrameDev) * n, &pin))) return rc;
+  if ((rc = pin_up(ctx, frames_bytes, &pin))) return rc;
+  int *tab_all = reinterpret_cast<int *>(pin + sizeof(FrameDev) * n);
   struct Grid { int tiles, bands, stiles, carryctas, max_bands, max_tiles, max_stiles; };
   std::vector<Grid> grids(chunks.size());
   for (size_t ci = 0; ci < chunks.size(); ci++) {
@@ -686,6 +704,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       if (!unproject_only && rowpath) o_rowpre[k] = C.take(P * 10 * moment_acc_bytes(prm->moments_precision));
     }
     FrameDev *fd = reinterpret_cast<FrameDev *>(pin) + i0;
+    int *tab_t = tab_all + tab_off[ci], *tab_b = tab_t + tab_tiles[ci], *tab_k = tab_b + tab_bands[ci];
     int tiles = 0, bands = 0, stiles = 0, carryctas = 0, max_bands = 0, max_tiles = 0, max_stiles = 0;
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
@@ -701,8 +720,10 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.cols = f.cols;
       d.tile_base = tiles;
       d.band_base = bands;
-      d.stat_tile_base = stiles;
       d.col_base = carryctas;
+      for (int q = 0, m = (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels); q < m; q++) tab_t[tiles + q] = k;
+      for (int q = 0, m = (f.rows + nb_rows - 1) / nb_rows; q < m; q++) tab_b[bands + q] = k;
+      for (int q = 0, m = (10 * f.cols + 127) / 128; q < m; q++) tab_k[carryctas + q] = k;
       tiles += (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels);
       bands += (f.rows + nb_rows - 1) / nb_rows;
       max_bands = std::max(max_bands, (f.rows + nb_rows - 1) / nb_rows);
@@ -760,8 +781,9 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     grids[ci] = {tiles, bands, stiles, carryctas, max_bands, max_tiles, max_stiles};
   }
   FrameDev *dfr_all = (FrameDev *)(ctx->ws + o_frames_all);
-  CK(ctx, cudaMemcpyAsync(dfr_all, pin, sizeof(FrameDev) * n, cudaMemcpyHostToDevice, s));
-  ctx->h2d_bytes += sizeof(FrameDev) * n;
+  CK(ctx, cudaMemcpyAsync(dfr_all, pin, frames_bytes, cudaMemcpyHostToDevice, s));
+  ctx->h2d_bytes += frames_bytes;
+  const int *dtab_all = reinterpret_cast<const int *>(ctx->ws + o_frames_all + sizeof(FrameDev) * n);
   CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
   if (any_staged) {
     if (!ctx->copy_stream) CK(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
@@ -813,9 +835,10 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     if (any_staged && (e = cudaStreamWaitEvent(s, ctx->copy_ev[ci], 0)) != cudaSuccess)
       return fail_staged(e, "cudaStreamWaitEvent");
     const FrameDev *dfr = dfr_all + i0;
-    launch_unproject(dfr, nf, g.tiles, s, &ctx->prof);
+    const int *ft = dtab_all + tab_off[ci], *fb = ft + tab_tiles[ci], *fk = fb + tab_bands[ci];
+    launch_unproject(dfr, nf, g.tiles, ft, s, &ctx->prof);
     if (!unproject_only) {
-      launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, g.max_bands, s, &ctx->prof);
+      launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, g.max_bands, fb, fk, s, &ctx->prof);
       launch_stats(prm->moments_precision, dfr, nf, g.max_stiles, s, &ctx->prof);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail_staged(e, "build launch");

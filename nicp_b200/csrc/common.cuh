@@ -54,7 +54,6 @@ struct FrameDev {
   int rows, cols;
   int tile_base;              // first unprojection tile of this frame in the grid
   int band_base;              // first 16-row moment band of this frame in the band grid
-  int stat_tile_base;         // first stats tile of this frame
   int col_base;               // first band-carry CTA of this frame (128 of its 10 x cols columns each)
   float depth_scale;
   float min_d, max_d;

@@ -27,27 +27,6 @@
 
 namespace nicp {
 
-// ------------------------------------------------------------ frame lookup
-template <int Field>
-__device__ __forceinline__ int frame_base(const FrameDev &f) {
-  if (Field == 0) return f.tile_base;
-  if (Field == 1) return f.band_base;
-  if (Field == 2) return f.stat_tile_base;
-  return f.col_base;
-}
-
-// Largest i with base(frames[i]) <= key.
-template <int Field>
-__device__ __forceinline__ int find_frame(const FrameDev *frames, int n, int key) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (frame_base<Field>(frames[mid]) <= key) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
 // ------------------------------------------------------------ unprojection
 // Loads the depth of 16 consecutive pixels starting at pix0; pixels at or
 // beyond P read as 0 (invalid).
@@ -101,9 +80,12 @@ __device__ __forceinline__ int block_sum_int(int v, int *smem) {
   return t;
 }
 
-__global__ void __launch_bounds__(256) k_unproject_count(const FrameDev *__restrict__ frames, int nframes) {
+// frame_of[blockIdx.x]: the frame of the CTA (a table filled on the host
+// with the frame descriptors; no search per CTA).
+__global__ void __launch_bounds__(256) k_unproject_count(const FrameDev *__restrict__ frames,
+                                                         const int *__restrict__ frame_of) {
   __shared__ int red[32];
-  int fi = find_frame<0>(frames, nframes, blockIdx.x);
+  int fi = frame_of[blockIdx.x];
   const FrameDev &f = frames[fi];
   int tile = blockIdx.x - f.tile_base;
   int P = f.rows * f.cols;
@@ -159,11 +141,12 @@ __device__ __forceinline__ void write_gaussian(const FrameDev &f, float4 *g, flo
 // row-major: within the tile, pixel order is (round, warp, lane) order.
 constexpr int kUnprojRounds = kUnprojTilePixels / 256;
 
-__global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restrict__ frames,
+                                                         const int *__restrict__ frame_of) {
   __shared__ int red[32];
   __shared__ int rcnt[kUnprojRounds * 8];  // valid pixels per (round, warp), then their exclusive prefix
   __shared__ int wtot[4];
-  int fi = find_frame<0>(frames, nframes, blockIdx.x);
+  int fi = frame_of[blockIdx.x];
   const FrameDev &f = frames[fi];
   const int tile = blockIdx.x - f.tile_base;
   const int P = f.rows * f.cols;
@@ -388,12 +371,13 @@ template <class M>
 constexpr int band_smem_bytes() { return 10 * kChunkPix * (int)sizeof(typename MomAcc<M>::T); }
 
 template <class M>
-__global__ void __launch_bounds__(kRowThreads) k_moments_band_totals(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(kRowThreads) k_moments_band_totals(const FrameDev *__restrict__ frames,
+                                                                     const int *__restrict__ frame_of) {
   typedef typename MomAcc<M>::T A;
   extern __shared__ __align__(16) unsigned char band_raw[];
   A *cs = reinterpret_cast<A *>(band_raw);  // [10][kChunkPix]
   __shared__ A wtot[kRowThreads / 32][10];
-  const int fi = find_frame<1>(frames, nframes, blockIdx.x);
+  const int fi = frame_of[blockIdx.x];
   const FrameDev &f = frames[fi];
   const int b = blockIdx.x - f.band_base;
   const int cols = f.cols;
@@ -479,10 +463,11 @@ __global__ void __launch_bounds__(kRowThreads) k_moments_band_totals(const Frame
 
 // One thread per (plane, column) of a frame: band totals -> band carries.
 template <class M>
-__global__ void __launch_bounds__(128) k_moments_band_carry(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(128) k_moments_band_carry(const FrameDev *__restrict__ frames,
+                                                            const int *__restrict__ frame_of) {
   typedef typename MomAcc<M>::T A;
   constexpr int kAhead = 8;
-  const int fi = find_frame<3>(frames, nframes, blockIdx.x);
+  const int fi = frame_of[blockIdx.x];
   const FrameDev &f = frames[fi];
   const int q = (blockIdx.x - f.col_base) * 128 + threadIdx.x;
   const size_t stride = (size_t)10 * f.cols;
@@ -826,10 +811,12 @@ void launch_depth_scale(const uint16_t *u16, const float *f32, size_t pitch_elem
                                                   orows, ocols);
 }
 
-void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof) {
+void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, const int *frame_of_tile, cudaStream_t s,
+                      Profiler *prof) {
+  (void)nframes;
   prof->begin(NICP_K_UNPROJECT, s);
-  k_unproject_count<<<total_tiles, 256, 0, s>>>(d_frames, nframes);
-  k_unproject_write<<<total_tiles, 256, 0, s>>>(d_frames, nframes);
+  k_unproject_count<<<total_tiles, 256, 0, s>>>(d_frames, frame_of_tile);
+  k_unproject_write<<<total_tiles, 256, 0, s>>>(d_frames, frame_of_tile);
   prof->end(NICP_K_UNPROJECT, s, 2);
 }
 
@@ -844,10 +831,11 @@ void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cu
 constexpr int kRowPathFrames = 2;
 
 template <class M>
-__global__ void __launch_bounds__(kRowThreads) k_moments_rowpre(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(kRowThreads) k_moments_rowpre(const FrameDev *__restrict__ frames,
+                                                                const int *__restrict__ frame_of) {
   typedef typename MomAcc<M>::T A;
   __shared__ A wtot[kRowThreads / 32][10];
-  const int fi = find_frame<1>(frames, nframes, blockIdx.x);
+  const int fi = frame_of[blockIdx.x];
   const FrameDev &f = frames[fi];
   const int r = ((int)blockIdx.x - f.band_base) * kBandRows + (int)blockIdx.y;
   if (r >= f.rows) return;  // the whole CTA
@@ -873,9 +861,10 @@ __global__ void __launch_bounds__(kRowThreads) k_moments_rowpre(const FrameDev *
 }
 
 template <class M>
-__global__ void __launch_bounds__(128) k_moments_colsum(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(128) k_moments_colsum(const FrameDev *__restrict__ frames,
+                                                        const int *__restrict__ frame_of) {
   typedef typename MomAcc<M>::T A;
-  const int fi = find_frame<3>(frames, nframes, blockIdx.x);
+  const int fi = frame_of[blockIdx.x];
   const FrameDev &f = frames[fi];
   const int cols = f.cols;
   const int q = ((int)blockIdx.x - f.col_base) * 128 + (int)threadIdx.x;  // plane * cols + column
@@ -902,7 +891,7 @@ bool moments_row_path(int nframes) { return nframes <= kRowPathFrames; }
 
 template <class M>
 static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas, int max_bands,
-                         cudaStream_t s, Profiler *prof) {
+                         const int *frame_of_band, const int *frame_of_carry, cudaStream_t s, Profiler *prof) {
   static bool configured = false;  // one attribute call per instantiation
   if (!configured) {
     cudaFuncSetAttribute(k_moments_band_totals<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes<M>());
@@ -910,13 +899,13 @@ static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands,
     configured = true;
   }
   prof->begin(NICP_K_MOMENTS_BANDS, s);
-  k_moments_band_totals<M><<<total_bands, kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, nframes);
-  k_moments_band_carry<M><<<total_carry_ctas, 128, 0, s>>>(d_frames, nframes);
+  k_moments_band_totals<M><<<total_bands, kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, frame_of_band);
+  k_moments_band_carry<M><<<total_carry_ctas, 128, 0, s>>>(d_frames, frame_of_carry);
   prof->end(NICP_K_MOMENTS_BANDS, s, 2);
   prof->begin(NICP_K_MOMENTS_SWEEP, s);
   if (moments_row_path(nframes) && max_bands <= 65535) {  // (grid y of the column sums)
-    k_moments_rowpre<M><<<dim3(total_bands, kBandRows), kRowThreads, 0, s>>>(d_frames, nframes);
-    k_moments_colsum<M><<<dim3(total_carry_ctas, max_bands), 128, 0, s>>>(d_frames, nframes);
+    k_moments_rowpre<M><<<dim3(total_bands, kBandRows), kRowThreads, 0, s>>>(d_frames, frame_of_band);
+    k_moments_colsum<M><<<dim3(total_carry_ctas, max_bands), 128, 0, s>>>(d_frames, frame_of_carry);
     prof->end(NICP_K_MOMENTS_SWEEP, s, 2);
   } else {
     k_moments_band_sweep<M><<<dim3(max_bands, nframes), kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, nframes);
@@ -928,12 +917,17 @@ int moment_band_rows() { return kBandRows; }
 size_t moment_acc_bytes(int precision) { return precision == NICP_MOMENTS_F32 ? 4 : 8; }
 
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
-                    int max_bands, cudaStream_t s, Profiler *prof) {
+                    int max_bands, const int *frame_of_band, const int *frame_of_carry, cudaStream_t s,
+                    Profiler *prof) {
   if (precision == NICP_MOMENTS_F32)
-    launch_bands<MomF32>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, s, prof);
+    launch_bands<MomF32>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, frame_of_band, frame_of_carry, s,
+                         prof);
   else if (precision == NICP_MOMENTS_TWOFLOAT)
-    launch_bands<MomTwoFloat>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, s, prof);
-  else launch_bands<MomF64>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, s, prof);
+    launch_bands<MomTwoFloat>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, frame_of_band,
+                              frame_of_carry, s, prof);
+  else
+    launch_bands<MomF64>(d_frames, nframes, total_bands, total_carry_ctas, max_bands, frame_of_band, frame_of_carry, s,
+                         prof);
 }
 
 void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_tiles, cudaStream_t s, Profiler *prof) {

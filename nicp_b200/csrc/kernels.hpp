@@ -60,7 +60,10 @@ struct Profiler {
   }
 };
 
-void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, cudaStream_t s, Profiler *prof);
+// frame_of_*: the frame of each CTA of the 1-D build grids (unprojection
+// tiles, 16-row bands, band-carry CTAs), filled on the host.
+void launch_unproject(const FrameDev *d_frames, int nframes, int total_tiles, const int *frame_of_tile, cudaStream_t s,
+                      Profiler *prof);
 void launch_depth_scale(const uint16_t *u16, const float *f32, size_t pitch_elems, int rows, int cols,
                         float depth_scale, int step, float max_cov, float *out, cudaStream_t s);
 // Integral image over 16-row bands (moment_band_rows()): total_bands band
@@ -72,7 +75,8 @@ int moment_band_rows();
 bool moments_row_path(int nframes);
 size_t moment_acc_bytes(int precision);
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
-                    int max_bands, cudaStream_t s, Profiler *prof);
+                    int max_bands, const int *frame_of_band, const int *frame_of_carry, cudaStream_t s,
+                    Profiler *prof);
 // (tile, frame) grid: max_tiles = the largest number of kStatsThreads-pixel
 // tiles of any frame of the launch; nframes <= 65535.
 void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_tiles, cudaStream_t s,
