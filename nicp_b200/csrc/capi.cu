@@ -687,7 +687,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   char *pin;
   if ((rc = pin_up(ctx, frames_bytes, &pin))) return rc;
   int *tab_all = reinterpret_cast<int *>(pin + sizeof(FrameDev) * n);
-  struct Grid { int tiles, bands, stiles, carryctas, max_bands, max_tiles, max_stiles; };
+  struct Grid { int tiles, bands, carryctas, max_bands, max_stiles; };
   std::vector<Grid> grids(chunks.size());
   for (size_t ci = 0; ci < chunks.size(); ci++) {
     const int i0 = chunks[ci].first, nf = chunks[ci].second - i0;
@@ -705,7 +705,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     }
     FrameDev *fd = reinterpret_cast<FrameDev *>(pin) + i0;
     int *tab_t = tab_all + tab_off[ci], *tab_b = tab_t + tab_tiles[ci], *tab_k = tab_b + tab_bands[ci];
-    int tiles = 0, bands = 0, stiles = 0, carryctas = 0, max_bands = 0, max_tiles = 0, max_stiles = 0;
+    int tiles = 0, bands = 0, carryctas = 0, max_bands = 0, max_stiles = 0;
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
       const nicp_camera &cam = cams[i0 + k];
@@ -727,9 +727,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       tiles += (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels);
       bands += (f.rows + nb_rows - 1) / nb_rows;
       max_bands = std::max(max_bands, (f.rows + nb_rows - 1) / nb_rows);
-      max_tiles = std::max(max_tiles, (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels));
       max_stiles = std::max(max_stiles, (int)((P + kStatsThreads - 1) / kStatsThreads));
-      stiles += (int)((P + kStatsThreads - 1) / kStatsThreads);
       carryctas += (10 * f.cols + 127) / 128;
       d.depth_scale = prm->depth_scale;
       d.min_d = cam.min_distance;
@@ -778,7 +776,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.band_tot = unproject_only ? nullptr : (void *)(ctx->ws + o_band[k]);
       d.rowpre = o_rowpre[k] ? (void *)(ctx->ws + o_rowpre[k]) : nullptr;
     }
-    grids[ci] = {tiles, bands, stiles, carryctas, max_bands, max_tiles, max_stiles};
+    grids[ci] = {tiles, bands, carryctas, max_bands, max_stiles};
   }
   FrameDev *dfr_all = (FrameDev *)(ctx->ws + o_frames_all);
   CK(ctx, cudaMemcpyAsync(dfr_all, pin, frames_bytes, cudaMemcpyHostToDevice, s));
