@@ -381,7 +381,10 @@ int nicp_linearize_noalloc(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_clou
 
 /* -------------------------------------------------------------- aligner */
 /* AlignerProjective::align for one pair (one call, one pair).  guess,
- * ref_offset, cur_offset may be NULL (identity). */
+ * ref_offset, cur_offset may be NULL (identity).  The Gauss-Newton loop is
+ * captured as a CUDA graph on the first call of a shape (image size,
+ * iteration counts, parameters) and replayed by later calls; the call
+ * synchronizes the context's stream to return its result. */
 int nicp_align(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const nicp_camera *cam,
                const float guess16[16], const float ref_offset16[16], const float cur_offset16[16],
                const nicp_corr_params *corr, const nicp_lin_params *lin,
