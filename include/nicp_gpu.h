@@ -305,7 +305,8 @@ int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *cam, const f
                float distance_threshold, float max_point_depth, int *removed);
 
 /* DepthImageConverterIntegralImage::compute.  depth: rows x cols u16 with
- * row pitch `pitch_bytes` (0 = packed), in host memory or, when
+ * row pitch `pitch_bytes` (0 = packed; otherwise at least cols * 2, else
+ * NICP_EINVAL), in host memory or, when
  * depth_on_device != 0, in device memory.  sensor_offset may be NULL
  * (identity).  index_out: optional host rows*cols int32 index image. */
 int nicp_cloud_from_depth_u16(nicp_ctx *ctx, const uint16_t *depth, int rows, int cols,

@@ -606,6 +606,8 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     if (!fin[i].depth || fin[i].rows <= 0 || fin[i].cols <= 0 || !clouds[i] || !valid_camera(&cams[i]))
       return fail(ctx, NICP_EINVAL, "bad frame " + std::to_string(i));
     if ((long long)fin[i].rows * fin[i].cols > (1ll << 30)) return fail(ctx, NICP_EINVAL, "frame too large");
+    if (fin[i].pitch && fin[i].pitch < (size_t)fin[i].cols * (fin[i].u16 ? 2 : 4))
+      return fail(ctx, NICP_EINVAL, "row pitch of frame " + std::to_string(i) + " is below its row width");
     if ((rc = cloud_reserve(clouds[i], fin[i].rows * fin[i].cols, fin[i].rows, fin[i].cols, prm->keep_stats != 0,
                             prm->keep_gaussians != 0)))
       return rc;

@@ -93,3 +93,19 @@ def test_host_batch_across_staging_chunks(ctx):
     api.build_batch(ctx, host, [cam_c] * n, prm, on_host)
     for a, b in zip(on_host, on_dev):
         _same(a, b)
+
+
+def test_short_row_pitch_rejected(ctx):
+    """A row pitch below the row width is an argument error (NICP_EINVAL),
+    caught before any copy; the context stays usable."""
+    d16, _, _, cam = synth.render_pair(73, "160x120")
+    proj, conv = converter(cam, ctx)
+    rows, cols = d16.shape
+    cam_c = proj.camera(rows, cols)
+    d = np.ascontiguousarray(d16)
+    cloud = api.Cloud(ctx)
+    rc = ctx.lib.nicp_cloud_from_depth_u16(ctx.h, C.c_void_p(d.ctypes.data), rows, cols, 2 * cols - 2, 0,
+                                           C.byref(cam_c), C.byref(conv.params()), None, cloud.h, None)
+    assert rc == L.NICP_EINVAL
+    _, idx = _build_one(ctx, conv, cam_c, d.ctypes.data, rows, cols, 0, False)
+    assert np.count_nonzero(idx >= 0) > 1000
