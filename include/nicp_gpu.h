@@ -190,7 +190,7 @@ int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable);
  * call with a new resolution mix (the multiset of pair image sizes, with the
  * iteration counts) times the Gauss-Newton loop with each candidate launch
  * shape -- z-buffer points per thread 1/2/4/8, fused correspondence +
- * linearizer CTAs per SM 1/2/as many as fit -- and keeps the fastest for
+ * linearizer CTAs per SM 2/3/as many as fit -- and keeps the fastest for
  * that mix.  Results do not depend on the launch shape (bitwise).  The
  * trials run on the context stream before the call's own loop. */
 int nicp_ctx_set_autotune(nicp_ctx *ctx, int enable);

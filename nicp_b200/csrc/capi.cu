@@ -45,6 +45,7 @@ struct Layout {
 
 struct nicp_ctx {
   int device = 0;
+  int sm_count = 148;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string err;
@@ -300,6 +301,7 @@ extern "C" int nicp_ctx_create(int device, void *stream, nicp_ctx **out) {
   if (cudaSetDevice(device) != cudaSuccess) return NICP_ECUDA;
   auto *ctx = new nicp_ctx();
   ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount > 0 ? prop.multiProcessorCount : 148;
   if (stream) {
     ctx->stream = (cudaStream_t)stream;
   } else {
@@ -310,6 +312,7 @@ extern "C" int nicp_ctx_create(int device, void *stream, nicp_ctx **out) {
     ctx->own_stream = true;
   }
   if (cudaEventCreateWithFlags(&ctx->pin_up_ev, cudaEventDisableTiming) != cudaSuccess) {
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NICP_ECUDA;
   }
@@ -1735,6 +1738,16 @@ static std::string tune_key(const PairPlan &pl, const AlignCall &a) {
   return k;
 }
 
+// Z-buffer points per thread unless the autotuner picked: once the
+// projection grid spans about two waves of its 128-thread CTAs (16 per SM),
+// more independent loads and atomics per thread pay (the 199-pair 640x480
+// sequence: 8 points per thread, 3 % faster than 4); below that (one or a
+// few pairs) more threads do.
+static int default_zb_ppt(const nicp_ctx *ctx, const PairPlan &pl) {
+  const long long ctas = (long long)pl.max_pt_tiles * pl.n;
+  return ctas >= 16ll * ctx->sm_count ? kZbufWidePPT : kZbufDefaultPPT;
+}
+
 // Times the loop with each candidate launch shape (direct launches, CUDA
 // events on the context stream) and keeps the fastest: z-buffer points per
 // thread first, then the fused kernel's CTAs per SM.  The loop re-initialises
@@ -1757,13 +1770,14 @@ static int autotune_loop(nicp_ctx *ctx, const PairPlan &pl, const AlignCall &a, 
     times.push_back(*ms);
     return NICP_OK;
   };
-  nicp_ctx::Launch cur;
+  const nicp_ctx::Launch cur = ctx->launch;  // the default shape for this call
   float ms = 0, best_ms = 0;
   int rc = trial(cur, &ms);  // warm-up (module load, caches)
   if (!rc) rc = trial(cur, &best_ms);
   *best = cur;
-  const int ppts[] = {1, 2, 8};
-  for (int i = 0; i < 3 && !rc; i++) {
+  const int ppts[] = {1, 2, 4, 8};  // the default is among them: skipped
+  for (int i = 0; i < 4 && !rc; i++) {
+    if (ppts[i] == cur.zb_ppt) continue;
     nicp_ctx::Launch c = *best;
     c.zb_ppt = ppts[i];
     if (!(rc = trial(c, &ms)) && ms < best_ms) { best_ms = ms; *best = c; }
@@ -1837,6 +1851,7 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
   CK(ctx, cudaEventRecord(ctx->pin_up_ev, s));
   ctx->h2d_bytes += (sizeof(PairDev) + 48 + 256) * (unsigned long long)a.n;
   ctx->launch = nicp_ctx::Launch();
+  ctx->launch.zb_ppt = default_zb_ppt(ctx, pl);
   if (ctx->autotune && !list_mode) {
     std::string tk = tune_key(pl, a);
     auto it = ctx->tuned.find(tk);

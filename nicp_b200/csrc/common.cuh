@@ -30,7 +30,8 @@ constexpr int kStatsThreads = 256;
 constexpr int kPartialWords = 32;       // doubles per CTA partial (21 H + 6 b + chi2 + inliers + C + K + pad)
 constexpr int kSolveCrossF32 = 32;      // k_solve mode bit: FP32 sum of the tile partials
 constexpr int kPointsPerCta = 1024;     // z-buffer kernel tile (points per CTA; threads = 1024 / points per thread)
-constexpr int kZbufDefaultPPT = 4;      // points per thread unless the autotuner picked another
+constexpr int kZbufDefaultPPT = 4;      // points per thread for small grids (one or a few clouds)
+constexpr int kZbufWidePPT = 8;         // points per thread for grids of two waves or more
 
 // pts[i].w is kNoNormalW for a point without a normal, and 1 + class for a
 // point with one, class = (point information matrix non-flat) + 2 (normal

@@ -52,6 +52,7 @@ def test_autotuned_shapes_give_identical_results(ctx, batch):
     prm = _params(ctx)
     ctx.set_autotune(False)
     base = _run(ctx, batch, prm)
+    # six pairs: fewer than two waves of z-buffer CTAs, so 4 points per thread
     assert ctx.launch_shape()[:2] == (4, 0)
     ctx.set_autotune(True)
     try:
