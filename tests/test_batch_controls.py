@@ -81,3 +81,27 @@ def test_early_exit(ctx, batch):
             assert er < 2e-3 and et < 2e-3, (er, et, e.outer_iterations_run)
         else:
             assert np.array_equal(np.array(e.T), np.array(f.T))
+
+
+def test_wide_batch_default_shape_matches_single_pairs(ctx):
+    """Eight 640x480 pairs give a z-buffer grid of two waves or more, where
+    the default is 8 points per thread; a pair alone runs with 4.  Both must
+    give bitwise the same poses (the z-buffer's atomicMin is order-free)."""
+    refs, curs, cams = [], [], []
+    for seed in range(61, 69):
+        d1, d2, _, cam = synth.render_pair(seed, "640x480", deg=0.5, deg_hi=5.0, meters=0.01, m_hi=0.08)
+        proj, conv = converter(cam, ctx)
+        refs.append(gpu_cloud(ctx, conv, d1, keep_index=False)[0])
+        curs.append(gpu_cloud(ctx, conv, d2, keep_index=False)[0])
+        cams.append(proj.camera())
+    prm = _params(ctx, outer=10, inner=1)
+    corr = api.CorrespondenceFinderProjective(ctx).params()
+    lin = api.Linearizer(ctx).params()
+    ctx.set_autotune(False)
+    wide = api.align_batch(ctx, refs, curs, cams, None, corr, lin, prm)
+    assert ctx.launch_shape()[:2] == (8, 0)
+    for i in range(len(refs)):
+        one = api.align_batch(ctx, refs[i:i + 1], curs[i:i + 1], cams[i:i + 1], None, corr, lin, prm)
+        assert ctx.launch_shape()[:2] == (4, 0)
+        assert np.array_equal(np.array(one[0].T), np.array(wide[i].T))
+        assert one[0].inliers == wide[i].inliers
