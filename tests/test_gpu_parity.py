@@ -458,3 +458,30 @@ def test_moments_precision_variants(ctx):
     print("max normal angle vs F64 oracle:", res)
     assert res[L.NICP_MOMENTS_F64] < 1e-5
     assert res[L.NICP_MOMENTS_TWOFLOAT] < 1e-5
+
+
+def test_empty_frame_and_alignment_against_it(ctx):
+    """An all-invalid depth frame (every pixel 0) gives an empty cloud and an
+    index image of -1.  Aligning with it on either side finds no
+    correspondences, so the pose stays at the guess (identity) with 0 inliers
+    and zero error, bitwise as in the oracle."""
+    _, d2, _, cam = synth.render_pair(5, "160x120")
+    proj, conv = converter(cam, ctx)
+    _, oc = cams(cam)
+    z = np.zeros_like(d2)
+    empty, eidx = gpu_cloud(ctx, conv, z)
+    assert len(empty) == 0 and (eidx == -1).all()
+    full, _ = gpu_cloud(ctx, conv, d2, keep_index=False)
+    oempty, oidx = O.build_cloud(O.REF32, z, oc)
+    assert np.array_equal(eidx, oidx)
+    ofull, _ = O.build_cloud(O.F64, d2, oc)
+    oempty64, _ = O.build_cloud(O.F64, z, oc)
+    for ref, cur, oref, ocur in ((empty, full, oempty64, ofull), (full, empty, ofull, oempty64)):
+        al = api.AlignerProjective(proj, api.Linearizer(ctx), api.CorrespondenceFinderProjective(ctx), ctx)
+        al.setReferenceCloud(ref)
+        al.setCurrentCloud(cur)
+        al.align()
+        r = O.align(O.F64, oref, ocur, oc)
+        assert r["inliers"] == 0 and np.array_equal(r["T"], np.eye(4))
+        assert al.inliers() == 0 and al.error() == 0.0
+        assert np.array_equal(al.T(), np.eye(4))
