@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <new>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -241,7 +242,19 @@ extern "C" int nicp_cloud_load(nicp_cloud *cloud, const char *filename, const ni
   nicp_default_cloud_params(&def);
   const nicp_cloud_params &P = prm ? *prm : def;
   const size_t n = (size_t)count;
-  std::vector<float> pts(4 * n), nrm(4 * n), omg(12 * n), st(kStatsWords * n);
+  // The arrays grow with the records actually read: the header's count
+  // bounds the loop but does not size an allocation (a damaged or hostile
+  // header could claim 2^30 points).
+  std::vector<float> pts, nrm, omg, st;
+  try {
+    const size_t r = std::min<size_t>(n, (size_t)1 << 16);
+    pts.reserve(4 * r);
+    nrm.reserve(4 * r);
+    omg.reserve(12 * r);
+    st.reserve(kStatsWords * r);
+  } catch (const std::bad_alloc &) {
+    return NICP_ENOMEM;
+  }
   int normals = 0;
   size_t k = 0;
   while (k < n && is.good()) {
@@ -264,6 +277,14 @@ extern "C" int nicp_cloud_load(nicp_cloud *cloud, const char *filename, const ni
       is.read((char *)raw, kStatsBytes);
       if (!is) break;
       s = unpack_stats(raw);
+    }
+    try {
+      pts.resize(4 * (k + 1));
+      nrm.resize(4 * (k + 1));
+      omg.resize(12 * (k + 1));
+      st.resize(kStatsWords * (k + 1));
+    } catch (const std::bad_alloc &) {
+      return NICP_ENOMEM;
     }
     // the device record: eigenvalues, eigenvectors, mean, n
     float *rec = &st[kStatsWords * k];

@@ -6,6 +6,7 @@ the expected bytes of a binary .nicp file from the cloud's downloaded arrays
 (Point, Normal, then the 96-byte Stats: 4x4 column-major, int n,
 eigenvalues, bool curvatureComputed at byte 80, float curvature at 84,
 zero padding), and the expected text lines with iostream's %g formatting."""
+import ctypes as C
 import math
 import struct
 
@@ -147,3 +148,12 @@ def test_step_and_header_count(ctx, tmp_path):
     bad.write_bytes(b"NOTACLOUD 3 1\n0 0 0 0 0 0\n")
     with pytest.raises(L.NicpError):
         api.Cloud(ctx).load(bad)
+    # a header that claims more points than the file holds (2^24 here): the
+    # records present are loaded, memory follows them (not the header), and
+    # the call reports NICP_EINVAL
+    short = tmp_path / "short.nicp"
+    short.write_bytes(b"NICPCLOUD %d 1\n" % (1 << 24) + line2 + b"\n" + body[:256])
+    got = api.Cloud(ctx)
+    k = C.c_int(-1)
+    rc = ctx.lib.nicp_cloud_load(got.h, str(short).encode(), None, None, C.byref(k))
+    assert rc == L.NICP_EINVAL and k.value == 2 and got.size() == 2
