@@ -33,7 +33,8 @@
  * Conventions
  *   - Every function returns an int status (NICP_OK on success); the text of
  *     the last failure on a context is nicp_ctx_last_error().  No C++
- *     exception crosses this boundary.
+ *     exception crosses this boundary: a host allocation failure inside a
+ *     call returns NICP_ENOMEM (any other exception NICP_ESTATE).
  *   - Matrices are row-major.  Transforms are 4x4 isometries; row 3 is
  *     forced to (0 0 0 1) as the reference does.
  *   - Host buffers are caller-owned; device buffers (clouds, scratch) are

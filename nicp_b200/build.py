@@ -23,7 +23,7 @@ SYNTH_LIB = os.path.join(HERE, "libnicp_synth.so")
 
 CUDA_SOURCES = ["k_cloud.cu", "k_align.cu", "k_merge.cu", "k_nn.cu", "capi.cu"]
 HOST_SOURCES = ["stats_host.cpp", "server.cpp", "cloud_io.cpp"]
-HEADERS = ["common.cuh", "kernels.hpp", "host_math.hpp"]
+HEADERS = ["common.cuh", "kernels.hpp", "host_math.hpp", "abi_guard.hpp"]
 
 NVCC = os.environ.get("NVCC", "nvcc")
 # The image may export CXX pointing at a toolchain without libgomp.

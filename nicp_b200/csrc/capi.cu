@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "abi_guard.hpp"
 #include "common.cuh"
 #include "host_math.hpp"
 #include "kernels.hpp"
@@ -288,6 +289,7 @@ extern "C" void nicp_default_align_params(nicp_align_params *p) {
 
 // ------------------------------------------------------------------ context
 extern "C" int nicp_ctx_create(int device, void *stream, nicp_ctx **out) {
+  NICP_ABI_TRY
   if (!out) return NICP_EINVAL;
   *out = nullptr;
   int n = 0;
@@ -318,9 +320,11 @@ extern "C" int nicp_ctx_create(int device, void *stream, nicp_ctx **out) {
   }
   *out = ctx;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_ctx_destroy(nicp_ctx *ctx) {
+  NICP_ABI_TRY
   if (!ctx) return NICP_EINVAL;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
@@ -337,14 +341,17 @@ extern "C" int nicp_ctx_destroy(nicp_ctx *ctx) {
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" const char *nicp_ctx_last_error(const nicp_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 extern "C" int nicp_ctx_synchronize(nicp_ctx *ctx) {
+  NICP_ABI_TRY
   if (!ctx) return NICP_EINVAL;
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" void *nicp_ctx_stream(nicp_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
@@ -352,29 +359,36 @@ extern "C" void *nicp_ctx_stream(nicp_ctx *ctx) { return ctx ? (void *)ctx->stre
 extern "C" size_t nicp_ctx_device_bytes(const nicp_ctx *ctx) { return ctx ? ctx->ws_cap + ctx->cloud_bytes : 0; }
 
 extern "C" int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable) {
+  NICP_ABI_TRY
   if (!ctx) return NICP_EINVAL;
   ctx->prof.enabled = enable != 0;
   ctx->prof.recs.clear();
   ctx->prof.next = 0;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_ctx_set_autotune(nicp_ctx *ctx, int enable) {
+  NICP_ABI_TRY
   if (!ctx) return NICP_EINVAL;
   ctx->autotune = enable != 0;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_ctx_launch_shape(const nicp_ctx *ctx, int *zbuffer_points_per_thread, int *corr_ctas_per_sm,
                                      int *tuned_mixes) {
+  NICP_ABI_TRY
   if (!ctx) return NICP_EINVAL;
   if (zbuffer_points_per_thread) *zbuffer_points_per_thread = ctx->launch.zb_ppt;
   if (corr_ctas_per_sm) *corr_ctas_per_sm = ctx->launch.corr_ctas;
   if (tuned_mixes) *tuned_mixes = (int)ctx->tuned.size();
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_ctx_read_profile(nicp_ctx *ctx, int kernel, double *total_ms, int *launches) {
+  NICP_ABI_TRY
   if (!ctx || kernel < 0 || kernel >= NICP_K_COUNT) return NICP_EINVAL;
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   double t = 0;
@@ -395,15 +409,18 @@ extern "C" int nicp_ctx_read_profile(nicp_ctx *ctx, int kernel, double *total_ms
   if (total_ms) *total_ms = t;
   if (launches) *launches = n;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" unsigned long long nicp_ctx_kernel_launches(const nicp_ctx *ctx) { return ctx ? ctx->prof.launches : 0; }
 
 extern "C" int nicp_ctx_transfer_bytes(const nicp_ctx *ctx, unsigned long long *h2d, unsigned long long *d2h) {
+  NICP_ABI_TRY
   if (!ctx) return NICP_EINVAL;
   if (h2d) *h2d = ctx->h2d_bytes;
   if (d2h) *d2h = ctx->d2h_bytes;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" const char *nicp_kernel_name(int k) {
@@ -415,14 +432,17 @@ extern "C" const char *nicp_kernel_name(int k) {
 
 // ------------------------------------------------------------------ clouds
 extern "C" int nicp_cloud_create(nicp_ctx *ctx, nicp_cloud **out) {
+  NICP_ABI_TRY
   if (!ctx || !out) return NICP_EINVAL;
   auto *c = new nicp_cloud();
   c->ctx = ctx;
   *out = c;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_destroy(nicp_cloud *c) {
+  NICP_ABI_TRY
   if (!c) return NICP_EINVAL;
   if (c->mem) {
     cudaStreamSynchronize(c->ctx->stream);
@@ -431,19 +451,23 @@ extern "C" int nicp_cloud_destroy(nicp_cloud *c) {
   }
   delete c;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_size(nicp_cloud *c, int *n) {
+  NICP_ABI_TRY
   if (!c || !n) return NICP_EINVAL;
   if (!c->mem) { *n = 0; return NICP_OK; }
   nicp_ctx *ctx = c->ctx;
   CK(ctx, cudaMemcpyAsync(n, c->count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *curv, float *op9, float *on9, float *ev3,
                                    float *U9) {
+  NICP_ABI_TRY
   if (!c) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int n = 0;
@@ -479,9 +503,11 @@ extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *c
     if (U9) for (int k = 0; k < 9; k++) U9[9 * (size_t)i + k] = eig[kStatsWords * (size_t)i + 3 + k];
   }
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_download_stats(nicp_cloud *c, float *eigval3, float *eigvec9, float *mean3, int *n_out) {
+  NICP_ABI_TRY
   if (!c) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int n = 0;
@@ -500,9 +526,11 @@ extern "C" int nicp_cloud_download_stats(nicp_cloud *c, float *eigval3, float *e
     if (n_out) n_out[i] = (int)r[15];
   }
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_download_gaussians(nicp_cloud *c, float *mean3, float *cov9) {
+  NICP_ABI_TRY
   if (!c) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int n = 0;
@@ -519,10 +547,12 @@ extern "C" int nicp_cloud_download_gaussians(nicp_cloud *c, float *mean3, float 
     if (cov9) for (int k = 0; k < 9; k++) cov9[9 * (size_t)i + k] = o[3 + k];
   }
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const float *n4, const float *curv,
                                  const float *op9, const float *on9) {
+  NICP_ABI_TRY
   if (!c || n < 0 || (n > 0 && (!p4 || !n4 || !curv))) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int rc = cloud_reserve(c, n, c->rows, c->cols, false);
@@ -549,9 +579,11 @@ extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const fl
   CK(ctx, cudaMemcpyAsync(c->count, counts, sizeof(counts), cudaMemcpyHostToDevice, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_transform(nicp_cloud *c, const float T16[16]) {
+  NICP_ABI_TRY
   if (!c || !T16) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   if (!c->mem) return NICP_OK;
@@ -573,6 +605,7 @@ extern "C" int nicp_cloud_transform(nicp_cloud *c, const float T16[16]) {
                          c->count, c->capacity, (const float *)(ctx->ws + o), ctx->stream, &ctx->prof);
   CK(ctx, cudaGetLastError());
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ cloud build
@@ -868,18 +901,23 @@ static int build_one(nicp_ctx *ctx, const void *depth, bool u16, int rows, int c
 extern "C" int nicp_cloud_from_depth_u16(nicp_ctx *ctx, const uint16_t *depth, int rows, int cols, size_t pitch,
                                          int on_device, const nicp_camera *cam, const nicp_cloud_params *prm,
                                          const float *offset, nicp_cloud *out, int32_t *index_out) {
+  NICP_ABI_TRY
   return build_one(ctx, depth, true, rows, cols, pitch, on_device, cam, prm, offset, out, index_out);
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_from_depth_f32(nicp_ctx *ctx, const float *depth, int rows, int cols, size_t pitch,
                                          int on_device, const nicp_camera *cam, const nicp_cloud_params *prm,
                                          const float *offset, nicp_cloud *out, int32_t *index_out) {
+  NICP_ABI_TRY
   return build_one(ctx, depth, false, rows, cols, pitch, on_device, cam, prm, offset, out, index_out);
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *rows, const int *cols,
                                 int on_device, const nicp_camera *cams, const nicp_cloud_params *prm,
                                 nicp_cloud *const *out) {
+  NICP_ABI_TRY
   if (!ctx || n < 0 || (n > 0 && (!depth || !rows || !cols || !cams || !prm || !out))) return NICP_EINVAL;
   std::vector<FrameIn> f(n);
   for (int i = 0; i < n; i++) {
@@ -887,20 +925,24 @@ extern "C" int nicp_build_batch(nicp_ctx *ctx, int n, const uint16_t *const *dep
     f[i] = FrameIn{depth[i], true, on_device != 0, 0, rows[i], cols[i], nullptr};
   }
   return build_frames(ctx, n, f.data(), cams, prm, out, false);
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ projector API
 extern "C" int nicp_projector_matrices(const nicp_camera *cam, const float T16[16], float KRt16[16], float iKRt16[16]) {
+  NICP_ABI_TRY
   if (!cam || !KRt16 || !iKRt16) return NICP_EINVAL;
   HM4 K, iK;
   projector_matrices(*cam, HM4::from(T16), K, iK);
   std::memcpy(KRt16, K.a, sizeof(K.a));
   std::memcpy(iKRt16, iK.a, sizeof(iK.a));
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_unproject(nicp_ctx *ctx, const float *depth, int rows, int cols, const nicp_camera *cam,
                               const float T16[16], float *points4_out, int32_t *index_out, int *n) {
+  NICP_ABI_TRY
   if (!ctx || !depth || !cam || !n) return NICP_EINVAL;
   int rc;
   if (!ctx->scratch_cloud && (rc = nicp_cloud_create(ctx, &ctx->scratch_cloud))) return rc;
@@ -916,10 +958,12 @@ extern "C" int nicp_unproject(nicp_ctx *ctx, const float *depth, int rows, int c
   if (index_out) CK(ctx, cudaMemcpyAsync(index_out, c->index, 4 * (size_t)rows * cols, cudaMemcpyDeviceToHost, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_project_intervals(nicp_ctx *ctx, const float *depth, int rows, int cols, const nicp_camera *cam,
                                       float world_radius, int32_t *radius_out) {
+  NICP_ABI_TRY
   if (!ctx || !depth || !cam || !radius_out || rows <= 0 || cols <= 0) return NICP_EINVAL;
   size_t P = (size_t)rows * cols;
   Layout L;
@@ -938,6 +982,7 @@ extern "C" int nicp_project_intervals(nicp_ctx *ctx, const float *depth, int row
   CK(ctx, cudaMemcpyAsync(radius_out, ctx->ws + o_o, 4 * P, cudaMemcpyDeviceToHost, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ pair workspace
@@ -1046,6 +1091,7 @@ static void fill_pairs(nicp_ctx *ctx, const PairPlan &pl, const nicp_camera *cam
 extern "C" int nicp_correspond(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const int32_t *ref_index,
                                const int32_t *cur_index, int rows, int cols, const float T16[16],
                                const nicp_corr_params *prm, int32_t *pairs_out, int *num_out) {
+  NICP_ABI_TRY
   if (!ctx || !ref || !cur || !ref_index || !cur_index || rows <= 0 || cols <= 0 || !T16 || !prm || !num_out)
     return NICP_EINVAL;
   nicp_camera cam;
@@ -1078,11 +1124,13 @@ extern "C" int nicp_correspond(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_
     CK(ctx, cudaStreamSynchronize(s));
   }
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const int32_t *pairs,
                               int num_pairs, const float T16[16], const nicp_lin_params *prm, int parity_threads,
                               double H36[36], double b6[6], double *error, int *inliers) {
+  NICP_ABI_TRY
   if (!ctx || !ref || !cur || (num_pairs > 0 && !pairs) || num_pairs < 0 || !T16 || !prm) return NICP_EINVAL;
   // list slots are tiled like pixels: a one-row image of num_pairs pixels
   nicp_camera cam;
@@ -1122,6 +1170,7 @@ extern "C" int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_c
   if (error) *error = st->error;
   if (inliers) *inliers = st->inliers;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 // Scratch-free linearizer (see nicp_gpu.h): unpacks the cloud handles and
@@ -1129,6 +1178,7 @@ extern "C" int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_c
 extern "C" int nicp_linearize_noalloc(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur,
                                       const int32_t *pairs_dev, int num_pairs, const float T16[16],
                                       const nicp_lin_params *prm, int parity_threads, double *out_dev) {
+  NICP_ABI_TRY
   if (!ctx || !ref || !cur || !T16 || !prm || !out_dev || num_pairs < 0 || (num_pairs > 0 && !pairs_dev))
     return NICP_EINVAL;
   if (num_pairs > NICP_LINEARIZE_NOALLOC_MAX_PAIRS) return NICP_EINVAL;
@@ -1150,11 +1200,13 @@ extern "C" int nicp_linearize_noalloc(nicp_ctx *ctx, const nicp_cloud *ref, cons
   rows12(HM4::from(T16), a.T);
   a.lp = lin_params(*prm);
   return lin_noalloc(a, out_dev, ctx->stream);
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ projection API
 extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_camera *cam, const float T16[16],
                             int32_t *index_out, float *depth_out) {
+  NICP_ABI_TRY
   if (!ctx || !cloud || !cam || !valid_camera(cam)) return NICP_EINVAL;
   PairPlan pl;
   int rc;
@@ -1182,12 +1234,14 @@ extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_c
   if (depth_out) CK(ctx, cudaMemcpyAsync(depth_out, ctx->ws + o_depth, 4 * P, cudaMemcpyDeviceToHost, s));
   CK(ctx, cudaStreamSynchronize(s));
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ multi-resolution input
 extern "C" int nicp_depth_scale(nicp_ctx *ctx, const void *depth, int is_u16, int rows, int cols, size_t pitch_bytes,
                                 int on_device, float depth_scale, int step, float max_depth_cov, float *out,
                                 int out_on_device) {
+  NICP_ABI_TRY
   if (!ctx || !depth || !out || rows <= 0 || cols <= 0 || step < 1) return NICP_EINVAL;
   const size_t elem = is_u16 ? 2 : 4;
   if (pitch_bytes == 0) pitch_bytes = elem * (size_t)cols;
@@ -1223,6 +1277,7 @@ extern "C" int nicp_depth_scale(nicp_ctx *ctx, const void *depth, int is_u16, in
     ctx->d2h_bytes += out_bytes;
   }
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ nearest-neighbour association
@@ -1344,6 +1399,7 @@ NNQuery nn_query(nicp_ctx *ctx, const NNPlan &pl, const nicp_cloud *ref, const n
 extern "C" int nicp_correspond_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const float T16[16],
                                   float normal_scaling, const nicp_corr_params *corr, int32_t *pairs_out,
                                   int *num_pairs) {
+  NICP_ABI_TRY
   if (!ctx || !ref || !cur || !T16 || !corr || !num_pairs) return NICP_EINVAL;
   NNPlan pl;
   int rc = nn_plan(ctx, ref, cur, corr->inlier_distance_threshold, pl);
@@ -1368,11 +1424,13 @@ extern "C" int nicp_correspond_nn(nicp_ctx *ctx, const nicp_cloud *ref, const ni
     CK(ctx, cudaMemcpy(pairs_out, ctx->ws + pl.o_pairs, 8 * (size_t)K, cudaMemcpyDeviceToHost));
   *num_pairs = K;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_align_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud *cur, const float guess16[16],
                              float normal_scaling, const nicp_corr_params *corr, const nicp_lin_params *lin,
                              const nicp_align_params *prm, nicp_align_result *out) {
+  NICP_ABI_TRY
   if (!ctx || !ref || !cur || !corr || !lin || !prm || !out) return NICP_EINVAL;
   if (prm->outer_iterations < 0 || prm->inner_iterations < 1 || prm->outer_iterations > 1000 ||
       prm->inner_iterations > 100)
@@ -1449,6 +1507,7 @@ extern "C" int nicp_align_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cl
                             out->translational_ratio > prm->translational_min_eigen_ratio);
   }
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ scene
@@ -1506,6 +1565,7 @@ static int cloud_counts2(nicp_cloud *c, int out[2]) {
 }
 
 extern "C" int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[16]) {
+  NICP_ABI_TRY
   if (!dst || !src || dst == src || dst->ctx != src->ctx) return NICP_EINVAL;
   nicp_ctx *ctx = dst->ctx;
   int rc = T16 ? nicp_cloud_transform(src, T16) : NICP_OK;  // Cloud::add moves the added cloud itself
@@ -1548,10 +1608,12 @@ extern "C" int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[
   dst->omega_structured = structured;
   if (empty) std::memcpy(dst->omd, src->omd, sizeof(src->omd));
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *cam, const float T16[16],
                           float distance_threshold, float max_point_depth, int *removed) {
+  NICP_ABI_TRY
   if (!ctx || !cloud || !cam || !valid_camera(cam) || cloud->ctx != ctx) return NICP_EINVAL;
   if (removed) *removed = 0;
   int cnt[2];
@@ -1635,6 +1697,7 @@ extern "C" int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *c
   if ((rc = cloud_counts2(cloud, after))) return rc;
   if (removed) *removed = n - after[0];
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ aligner
@@ -1932,17 +1995,21 @@ extern "C" int nicp_align(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud
                           const float guess16[16], const float ref_offset16[16], const float cur_offset16[16],
                           const nicp_corr_params *corr, const nicp_lin_params *lin, const nicp_align_params *prm,
                           nicp_align_result *out) {
+  NICP_ABI_TRY
   // replayed from a cached CUDA graph like a batch: the pair descriptors are
   // uploaded per call, so one graph serves every pair of the same shape
   AlignCall a{1, &ref, &cur, cam, guess16, ref_offset16, cur_offset16, corr, lin, prm, true};
   return align_impl(ctx, a, out);
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs, const nicp_cloud *const *curs,
                                 const nicp_camera *cams, const float *guesses, const nicp_corr_params *corr,
                                 const nicp_lin_params *lin, const nicp_align_params *prm, nicp_align_result *out) {
+  NICP_ABI_TRY
   AlignCall a{n, refs, curs, cams, guesses, nullptr, nullptr, corr, lin, prm, true};
   return align_impl(ctx, a, out);
+  NICP_ABI_CATCH
 }
 
 // ------------------------------------------------------------------ internal hooks of the server

@@ -34,6 +34,7 @@
 #include <string>
 #include <vector>
 
+#include "abi_guard.hpp"
 #include "nicp_gpu.h"
 
 namespace nicp {
@@ -185,6 +186,7 @@ float curvature_of(const StatsRec &s) {
 }  // namespace
 
 extern "C" int nicp_cloud_save(nicp_cloud *cloud, const char *filename, const float T16[16], int step, int binary) {
+  NICP_ABI_TRY
   if (!cloud || !filename || step < 1) return NICP_EINVAL;
   std::vector<float> pts, nrm, st;
   bool has_stats = false;
@@ -218,10 +220,12 @@ extern "C" int nicp_cloud_save(nicp_cloud *cloud, const char *filename, const fl
     }
   }
   return os.good() ? NICP_OK : NICP_EINVAL;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_cloud_load(nicp_cloud *cloud, const char *filename, const nicp_cloud_params *prm,
                                float T16_out[16], int *num_points) {
+  NICP_ABI_TRY
   if (!cloud || !filename) return NICP_EINVAL;
   std::ifstream is(filename, std::ios::binary);
   if (!is) return NICP_EINVAL;
@@ -331,9 +335,11 @@ extern "C" int nicp_cloud_load(nicp_cloud *cloud, const char *filename, const ni
   if (rc) return rc;
   if (num_points) *num_points = (int)k;
   return k == n ? NICP_OK : NICP_EINVAL;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_trajectory_line(const char *timestamp, const float T16[16], char *out, size_t capacity) {
+  NICP_ABI_TRY
   if (!timestamp || !T16 || !out) return NICP_EINVAL;
   double R[3][3], q[4];
   rot_of(T16, R);
@@ -345,4 +351,5 @@ extern "C" int nicp_trajectory_line(const char *timestamp, const float T16[16], 
   if (s.size() + 1 > capacity) return NICP_EINVAL;
   std::memcpy(out, s.c_str(), s.size() + 1);
   return NICP_OK;
+  NICP_ABI_CATCH
 }

@@ -25,6 +25,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "abi_guard.hpp"
 #include "nicp_gpu.h"
 
 namespace nicp {
@@ -277,6 +278,7 @@ extern "C" void nicp_default_server_params(nicp_server_params *p) {
 }
 
 extern "C" int nicp_server_create(int device, const nicp_server_params *prm, nicp_server **out) {
+  NICP_ABI_TRY
   if (!prm || !out || prm->workers < 1 || prm->workers > 16 || prm->max_batch < 1) return NICP_EINVAL;
   *out = nullptr;
   auto *s = new nicp_server();
@@ -295,10 +297,12 @@ extern "C" int nicp_server_create(int device, const nicp_server_params *prm, nic
   for (int w = 0; w < prm->workers; w++) s->threads.emplace_back([s, w] { s->worker(w); });
   *out = s;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_server_submit(nicp_server *s, int stream_id, uint64_t request_id, const uint16_t *depth, int rows,
                                   int cols, const nicp_camera *cam) {
+  NICP_ABI_TRY
   if (!s || !depth || rows <= 0 || cols <= 0 || !cam) return NICP_EINVAL;
   Request r;
   r.submitted = Clock::now();  // latency counts the copy of the frame below
@@ -317,9 +321,11 @@ extern "C" int nicp_server_submit(nicp_server *s, int stream_id, uint64_t reques
   }
   s->cv_work.notify_one();
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_server_poll(nicp_server *s, nicp_server_result *out, int max, int *n, int wait_ms) {
+  NICP_ABI_TRY
   if (!s || !out || !n || max < 0) return NICP_EINVAL;
   std::unique_lock<std::mutex> lk(s->m);
   if (s->done.empty() && wait_ms > 0)
@@ -331,9 +337,11 @@ extern "C" int nicp_server_poll(nicp_server *s, nicp_server_result *out, int max
   }
   *n = k;
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_server_status(nicp_server *s, int *pending, size_t *device_bytes) {
+  NICP_ABI_TRY
   if (!s) return NICP_EINVAL;
   std::lock_guard<std::mutex> lk(s->m);
   if (pending) *pending = s->npending + s->inflight_requests;
@@ -343,9 +351,11 @@ extern "C" int nicp_server_status(nicp_server *s, int *pending, size_t *device_b
     *device_bytes = b;
   }
   return NICP_OK;
+  NICP_ABI_CATCH
 }
 
 extern "C" int nicp_server_destroy(nicp_server *s) {
+  NICP_ABI_TRY
   if (!s) return NICP_EINVAL;
   {
     std::lock_guard<std::mutex> lk(s->m);
@@ -357,4 +367,5 @@ extern "C" int nicp_server_destroy(nicp_server *s) {
   for (auto *c : s->ctxs) nicp_ctx_destroy(c);
   delete s;
   return NICP_OK;
+  NICP_ABI_CATCH
 }

@@ -102,3 +102,52 @@ def test_bad_arguments_rejected(built):
     lib = L.load()
     assert lib.nicp_ctx_create(0, None, None) == L.NICP_EINVAL
     assert lib.nicp_projector_matrices(None, None, None, None) == L.NICP_EINVAL
+
+
+GUARD_PROBE = r"""
+#include <cstdio>
+#include <stdexcept>
+#include <vector>
+#include "abi_guard.hpp"
+
+static int entry(int what) {
+  NICP_ABI_TRY
+  if (what == 1) throw std::bad_alloc();
+  if (what == 2) { std::vector<double> v; v.reserve(v.max_size() + 1); }
+  if (what == 3) throw std::runtime_error("other");
+  return NICP_OK;
+  NICP_ABI_CATCH
+}
+
+int main() {
+  for (int w = 0; w < 4; w++) std::printf("%d ", entry(w));
+  return 0;
+}
+"""
+
+
+def test_abi_guard_turns_exceptions_into_status(tmp_path):
+    """Every C entry point runs inside NICP_ABI_TRY / NICP_ABI_CATCH: an
+    allocation failure or an oversized container request comes back as
+    NICP_ENOMEM, any other exception as NICP_ESTATE, and nothing escapes."""
+    import subprocess
+    src = tmp_path / "guard.cpp"
+    src.write_text(GUARD_PROBE)
+    exe = tmp_path / "guard"
+    subprocess.run([os.environ.get("NICP_CXX", "g++"), "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                    "-I", os.path.join(ROOT, "nicp_b200", "csrc"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert [int(x) for x in out] == [L.NICP_OK, L.NICP_ENOMEM, L.NICP_ENOMEM, L.NICP_ESTATE]
+
+
+def test_every_entry_point_is_guarded():
+    """Each `extern "C" int` definition in the library's sources opens with
+    NICP_ABI_TRY and closes with NICP_ABI_CATCH."""
+    csrc = os.path.join(ROOT, "nicp_b200", "csrc")
+    for name in ("capi.cu", "cloud_io.cpp", "server.cpp"):
+        src = open(os.path.join(csrc, name)).read()
+        defs = re.findall(r'^extern "C" int (nicp_\w+)\([^;{]*\)\s*\{\n  NICP_ABI_TRY\n', src, flags=re.M)
+        total = re.findall(r'^extern "C" int (nicp_\w+)\([^;{]*\)\s*\{', src, flags=re.M)
+        assert total and sorted(defs) == sorted(total), (name, sorted(set(total) - set(defs)))
+        assert src.count("NICP_ABI_CATCH") == len(total), name
