@@ -975,22 +975,39 @@ void launch_resolve(const PairDev *d_pairs, int npairs, int max_tiles, int to_re
 
 // Persistent grid: as many CTAs as fit on the device at once, never more
 // than there are tiles.
+// The shared-memory opt-in holds for the device that was current when it was
+// set, and the occupancy is that device's: both are taken once per device
+// (std::call_once: host threads on other contexts wait rather than race).
 template <bool kStructured>
 static int corr_lin_grid(int total_tiles, int ctas_per_sm) {
-  static int resident = 0, sm_count = 0, per_sm_max = 0;
-  if (!resident) {
+  struct Occupancy {
+    int sm_count = 1, per_sm_max = 1;
+  };
+  constexpr int kMaxDevices = 64;
+  static Occupancy occ[kMaxDevices];
+  static std::once_flag once[kMaxDevices];
+  auto query = [](int dev, Occupancy *o) {
     cudaFuncSetAttribute(k_corr_lin<kStructured>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          corr_smem<kStructured>());
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
+    int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lin<kStructured>, kFusedThreads,
                                                   corr_smem<kStructured>());
-    per_sm_max = std::max(1, per_sm);
-    sm_count = std::max(1, sms);
-    resident = sm_count * per_sm_max;
+    o->per_sm_max = std::max(1, per_sm);
+    o->sm_count = std::max(1, sms);
+  };
+  int dev = 0;
+  cudaGetDevice(&dev);
+  Occupancy local;
+  const Occupancy *o = &local;
+  if (dev >= 0 && dev < kMaxDevices) {
+    std::call_once(once[dev], query, dev, &occ[dev]);
+    o = &occ[dev];
+  } else {
+    query(dev, &local);
   }
-  int grid = (ctas_per_sm > 0 && ctas_per_sm < per_sm_max) ? sm_count * ctas_per_sm : resident;
+  const int resident = o->sm_count * o->per_sm_max;
+  const int grid = (ctas_per_sm > 0 && ctas_per_sm < o->per_sm_max) ? o->sm_count * ctas_per_sm : resident;
   return std::min(total_tiles, grid);
 }
 

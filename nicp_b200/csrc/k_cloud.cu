@@ -22,6 +22,8 @@
 //       Cloud::transformInPlace (cloud.cpp:191-204).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.hpp"
 
@@ -889,15 +891,30 @@ __global__ void __launch_bounds__(128) k_moments_colsum(const FrameDev *__restri
 
 bool moments_row_path(int nframes) { return nframes <= kRowPathFrames; }
 
+// The dynamic shared-memory opt-in of a kernel holds for the device that was
+// current when it was set: it is set once per device and instantiation
+// (std::call_once, so that host threads building at the same time wait for
+// it rather than race).
+template <class M>
+static void configure_bands() {
+  constexpr int kMaxDevices = 64;
+  static std::once_flag once[kMaxDevices];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  auto set = [] {
+    cudaFuncSetAttribute(k_moments_band_totals<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes<M>());
+    cudaFuncSetAttribute(k_moments_band_sweep<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes<M>());
+  };
+  if (dev >= 0 && dev < kMaxDevices)
+    std::call_once(once[dev], set);
+  else
+    set();
+}
+
 template <class M>
 static void launch_bands(const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas, int max_bands,
                          const int *frame_of_band, const int *frame_of_carry, cudaStream_t s, Profiler *prof) {
-  static bool configured = false;  // one attribute call per instantiation
-  if (!configured) {
-    cudaFuncSetAttribute(k_moments_band_totals<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes<M>());
-    cudaFuncSetAttribute(k_moments_band_sweep<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes<M>());
-    configured = true;
-  }
+  configure_bands<M>();
   prof->begin(NICP_K_MOMENTS_BANDS, s);
   k_moments_band_totals<M><<<total_bands, kRowThreads, band_smem_bytes<M>(), s>>>(d_frames, frame_of_band);
   k_moments_band_carry<M><<<total_carry_ctas, 128, 0, s>>>(d_frames, frame_of_carry);
