@@ -49,7 +49,10 @@
  *     before the build kernels that read them.
  *   - There is no CPU fallback: creating a context fails on a host without
  *     an sm_100 GPU.
- *   - A context is not thread-safe: use one per host thread.
+ *   - A context is not thread-safe: use one per host thread.  Calls run on
+ *     the calling thread's current device, which nicp_ctx_create sets to the
+ *     context's: use each context from a thread whose current device is
+ *     its own.
  */
 #ifndef NICP_GPU_H
 #define NICP_GPU_H
