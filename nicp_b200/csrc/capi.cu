@@ -2016,6 +2016,13 @@ extern "C" int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *r
 namespace nicp {
 namespace internal {
 
+// Makes the context's device current on the calling thread: a thread that
+// did not create the context starts on device 0.
+int ctx_make_current(nicp_ctx *ctx) {
+  if (!ctx) return NICP_EINVAL;
+  return cudaSetDevice(ctx->device) == cudaSuccess ? NICP_OK : NICP_ECUDA;
+}
+
 // Batch build into clouds that may belong to another context of this device.
 int build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *rows, const int *cols,
                 const nicp_camera *cams, const nicp_cloud_params *prm, nicp_cloud *const *out) {

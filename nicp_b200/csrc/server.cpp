@@ -37,6 +37,7 @@ int align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs, const nicp_
                 const nicp_lin_params *lin, const nicp_align_params *prm, nicp_align_result *out);
 int cloud_normal_counts(nicp_ctx *ctx, int n, const nicp_cloud *const *c, int *out);
 size_t cloud_bytes(const nicp_cloud *c);
+int ctx_make_current(nicp_ctx *ctx);
 }  // namespace internal
 }  // namespace nicp
 
@@ -114,6 +115,10 @@ struct nicp_server {
 
 void nicp_server::worker(int w) {
   nicp_ctx *ctx = ctxs[w];
+  // the contexts were created on the submitting thread; this thread starts
+  // on device 0 unless told otherwise (a failure here surfaces as an error
+  // of the first request's calls)
+  nicp::internal::ctx_make_current(ctx);
   for (;;) {
     std::vector<Request> batch;
     std::vector<nicp_cloud *> cur_clouds;
