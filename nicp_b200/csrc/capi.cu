@@ -328,13 +328,13 @@ extern "C" int nicp_ctx_destroy(nicp_ctx *ctx) {
   if (!ctx) return NICP_EINVAL;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // staging copies write into ws
   if (ctx->scratch_cloud) nicp_cloud_destroy(ctx->scratch_cloud);
   for (auto &g : ctx->graphs) cudaGraphExecDestroy(g.exec);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->pin_up) cudaFreeHost(ctx->pin_up);
   if (ctx->pin_down) cudaFreeHost(ctx->pin_down);
   cudaEventDestroy(ctx->pin_up_ev);
-  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   for (cudaEvent_t e : ctx->copy_ev) cudaEventDestroy(e);
   if (ctx->copy_start) cudaEventDestroy(ctx->copy_start);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
