@@ -535,10 +535,15 @@ template <class S> struct Integral {
   }
 };
 
+// imageutils.cpp:85-99: dest = scale * src for non-zero pixels, computed in
+// float: the converter's input is the float DepthImage this conversion writes
+// (cv::Mat_<float>), so both modes start from the same float depths and F64
+// promotes them exactly.  (Converting in double instead moves the FP64 pose by
+// as much as a one-ulp perturbation of the float depths does; that is a
+// different input, not a more precise evaluation of this one.)
 template <class S> static inline S cast_depth(float scale, uint16_t u) {
-  // imageutils.cpp:85-99: dest = scale * src for non-zero pixels.
   if (!u) return S(0);
-  return S(scale) * S((int)u);
+  return S(scale * (float)u);
 }
 
 // Cloud::transformInPlace (cloud.cpp:191-204), with the Gaussians moved as
@@ -979,9 +984,12 @@ static bool inverse6(const double *A, double *out) {
   return true;
 }
 
-static void solution_statistics(const double H36[36], const M4<double> &T, double *tr, double *rr) {
+static void solution_statistics(const double H36[36], const M4<double> &T, double *tr, double *rr,
+                                double *omega36, double *mean6) {
   *tr = std::numeric_limits<double>::max();
   *rr = std::numeric_limits<double>::max();
+  for (int i = 0; i < 36; i++) omega36[i] = 0;
+  for (int i = 0; i < 6; i++) mean6[i] = 0;
   double A[36], V[36], w[6];
   for (int i = 0; i < 36; i++) A[i] = H36[i];
   for (int i = 0; i < 6; i++)
@@ -1035,10 +1043,12 @@ static void solution_statistics(const double H36[36], const M4<double> &T, doubl
   for (int k = 0; k < np; k++)
     for (int r = 0; r < 6; r++)
       for (int c = 0; c < 6; c++) cov[r * 6 + c] += wcov[k] * (samp[k][r] - mean[r]) * (samp[k][c] - mean[c]);
+  for (int i = 0; i < 6; i++) mean6[i] = mean[i];
   double Om[36];
   if (!inverse6(cov, Om)) return;
   for (int i = 0; i < 6; i++)
     for (int j = 0; j < 6; j++) A[i * 6 + j] = 0.5 * (Om[i * 6 + j] + Om[j * 6 + i]);
+  for (int i = 0; i < 36; i++) omega36[i] = A[i];
   for (int blk = 0; blk < 2; blk++) {
     double B6[6] = {A[(3 * blk) * 6 + 3 * blk], A[(3 * blk) * 6 + 3 * blk + 1], A[(3 * blk) * 6 + 3 * blk + 2],
                     A[(3 * blk + 1) * 6 + 3 * blk + 1], A[(3 * blk + 1) * 6 + 3 * blk + 2],
@@ -1068,9 +1078,10 @@ static void align(const Cloud<S> &ref, const Cloud<S> &cur, const orc_camera &ca
   project(cur, Pc, ci.data(), cd.data());
   M4<S> T = G;
   double H[36], b[6], err = 0;
-  int inl = 0, K = 0;
+  int inl = 0, K = 0, run = 0;
   for (int i = 0; i < prm.outer_iterations; i++) {
     set_row3(T);
+    const M4<S> Tstart = T;
     Projector<S> Pr = make_projector<S>(cam, mm(T, RO));
     project(ref, Pr, ri.data(), rd.data());
     K = correspond(ref, cur, ri.data(), ci.data(), Pr.rows, Pr.cols, iso_inverse(T), prm, pairs.data(), f64mode);
@@ -1089,13 +1100,24 @@ static void align(const Cloud<S> &ref, const Cloud<S> &cur, const orc_camera &ca
     t2v(T, x);
     T = v2t(x);
     set_row3(T);
+    run++;
+    if (prm.early_exit_eps > 0) {  // new (the reference always runs every iteration)
+      S dv[6];
+      t2v(mm(T, iso_inverse(Tstart)), dv);
+      double m = 0;
+      for (int k = 0; k < 6; k++) m = std::max(m, std::fabs((double)dv[k]));
+      if (m < prm.early_exit_eps) break;
+    }
   }
   for (int i = 0; i < 16; i++) out->T[i] = (double)T.a[i];
   out->error = err;
   out->inliers = inl;
   out->num_correspondences = K;
+  out->outer_iterations_run = run;
   out->translational_ratio = out->rotational_ratio = 0;
   out->solution_valid = 0;
+  for (int i = 0; i < 36; i++) out->omega[i] = 0;
+  for (int i = 0; i < 6; i++) out->mean[i] = 0;
   if (stats) {
     M4<S> invT = iso_inverse(T);
     set_row3(invT);
@@ -1104,7 +1126,7 @@ static void align(const Cloud<S> &ref, const Cloud<S> &cur, const orc_camera &ca
     linearize(ref, cur, pairs.data(), K, invT, prm, f64mode, Hs, bs, &e2, &i2);
     M4<double> Td;
     for (int i = 0; i < 16; i++) Td.a[i] = (double)T.a[i];
-    solution_statistics(Hs, Td, &out->translational_ratio, &out->rotational_ratio);
+    solution_statistics(Hs, Td, &out->translational_ratio, &out->rotational_ratio, out->omega, out->mean);
     out->solution_valid = !(out->rotational_ratio > prm.rotational_min_eigen_ratio ||
                             out->translational_ratio > prm.translational_min_eigen_ratio);
   }
@@ -1190,9 +1212,10 @@ static void align_nn(const Cloud<S> &ref, const Cloud<S> &cur, const double *gue
   M4<S> T = guess ? load_T<S>(guess) : M4<S>::identity();
   std::vector<int32_t> pairs(2 * (size_t)std::max(ref.n, 1));
   double H[36], b[6], err = 0;
-  int inl = 0, K = 0;
+  int inl = 0, K = 0, run = 0;
   for (int i = 0; i < prm.outer_iterations; i++) {
     set_row3(T);
+    const M4<S> Tstart = T;
     K = correspond_nn(ref, cur, iso_inverse(T), nscale, prm, pairs.data());
     M4<S> invT = iso_inverse(T);
     for (int k = 0; k < prm.inner_iterations; k++) {
@@ -1209,13 +1232,24 @@ static void align_nn(const Cloud<S> &ref, const Cloud<S> &cur, const double *gue
     t2v(T, x);
     T = v2t(x);
     set_row3(T);
+    run++;
+    if (prm.early_exit_eps > 0) {  // new (the reference always runs every iteration)
+      S dv[6];
+      t2v(mm(T, iso_inverse(Tstart)), dv);
+      double m = 0;
+      for (int k = 0; k < 6; k++) m = std::max(m, std::fabs((double)dv[k]));
+      if (m < prm.early_exit_eps) break;
+    }
   }
   for (int i = 0; i < 16; i++) out->T[i] = (double)T.a[i];
   out->error = err;
   out->inliers = inl;
   out->num_correspondences = K;
+  out->outer_iterations_run = run;
   out->translational_ratio = out->rotational_ratio = 0;
   out->solution_valid = 0;
+  for (int i = 0; i < 36; i++) out->omega[i] = 0;
+  for (int i = 0; i < 6; i++) out->mean[i] = 0;
   if (stats) {
     M4<S> invT = iso_inverse(T);
     set_row3(invT);
@@ -1224,7 +1258,7 @@ static void align_nn(const Cloud<S> &ref, const Cloud<S> &cur, const double *gue
     linearize(ref, cur, pairs.data(), K, invT, prm, f64mode, Hs, bs, &e2, &i2);
     M4<double> Td;
     for (int i = 0; i < 16; i++) Td.a[i] = (double)T.a[i];
-    solution_statistics(Hs, Td, &out->translational_ratio, &out->rotational_ratio);
+    solution_statistics(Hs, Td, &out->translational_ratio, &out->rotational_ratio, out->omega, out->mean);
     out->solution_valid = !(out->rotational_ratio > prm.rotational_min_eigen_ratio ||
                             out->translational_ratio > prm.translational_min_eigen_ratio);
   }

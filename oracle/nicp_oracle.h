@@ -71,6 +71,8 @@ typedef struct {
   float lambda;
   float translational_min_eigen_ratio, rotational_min_eigen_ratio;
   int threads;               /* emulated omp_get_max_threads() */
+  double early_exit_eps;     /* stop once an outer iteration moves the pose by less
+                                (max |t2v(T T_start^-1)|); 0 = the reference's fixed count */
 } orc_align_params;
 
 typedef struct orc_cloud orc_cloud;
@@ -141,6 +143,9 @@ typedef struct {
   int num_correspondences;   /* of the last outer iteration */
   double translational_ratio, rotational_ratio;
   int solution_valid;
+  int outer_iterations_run;
+  double omega[36];          /* Aligner::omega() (aligner.cpp:124-126), row-major */
+  double mean[6];            /* Aligner::_mean: the reconstructed Gaussian's mean */
 } orc_align_result;
 
 /* CorrespondenceFinderNN::compute (correspondencefindernn.cpp:44-97) with an

@@ -42,13 +42,14 @@ class AlignParams(C.Structure):
                 ("z_scaling", C.c_int), ("lin_scale", C.c_float), ("lin_demoted_to_gicp", C.c_int),
                 ("outer_iterations", C.c_int), ("inner_iterations", C.c_int), ("lambda_", C.c_float),
                 ("translational_min_eigen_ratio", C.c_float), ("rotational_min_eigen_ratio", C.c_float),
-                ("threads", C.c_int)]
+                ("threads", C.c_int), ("early_exit_eps", C.c_double)]
 
 
 class AlignResult(C.Structure):
     _fields_ = [("T", C.c_double * 16), ("error", C.c_double), ("inliers", C.c_int),
                 ("num_correspondences", C.c_int), ("translational_ratio", C.c_double),
-                ("rotational_ratio", C.c_double), ("solution_valid", C.c_int)]
+                ("rotational_ratio", C.c_double), ("solution_valid", C.c_int), ("outer_iterations_run", C.c_int),
+                ("omega", C.c_double * 36), ("mean", C.c_double * 6)]
 
 
 _lib = None
@@ -156,6 +157,7 @@ def align_params(**kw):
     p.lambda_ = 1e3
     p.translational_min_eigen_ratio = p.rotational_min_eigen_ratio = 50.0
     p.threads = 1
+    p.early_exit_eps = 0.0
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -329,7 +331,9 @@ def align(mode, ref, cur, cam, guess=None, ref_offset=None, cur_offset=None, prm
                      1 if statistics else 0, C.byref(r))
     return dict(T=np.array(r.T).reshape(4, 4), error=r.error, inliers=r.inliers,
                 num_correspondences=r.num_correspondences, translational_ratio=r.translational_ratio,
-                rotational_ratio=r.rotational_ratio, solution_valid=r.solution_valid)
+                rotational_ratio=r.rotational_ratio, solution_valid=r.solution_valid,
+                outer_iterations_run=r.outer_iterations_run, omega=np.array(r.omega).reshape(6, 6),
+                mean=np.array(r.mean))
 
 
 def eig3(mode, A6):

@@ -83,7 +83,8 @@ def radius_image(depth_u16, cam, dtype, world_radius=0.1, depth_scale=0.001):
     float32 (the reference and the CUDA path) or float64 (the FP64 oracle)."""
     t = np.dtype(dtype).type
     u = depth_u16.astype(np.int64)
-    d = t(np.float32(depth_scale)) * u.astype(dtype)
+    # both start from the float DepthImage (imageutils.cpp:85-99); FP64 promotes it
+    d = (np.float32(depth_scale) * u.astype(np.float32)).astype(dtype)
     d = np.where(u == 0, t(0), d)
     R = t(np.float32(world_radius))
     with np.errstate(divide="ignore", invalid="ignore"):

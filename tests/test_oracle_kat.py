@@ -119,7 +119,7 @@ def test_unprojection_analytic():
     cl, idx = O.build_cloud(O.F64, d, oc)
     assert idx[5, 7] == -1 and idx[0, 0] == 0 and idx[5, 8] == 5 * cam["cols"] + 7
     P = cl.get("points")
-    z = np.float64(np.float32(0.001)) * 2000
+    z = np.float64(np.float32(0.001) * np.float32(2000))  # the float DepthImage, promoted
     r, c = 10, 20
     k = idx[r, c]
     assert np.allclose(P[k, :3], [(c - cam["cx"]) / cam["fx"] * z, (r - cam["cy"]) / cam["fy"] * z, z], atol=1e-12)
@@ -142,7 +142,7 @@ def test_stats_match_brute_force_windows():
         k = idx[r, c]
         if k < 0:
             continue
-        z = np.float64(np.float32(0.001)) * int(d1[r, c])
+        z = np.float64(np.float32(0.001) * np.float32(int(d1[r, c])))  # the float DepthImage, promoted
         R = np.float64(np.float32(0.1))
         rad = int(max(cam["fx"] * R * (1 / z), cam["fy"] * R * (1 / z)))
         if rad < 10:
@@ -279,7 +279,7 @@ def test_unprojection_gaussian_analytic():
     cl, idx = O.build_cloud(O.F64, d, oc)
     cov = cl.get("gaussian_cov").reshape(-1, 3, 3)
     mean = cl.get("gaussian_mean").reshape(-1, 3)
-    z = np.float64(np.float32(0.001)) * 2500
+    z = np.float64(np.float32(0.001) * np.float32(2500))  # the float DepthImage, promoted
     f, B, a = cam["fx"], 0.075, np.float64(np.float32(0.1))
     for r, c in [(0, 0), (37, 101), (119, 159)]:
         k = idx[r, c]
