@@ -49,10 +49,18 @@
  *     before the build kernels that read them.
  *   - There is no CPU fallback: creating a context fails on a host without
  *     an sm_100 GPU.
- *   - A context is not thread-safe: use one per host thread.  Calls run on
- *     the calling thread's current device, which nicp_ctx_create sets to the
- *     context's: use each context from a thread whose current device is
- *     its own.
+ *   - A context is not thread-safe: use one per host thread.  Every call
+ *     that takes a context (or a cloud of one) runs on the context's device
+ *     whatever device the calling thread has current, and leaves the
+ *     thread's current device as it found it (nicp_ctx_create and
+ *     nicp_ctx_destroy included), so one thread may drive contexts on
+ *     several GPUs.  The one exception is nicp_linearize_noalloc, which
+ *     switches nothing and refuses a call whose context's device is not
+ *     current (NICP_ESTATE).
+ *   - The library's per-device state (kernel attributes set once per
+ *     device, the allocation-free linearizer's array address) does not
+ *     survive cudaDeviceReset: destroy every context and server first, and
+ *     do not use the library on a device after resetting it.
  */
 #ifndef NICP_GPU_H
 #define NICP_GPU_H

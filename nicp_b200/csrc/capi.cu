@@ -103,6 +103,41 @@ static int fail(nicp_ctx *ctx, int code, const std::string &msg) {
   return code;
 }
 
+// Every call on a context runs on the context's device, whatever device the
+// calling thread has current, and gives the thread its previous device back
+// on return: workspaces, clouds and kernels of a context never land on
+// another GPU, and a thread that drives contexts on several GPUs needs no
+// cudaSetDevice of its own.
+class DeviceScope {
+ public:
+  explicit DeviceScope(const nicp_ctx *ctx) {
+    if (!ctx) return;
+    if (cudaGetDevice(&prev_) != cudaSuccess) {
+      cudaGetLastError();
+      prev_ = -1;
+    }
+    if (prev_ != ctx->device) {
+      ok_ = cudaSetDevice(ctx->device) == cudaSuccess;
+      if (!ok_) cudaGetLastError();
+      switched_ = ok_ && prev_ >= 0;
+    }
+  }
+  ~DeviceScope() {
+    if (switched_) cudaSetDevice(prev_);
+  }
+  DeviceScope(const DeviceScope &) = delete;
+  DeviceScope &operator=(const DeviceScope &) = delete;
+  bool ok() const { return ok_; }
+
+ private:
+  int prev_ = -1;
+  bool switched_ = false, ok_ = true;
+};
+
+#define NICP_ON_DEVICE(ctx_expr)             \
+  DeviceScope device_scope_(ctx_expr);        \
+  if (!device_scope_.ok()) return NICP_ECUDA
+
 #define CK(ctx, call)                                                                          \
   do {                                                                                         \
     cudaError_t e_ = (call);                                                                   \
@@ -300,9 +335,14 @@ extern "C" int nicp_ctx_create(int device, void *stream, nicp_ctx **out) {
   if (device < 0 || device >= n) return NICP_EINVAL;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) return NICP_ECUDA;
-  if (cudaSetDevice(device) != cudaSuccess) return NICP_ECUDA;
   auto *ctx = new nicp_ctx();
   ctx->device = device;
+  // the stream and event belong to `device`; the caller's device is current again on return
+  DeviceScope on_device(ctx);
+  if (!on_device.ok()) {
+    delete ctx;
+    return NICP_ECUDA;
+  }
   ctx->sm_count = prop.multiProcessorCount > 0 ? prop.multiProcessorCount : 148;
   if (stream) {
     ctx->stream = (cudaStream_t)stream;
@@ -325,8 +365,8 @@ extern "C" int nicp_ctx_create(int device, void *stream, nicp_ctx **out) {
 
 extern "C" int nicp_ctx_destroy(nicp_ctx *ctx) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx) return NICP_EINVAL;
-  cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // staging copies write into ws
   if (ctx->scratch_cloud) nicp_cloud_destroy(ctx->scratch_cloud);
@@ -348,6 +388,7 @@ extern "C" const char *nicp_ctx_last_error(const nicp_ctx *ctx) { return ctx ? c
 
 extern "C" int nicp_ctx_synchronize(nicp_ctx *ctx) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx) return NICP_EINVAL;
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return NICP_OK;
@@ -360,6 +401,7 @@ extern "C" size_t nicp_ctx_device_bytes(const nicp_ctx *ctx) { return ctx ? ctx-
 
 extern "C" int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx) return NICP_EINVAL;
   ctx->prof.enabled = enable != 0;
   ctx->prof.recs.clear();
@@ -370,6 +412,7 @@ extern "C" int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable) {
 
 extern "C" int nicp_ctx_set_autotune(nicp_ctx *ctx, int enable) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx) return NICP_EINVAL;
   ctx->autotune = enable != 0;
   return NICP_OK;
@@ -379,6 +422,7 @@ extern "C" int nicp_ctx_set_autotune(nicp_ctx *ctx, int enable) {
 extern "C" int nicp_ctx_launch_shape(const nicp_ctx *ctx, int *zbuffer_points_per_thread, int *corr_ctas_per_sm,
                                      int *tuned_mixes) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx) return NICP_EINVAL;
   if (zbuffer_points_per_thread) *zbuffer_points_per_thread = ctx->launch.zb_ppt;
   if (corr_ctas_per_sm) *corr_ctas_per_sm = ctx->launch.corr_ctas;
@@ -389,6 +433,7 @@ extern "C" int nicp_ctx_launch_shape(const nicp_ctx *ctx, int *zbuffer_points_pe
 
 extern "C" int nicp_ctx_read_profile(nicp_ctx *ctx, int kernel, double *total_ms, int *launches) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || kernel < 0 || kernel >= NICP_K_COUNT) return NICP_EINVAL;
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   double t = 0;
@@ -416,6 +461,7 @@ extern "C" unsigned long long nicp_ctx_kernel_launches(const nicp_ctx *ctx) { re
 
 extern "C" int nicp_ctx_transfer_bytes(const nicp_ctx *ctx, unsigned long long *h2d, unsigned long long *d2h) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx) return NICP_EINVAL;
   if (h2d) *h2d = ctx->h2d_bytes;
   if (d2h) *d2h = ctx->d2h_bytes;
@@ -433,6 +479,7 @@ extern "C" const char *nicp_kernel_name(int k) {
 // ------------------------------------------------------------------ clouds
 extern "C" int nicp_cloud_create(nicp_ctx *ctx, nicp_cloud **out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !out) return NICP_EINVAL;
   auto *c = new nicp_cloud();
   c->ctx = ctx;
@@ -443,6 +490,7 @@ extern "C" int nicp_cloud_create(nicp_ctx *ctx, nicp_cloud **out) {
 
 extern "C" int nicp_cloud_destroy(nicp_cloud *c) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(c ? c->ctx : nullptr);
   if (!c) return NICP_EINVAL;
   if (c->mem) {
     cudaStreamSynchronize(c->ctx->stream);
@@ -456,6 +504,7 @@ extern "C" int nicp_cloud_destroy(nicp_cloud *c) {
 
 extern "C" int nicp_cloud_size(nicp_cloud *c, int *n) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(c ? c->ctx : nullptr);
   if (!c || !n) return NICP_EINVAL;
   if (!c->mem) { *n = 0; return NICP_OK; }
   nicp_ctx *ctx = c->ctx;
@@ -468,6 +517,7 @@ extern "C" int nicp_cloud_size(nicp_cloud *c, int *n) {
 extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *curv, float *op9, float *on9, float *ev3,
                                    float *U9) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(c ? c->ctx : nullptr);
   if (!c) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int n = 0;
@@ -508,6 +558,7 @@ extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *c
 
 extern "C" int nicp_cloud_download_stats(nicp_cloud *c, float *eigval3, float *eigvec9, float *mean3, int *n_out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(c ? c->ctx : nullptr);
   if (!c) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int n = 0;
@@ -531,6 +582,7 @@ extern "C" int nicp_cloud_download_stats(nicp_cloud *c, float *eigval3, float *e
 
 extern "C" int nicp_cloud_download_gaussians(nicp_cloud *c, float *mean3, float *cov9) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(c ? c->ctx : nullptr);
   if (!c) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int n = 0;
@@ -553,6 +605,7 @@ extern "C" int nicp_cloud_download_gaussians(nicp_cloud *c, float *mean3, float 
 extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const float *n4, const float *curv,
                                  const float *op9, const float *on9) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(c ? c->ctx : nullptr);
   if (!c || n < 0 || (n > 0 && (!p4 || !n4 || !curv))) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   int rc = cloud_reserve(c, n, c->rows, c->cols, false);
@@ -584,6 +637,7 @@ extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const fl
 
 extern "C" int nicp_cloud_transform(nicp_cloud *c, const float T16[16]) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(c ? c->ctx : nullptr);
   if (!c || !T16) return NICP_EINVAL;
   nicp_ctx *ctx = c->ctx;
   if (!c->mem) return NICP_OK;
@@ -902,6 +956,7 @@ extern "C" int nicp_cloud_from_depth_u16(nicp_ctx *ctx, const uint16_t *depth, i
                                          int on_device, const nicp_camera *cam, const nicp_cloud_params *prm,
                                          const float *offset, nicp_cloud *out, int32_t *index_out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   return build_one(ctx, depth, true, rows, cols, pitch, on_device, cam, prm, offset, out, index_out);
   NICP_ABI_CATCH
 }
@@ -910,6 +965,7 @@ extern "C" int nicp_cloud_from_depth_f32(nicp_ctx *ctx, const float *depth, int 
                                          int on_device, const nicp_camera *cam, const nicp_cloud_params *prm,
                                          const float *offset, nicp_cloud *out, int32_t *index_out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   return build_one(ctx, depth, false, rows, cols, pitch, on_device, cam, prm, offset, out, index_out);
   NICP_ABI_CATCH
 }
@@ -918,6 +974,7 @@ extern "C" int nicp_build_batch(nicp_ctx *ctx, int n, const uint16_t *const *dep
                                 int on_device, const nicp_camera *cams, const nicp_cloud_params *prm,
                                 nicp_cloud *const *out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || n < 0 || (n > 0 && (!depth || !rows || !cols || !cams || !prm || !out))) return NICP_EINVAL;
   std::vector<FrameIn> f(n);
   for (int i = 0; i < n; i++) {
@@ -943,6 +1000,7 @@ extern "C" int nicp_projector_matrices(const nicp_camera *cam, const float T16[1
 extern "C" int nicp_unproject(nicp_ctx *ctx, const float *depth, int rows, int cols, const nicp_camera *cam,
                               const float T16[16], float *points4_out, int32_t *index_out, int *n) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !depth || !cam || !n) return NICP_EINVAL;
   int rc;
   if (!ctx->scratch_cloud && (rc = nicp_cloud_create(ctx, &ctx->scratch_cloud))) return rc;
@@ -964,6 +1022,7 @@ extern "C" int nicp_unproject(nicp_ctx *ctx, const float *depth, int rows, int c
 extern "C" int nicp_project_intervals(nicp_ctx *ctx, const float *depth, int rows, int cols, const nicp_camera *cam,
                                       float world_radius, int32_t *radius_out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !depth || !cam || !radius_out || rows <= 0 || cols <= 0) return NICP_EINVAL;
   size_t P = (size_t)rows * cols;
   Layout L;
@@ -1092,6 +1151,7 @@ extern "C" int nicp_correspond(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_
                                const int32_t *cur_index, int rows, int cols, const float T16[16],
                                const nicp_corr_params *prm, int32_t *pairs_out, int *num_out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !ref || !cur || !ref_index || !cur_index || rows <= 0 || cols <= 0 || !T16 || !prm || !num_out)
     return NICP_EINVAL;
   nicp_camera cam;
@@ -1131,6 +1191,7 @@ extern "C" int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_c
                               int num_pairs, const float T16[16], const nicp_lin_params *prm, int parity_threads,
                               double H36[36], double b6[6], double *error, int *inliers) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !ref || !cur || (num_pairs > 0 && !pairs) || num_pairs < 0 || !T16 || !prm) return NICP_EINVAL;
   // list slots are tiled like pixels: a one-row image of num_pairs pixels
   nicp_camera cam;
@@ -1207,6 +1268,7 @@ extern "C" int nicp_linearize_noalloc(nicp_ctx *ctx, const nicp_cloud *ref, cons
 extern "C" int nicp_project(nicp_ctx *ctx, const nicp_cloud *cloud, const nicp_camera *cam, const float T16[16],
                             int32_t *index_out, float *depth_out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !cloud || !cam || !valid_camera(cam)) return NICP_EINVAL;
   PairPlan pl;
   int rc;
@@ -1242,6 +1304,7 @@ extern "C" int nicp_depth_scale(nicp_ctx *ctx, const void *depth, int is_u16, in
                                 int on_device, float depth_scale, int step, float max_depth_cov, float *out,
                                 int out_on_device) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !depth || !out || rows <= 0 || cols <= 0 || step < 1) return NICP_EINVAL;
   const size_t elem = is_u16 ? 2 : 4;
   if (pitch_bytes == 0) pitch_bytes = elem * (size_t)cols;
@@ -1400,6 +1463,7 @@ extern "C" int nicp_correspond_nn(nicp_ctx *ctx, const nicp_cloud *ref, const ni
                                   float normal_scaling, const nicp_corr_params *corr, int32_t *pairs_out,
                                   int *num_pairs) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !ref || !cur || !T16 || !corr || !num_pairs) return NICP_EINVAL;
   NNPlan pl;
   int rc = nn_plan(ctx, ref, cur, corr->inlier_distance_threshold, pl);
@@ -1431,6 +1495,7 @@ extern "C" int nicp_align_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cl
                              float normal_scaling, const nicp_corr_params *corr, const nicp_lin_params *lin,
                              const nicp_align_params *prm, nicp_align_result *out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !ref || !cur || !corr || !lin || !prm || !out) return NICP_EINVAL;
   if (prm->outer_iterations < 0 || prm->inner_iterations < 1 || prm->outer_iterations > 1000 ||
       prm->inner_iterations > 100)
@@ -1566,6 +1631,7 @@ static int cloud_counts2(nicp_cloud *c, int out[2]) {
 
 extern "C" int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[16]) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(dst ? dst->ctx : nullptr);
   if (!dst || !src || dst == src || dst->ctx != src->ctx) return NICP_EINVAL;
   nicp_ctx *ctx = dst->ctx;
   int rc = T16 ? nicp_cloud_transform(src, T16) : NICP_OK;  // Cloud::add moves the added cloud itself
@@ -1614,6 +1680,7 @@ extern "C" int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[
 extern "C" int nicp_merge(nicp_ctx *ctx, nicp_cloud *cloud, const nicp_camera *cam, const float T16[16],
                           float distance_threshold, float max_point_depth, int *removed) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   if (!ctx || !cloud || !cam || !valid_camera(cam) || cloud->ctx != ctx) return NICP_EINVAL;
   if (removed) *removed = 0;
   int cnt[2];
@@ -1996,6 +2063,7 @@ extern "C" int nicp_align(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cloud
                           const nicp_corr_params *corr, const nicp_lin_params *lin, const nicp_align_params *prm,
                           nicp_align_result *out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   // replayed from a cached CUDA graph like a batch: the pair descriptors are
   // uploaded per call, so one graph serves every pair of the same shape
   AlignCall a{1, &ref, &cur, cam, guess16, ref_offset16, cur_offset16, corr, lin, prm, true};
@@ -2007,6 +2075,7 @@ extern "C" int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *r
                                 const nicp_camera *cams, const float *guesses, const nicp_corr_params *corr,
                                 const nicp_lin_params *lin, const nicp_align_params *prm, nicp_align_result *out) {
   NICP_ABI_TRY
+  NICP_ON_DEVICE(ctx);
   AlignCall a{n, refs, curs, cams, guesses, nullptr, nullptr, corr, lin, prm, true};
   return align_impl(ctx, a, out);
   NICP_ABI_CATCH
@@ -2027,6 +2096,7 @@ int ctx_make_current(nicp_ctx *ctx) {
 int build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *rows, const int *cols,
                 const nicp_camera *cams, const nicp_cloud_params *prm, nicp_cloud *const *out) {
   if (!ctx || n < 0) return NICP_EINVAL;
+  NICP_ON_DEVICE(ctx);
   std::vector<FrameIn> f(n);
   for (int i = 0; i < n; i++) f[i] = FrameIn{depth[i], true, false, 0, rows[i], cols[i], nullptr};
   return build_frames(ctx, n, f.data(), cams, prm, out, false);
@@ -2036,12 +2106,14 @@ int build_batch(nicp_ctx *ctx, int n, const uint16_t *const *depth, const int *r
 int align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs, const nicp_cloud *const *curs,
                 const nicp_camera *cams, const float *guesses, const nicp_corr_params *corr,
                 const nicp_lin_params *lin, const nicp_align_params *prm, nicp_align_result *out) {
+  NICP_ON_DEVICE(ctx);
   AlignCall a{n, refs, curs, cams, guesses, nullptr, nullptr, corr, lin, prm, false, true};
   return align_impl(ctx, a, out);
 }
 
 // Counts of points with a normal of n clouds, with one synchronisation.
 int cloud_normal_counts(nicp_ctx *ctx, int n, const nicp_cloud *const *c, int *out) {
+  NICP_ON_DEVICE(ctx);
   char *pin;
   int rc = pin_down(ctx, sizeof(int) * (size_t)std::max(n, 1), &pin);
   if (rc) return rc;
@@ -2064,6 +2136,7 @@ int cloud_host_arrays(nicp_cloud *c, std::vector<float> &pts4, std::vector<float
   int rc = nicp_cloud_size(c, &n);
   if (rc) return rc;
   nicp_ctx *ctx = c->ctx;
+  NICP_ON_DEVICE(ctx);
   pts4.resize(4 * (size_t)n);
   nrm4.resize(4 * (size_t)n);
   has_stats = c->eig_valid;
@@ -2084,6 +2157,7 @@ int cloud_host_arrays(nicp_cloud *c, std::vector<float> &pts4, std::vector<float
 int cloud_set_host_arrays(nicp_cloud *c, int n, const float *pts4, const float *nrm4, const float *omg12,
                           const float *stats, int normals, bool structured, const float omd[8]) {
   nicp_ctx *ctx = c->ctx;
+  NICP_ON_DEVICE(ctx);
   int rc = cloud_reserve(c, n, c->rows, c->cols, true, false);
   if (rc) return rc;
   if (n > 0) {

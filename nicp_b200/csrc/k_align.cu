@@ -1088,6 +1088,7 @@ static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxTiles * kP
 
 __global__ void __launch_bounds__(kCorrThreads) k_lin_noalloc(NoAllocLinArgs a, double *__restrict__ partials) {
   const int tile = blockIdx.x;
+  if (tile >= kNoAllocMaxTiles) return;  // the host refuses longer lists; never write past the array
   int K = a.num_pairs;
   if (a.parity_threads > 1) K = (K / a.parity_threads) * a.parity_threads;
   const int nref = *a.ref_count, ncur = *a.cur_count;
@@ -1117,7 +1118,8 @@ __global__ void __launch_bounds__(128) k_lin_noalloc_sum(int ntiles, const doubl
   __shared__ double tot[32];
   const int e = threadIdx.x & 31, g = threadIdx.x >> 5;
   double s = 0.0;
-  for (int t = g; t < ntiles; t += 4) s += partials[(size_t)t * kPartialWords + e];
+  const int nt = min(ntiles, kNoAllocMaxTiles);
+  for (int t = g; t < nt; t += 4) s += partials[(size_t)t * kPartialWords + e];
   part[g][e] = s;
   __syncthreads();
   if (threadIdx.x < 32) tot[e] = ((part[0][e] + part[1][e]) + part[2][e]) + part[3][e];

@@ -115,9 +115,10 @@ struct nicp_server {
 
 void nicp_server::worker(int w) {
   nicp_ctx *ctx = ctxs[w];
-  // the contexts were created on the submitting thread; this thread starts
-  // on device 0 unless told otherwise (a failure here surfaces as an error
-  // of the first request's calls)
+  // the contexts were created on the submitting thread; every library call
+  // below makes the context's device current for itself (a device that cannot
+  // be made current fails each request's calls with NICP_ECUDA), so this only
+  // sets the thread's default for anything else it does
   nicp::internal::ctx_make_current(ctx);
   for (;;) {
     std::vector<Request> batch;

@@ -70,8 +70,18 @@ def test_noalloc_rejects_oversized_list(ctx):
     d1, _, _, cam = synth.render_pair(24, "160x120")
     proj, conv = converter(cam, ctx)
     c, _ = gpu_cloud(ctx, conv, d1, keep_index=False)
+    import torch
     lp = api.Linearizer(ctx).params()
     T = np.eye(4, dtype=np.float32)
-    rc = ctx.lib.nicp_linearize_noalloc(ctx.h, c.h, c.h, C.c_void_p(16), L.NICP_LINEARIZE_NOALLOC_MAX_PAIRS + 1,
-                                        L.fptr(T), C.byref(lp), 1, C.c_void_p(16))
+    # real buffers of the oversized length (no fake addresses): should the
+    # host's size check ever regress, the kernels read valid (empty) pairs
+    # and their own tile bound keeps them inside the partial-sum array, so
+    # the regression shows up as this assertion, not as a GPU fault
+    n = L.NICP_LINEARIZE_NOALLOC_MAX_PAIRS + 1
+    dev_pairs = torch.full((2 * n,), -1, dtype=torch.int32, device="cuda")
+    out = torch.zeros((44,), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rc = ctx.lib.nicp_linearize_noalloc(ctx.h, c.h, c.h, C.c_void_p(dev_pairs.data_ptr()), n, L.fptr(T), C.byref(lp),
+                                        1, C.c_void_p(out.data_ptr()))
+    ctx.synchronize()
     assert rc == L.NICP_EINVAL
