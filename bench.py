@@ -179,6 +179,25 @@ def run_step(ctx, frames_ptrs, cam_c, prm_c, clouds, corr, lin, prm, on_device):
 #                    information matrices are rebuilt from the current normal
 #                    (structured Omega), not read (the general path adds 48 C)
 #                    (s = 8 bytes per FP64 moment)
+def build_bytes(P, V, s=8):
+    """One frame build: S1 + band totals/carries + sweep + S3 (bytes)."""
+    return (2 * P + 4 * P + 12 * V) + (2 * P + 3 * 10 * s * P / 16) + (2 * P + 10 * s * P / 16 + 10 * s * P) + \
+        (10 * s * P + 6 * P + 76 * V)
+
+
+def align_bytes(P, V, C, outer, inner):
+    """One alignment: the current cloud's projection (z-buffer 12V + 8V) and
+    resolve (z-buffer read 8P, index write 4P, z-buffer reset 8P), then per
+    outer iteration the reference projection (20V) and per inner iteration
+    the fused pass: z-buffer read and reset (16P) + current index (4P) on the
+    first, plus the reference index written (4P) when more follow; later
+    inner iterations read both index images (8P); 56 bytes per accepted
+    correspondence (points, normals, curvatures of both clouds)."""
+    first = 20 * P + (4 * P if inner > 1 else 0) + 56 * C
+    later = (inner - 1) * (8 * P + 56 * C)
+    return 20 * V + 20 * P + outer * (20 * V + first + later)
+
+
 def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     s = 8
     if kernel == "unproject":
@@ -192,7 +211,7 @@ def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     if kernel == "zbuffer":
         return (12 * V + 8 * V) * pairs
     if kernel == "corr_lin":
-        return (8 * P + 56 * C) * pairs
+        return (20 * P + 56 * C) * pairs
     if kernel == "resolve":
         return (8 * P + 4 * P) * pairs
     return 0
@@ -251,6 +270,31 @@ def cpu_baseline(frames, cam, seconds=15.0, threads=None):
     dt = time.perf_counter() - t0
     # the first frame's build is included in dt: amortised over the sample
     return pairs / dt, pairs, dt, threads
+
+
+def oracle_pose_check(cases, threads=None):
+    """The checker: each case (u16 reference frame, u16 current frame,
+    camera dict, GPU pose, outer, inner, early-exit eps) is run through the
+    oracle's FP64 pipeline (the reference algorithm in double, from the same
+    frames) and the GPU pose's distance to it is reported (radians, metres)."""
+    from oracle import oracle as O
+    from nicp_b200 import synth
+    threads = threads or os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    errs = []
+    for d1, d2, cam, T, outer, inner, eps in cases:
+        oc = O.camera(cam["rows"], cam["cols"], cam["fx"], cam["fy"], cam["cx"], cam["cy"],
+                      max_distance=cam.get("max_distance", 6.0))
+        a, _ = O.build_cloud(O.F64, d1, oc)
+        b, _ = O.build_cloud(O.F64, d2, oc)
+        r = O.align(O.F64, a, b, oc, prm=O.align_params(outer_iterations=outer, inner_iterations=inner,
+                                                         early_exit_eps=eps))
+        errs.append(synth.pose_error(np.asarray(T, float).reshape(4, 4), r["T"]))
+    er = np.array([e[0] for e in errs])
+    et = np.array([e[1] for e in errs])
+    return {"pairs": len(errs), "rad_max": float(er.max()), "rad_p99": float(np.percentile(er, 99)),
+            "rad_median": float(np.median(er)), "m_max": float(et.max()), "m_p99": float(np.percentile(et, 99)),
+            "within_1e-5rad_0.05mm": int(np.sum((er <= 1e-5) & (et <= 5e-5)))}
 
 
 def reference_arm(args, rank, world):
@@ -357,6 +401,18 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
     total = sum(v[0] for v in prof.values()) or 1.0
     shares = {k: [round(v[0] / total, 4), v[1]] for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
     iters = [r.outer_iterations_run for r in res]
+    # HBM ceiling of this batch: its algorithmic bytes (two builds and the
+    # alignment of every pair, with the iterations each pair ran) at the
+    # measured copy bandwidth
+    sizes = [c.size() for c in clouds]
+    total_bytes = 0.0
+    for i, (r, pr) in enumerate(zip(res, pairs)):
+        P = pr[3]["rows"] * pr[3]["cols"]
+        total_bytes += build_bytes(P, sizes[2 * i]) + build_bytes(P, sizes[2 * i + 1])
+        total_bytes += align_bytes(P, sizes[2 * i], r.num_correspondences, r.outer_iterations_run, 2)
+    peak, _ = measured_peak_gbs()
+    ceiling = npairs / (total_bytes / (peak * 1e9))
+    checks = [(pairs[i][0], pairs[i][1], pairs[i][3], np.array(res[i].T), 20, 2, 1e-6) for i in range(6)]
     errs = [synth.pose_error(np.array(r.T).reshape(4, 4), p[2]) for r, p in zip(res, pairs)]
     ok = [e for e in errs if e[0] < 0.01 and e[1] < 0.02]
     # equal results with and without early exit, where a pair converged
@@ -385,6 +441,8 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
     return {"workload": "%d independent pairs, resolutions uniform over %s, offsets 0.5-5 deg / 1-8 cm, "
                         "<= 20 outer x 2 inner, early exit at pose change < 1e-6" % (npairs, "/".join(MIXED_CAMS)),
             "pairs_per_s": value, "ms_per_step": ms, "pairs_per_s_no_early_exit": npairs / (ms_fixed / 1e3),
+            "algorithmic_bytes_per_step": total_bytes, "hbm_ceiling_pairs_per_s": ceiling,
+            "frac_of_hbm_ceiling": value / ceiling,
             "plain_pairs_per_s": plain, "batched_over_plain": value / plain,
             "outer_iterations_run": {"mean": float(np.mean(iters)), "max": int(max(iters)), "min": int(min(iters))},
             "max_abs_T_diff_vs_no_early_exit": dT,
@@ -394,7 +452,7 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
             "resolution_counts": {n: names.count(n) for n in MIXED_CAMS},
             "kernel_shares_and_launches": shares, "profiled_step_ms": total,
             "autotuned_launch_shape": {"zbuffer_points_per_thread": shape[0],
-                                       "corr_lin_ctas_per_sm": shape[1] or "all that fit"}}
+                                       "corr_lin_ctas_per_sm": shape[1] or "all that fit"}}, checks
 
 
 # ------------------------------------------------------------------ scene fusion leg
@@ -639,6 +697,8 @@ def main():
                          "has the per-frame motion of the 200-frame workload (small profiling cases)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--oracle-pairs", type=int, default=10,
+                    help="pairs of the timed sequence checked against the FP64 oracle (CPU leg)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-call leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
@@ -763,7 +823,7 @@ def main():
     top_ms, top_n = prof[top]
     launches_per_step = top_n
     per_launch_bytes = {
-        "corr_lin": (8 * P + 56 * C) * npairs,
+        "corr_lin": (20 * P + 56 * C) * npairs,
         "zbuffer": (12 * V + 8 * V) * npairs,
         "stats_omega": (10 * 8 * P + 6 * P + 76 * V) * F,
         "moments_bands": (2 * P + 3 * 80 * P / 16) * F / 2,  # two kernels per stage launch
@@ -805,9 +865,15 @@ def main():
             pl.append(nplain / (time.perf_counter() - t0))
         plain = max(pl)
 
-    mixed = None
+    # whole step: every frame built once, every pair aligned (10 outer x 1 inner)
+    step_bytes = F * build_bytes(P, V) + npairs * align_bytes(P, V, C, 10, 1)
+    whole_step = {"algorithmic_bytes": step_bytes, "gbs": step_bytes / (ms / args.steps / 1e3) / 1e9,
+                  "frac": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak,
+                  "hbm_ceiling_pairs_per_s": npairs / (step_bytes / (peak * 1e9))}
+
+    mixed, mixed_checks = None, []
     if not args.no_mixed and rank == 0:
-        mixed = mixed_batch_leg(ctx, stream, local, args.seed + 17)
+        mixed, mixed_checks = mixed_batch_leg(ctx, stream, local, args.seed + 17)
 
     fusion = None
     if not args.no_fusion and rank == 0:
@@ -821,25 +887,51 @@ def main():
     if not args.no_serve and rank == 0:
         serving = serve_leg(local, [float(r) for r in args.serve_rates.split(",")], args.serve_seconds, args.seed)
 
-    cpu = None
+    cpu, oracle_seq, oracle_mixed = None, None, None
     if not args.no_cpu and rank == 0:
         v, n, dt, threads = cpu_baseline(frames, cam, seconds=args.cpu_seconds)
         cpu = {"value": v, "unit": "pairs/s", "cores": threads, "kind": "port",
                "sample": "%d consecutive 640x480 frame pairs (build + align, oracle REF32, %d threads, %.1f s)"
                          % (n, threads, dt)}
+        # the checker: the first pairs of the timed workload (and a few
+        # mixed-batch pairs) against the oracle's FP64 pipeline
+        seq_cases = [(frames[i], frames[i + 1], cam, np.array(res[i].T), 10, 1, 0.0)
+                     for i in range(min(args.oracle_pairs, npairs))]
+        oracle_seq = oracle_pose_check(seq_cases, threads)
+        oracle_mixed = oracle_pose_check(mixed_checks, threads) if mixed_checks else None
 
     if rank == 0:
+        # the headline figures first (scalars), the bulky per-leg records last
+        rates = (serving or {}).get("rates", [])
+        summary = {
+            "plain_pairs_per_s": plain, "batched_over_plain": (value / world / plain) if plain else None,
+            "pose_err_vs_oracle_rad_max": oracle_seq["rad_max"] if oracle_seq else None,
+            "pose_err_vs_oracle_m_max": oracle_seq["m_max"] if oracle_seq else None,
+            "pose_err_vs_oracle_pairs": oracle_seq["pairs"] if oracle_seq else None,
+            "whole_step_gbs": whole_step["gbs"], "whole_step_frac": whole_step["frac"],
+            "hbm_ceiling_pairs_per_s": whole_step["hbm_ceiling_pairs_per_s"],
+            "mixed_pairs_per_s": mixed["pairs_per_s"] if mixed else None,
+            "mixed_plain_pairs_per_s": mixed["plain_pairs_per_s"] if mixed else None,
+            "mixed_batched_over_plain": mixed["batched_over_plain"] if mixed else None,
+            "mixed_frac_of_hbm_ceiling": mixed["frac_of_hbm_ceiling"] if mixed else None,
+            "mixed_pose_err_vs_oracle_rad_max": oracle_mixed["rad_max"] if oracle_mixed else None,
+        }
+        for r in rates:
+            summary["serve_%d_rps_p50_ms" % r["offered_rps"]] = r["p50_ms"]
+            summary["serve_%d_rps_p99_ms" % r["offered_rps"]] = r["p99_ms"]
+            summary["serve_%d_rps_throughput" % r["offered_rps"]] = r["throughput_rps"]
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(args),
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": (h1 - h0) // args.steps,
                         "d2h_bytes_per_step": (d1 - d0) // args.steps},
-                "gpu_launches": int(launches), "clocks": clk,
-                "plain_pairs_per_s": plain, "batched_over_plain": (value / world / plain) if plain else None,
-                "pose_err_vs_truth_median": {"rad": rot_med, "m": tr_med},
-                "points_per_frame": V, "correspondences_per_pair": C, "mixed_batch": mixed, "scene_fusion": fusion, "nn_align": nn,
-                "serving": serving}
+                "gpu_launches": int(launches), "clocks": clk}
+        line.update(summary)
+        line.update({"pose_err_vs_truth_median": {"rad": rot_med, "m": tr_med},
+                     "pose_err_vs_oracle": {"sequence": oracle_seq, "mixed_batch": oracle_mixed},
+                     "whole_step": whole_step, "points_per_frame": V, "correspondences_per_pair": C,
+                     "mixed_batch": mixed, "scene_fusion": fusion, "nn_align": nn, "serving": serving})
         print(json.dumps(line), flush=True)
     del clouds
     ctx.close()

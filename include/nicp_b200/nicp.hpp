@@ -388,6 +388,11 @@ class CorrespondenceFinderProjective {
   float inlierCurvatureRatioThreshold() const { return p_.inlier_curvature_ratio_threshold; }
   void setDemotedToGICP(bool v) { p_.demoted_to_gicp = v; }
   void setParityThreads(int t) { p_.parity_threads = t; }
+  // correspondencefinderprojective.h:146-150 (0 0: the pixel itself)
+  void setRowSearchRegion(int r) { p_.row_search_region = r; }
+  void setColSearchRegion(int c) { p_.col_search_region = c; }
+  int rowSearchRegion() const { return p_.row_search_region; }
+  int colSearchRegion() const { return p_.col_search_region; }
   void setImageSize(int rows, int cols) { rows_ = rows; cols_ = cols; }
   std::vector<int32_t> &referenceIndexImage() { return ref_index_; }
   std::vector<int32_t> &currentIndexImage() { return cur_index_; }
@@ -507,6 +512,9 @@ class AlignerProjective {
   bool solutionValid() const { return res_.solution_valid == 1; }
   float translationalEigenRatio() const { return (float)res_.translational_ratio; }
   float rotationalEigenRatio() const { return (float)res_.rotational_ratio; }
+  // Aligner::omega() (aligner.h:325): 6x6 row-major, (t, quaternion-vector)
+  const double *omega() const { return res_.omega; }
+  const double *mean() const { return res_.mean; }
   const nicp_align_result &result() const { return res_; }
 
  private:

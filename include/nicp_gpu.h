@@ -72,7 +72,7 @@
 extern "C" {
 #endif
 
-#define NICP_API_VERSION 1
+#define NICP_API_VERSION 2
 
 enum {
   NICP_OK = 0,
@@ -133,6 +133,13 @@ typedef struct {
    * the last rows % T image rows and the last K % T correspondences are
    * skipped exactly as the reference skips them.  1 (default) = no drops. */
   int parity_threads;
+  /* CorrespondenceFinderProjective::setRowSearchRegion / setColSearchRegion
+   * (correspondencefinderprojective.h:146-150).  0 0 (default): the pixel's
+   * own current point (_computeSingle); otherwise every reference pixel
+   * takes the best current point of the (2 rows + 1) x (2 cols + 1) window
+   * around it (_computeMulti, correspondencefinderprojective.cpp:119-257);
+   * the aligner then runs its list path.  At most 16 each. */
+  int row_search_region, col_search_region;
 } nicp_corr_params;
 
 /* Linearizer (linearizer.cpp:9-19). */
@@ -170,6 +177,13 @@ typedef struct {
   double translational_ratio, rotational_ratio;
   int solution_valid;    /* -1 when statistics were not computed */
   int status;            /* NICP_OK or a per-pair error */
+  /* Aligner::omega() (aligner.h:325, filled at aligner.cpp:108-134): the
+   * 6x6 information matrix of the solution in (t, quaternion-vector)
+   * coordinates, row-major, symmetrised; Aligner::_mean: the mean of the
+   * unscented reconstruction.  Zero when statistics were not computed or
+   * the system was singular. */
+  double omega[36];
+  double mean[6];
 } nicp_align_result;
 
 void nicp_default_camera(nicp_camera *c);

@@ -42,7 +42,8 @@ class CloudParams(C.Structure):
 class CorrParams(C.Structure):
     _fields_ = [("inlier_distance_threshold", C.c_float), ("inlier_normal_angular_threshold", C.c_float),
                 ("flat_curvature_threshold", C.c_float), ("inlier_curvature_ratio_threshold", C.c_float),
-                ("demoted_to_gicp", C.c_int), ("parity_threads", C.c_int)]
+                ("demoted_to_gicp", C.c_int), ("parity_threads", C.c_int), ("row_search_region", C.c_int),
+                ("col_search_region", C.c_int)]
 
 
 class LinParams(C.Structure):
@@ -60,7 +61,8 @@ class AlignParams(C.Structure):
 class AlignResult(C.Structure):
     _fields_ = [("T", D16), ("error", C.c_float), ("inliers", C.c_int), ("num_correspondences", C.c_int),
                 ("outer_iterations_run", C.c_int), ("translational_ratio", C.c_double),
-                ("rotational_ratio", C.c_double), ("solution_valid", C.c_int), ("status", C.c_int)]
+                ("rotational_ratio", C.c_double), ("solution_valid", C.c_int), ("status", C.c_int),
+                ("omega", C.c_double * 36), ("mean", C.c_double * 6)]
 
 
 class ServerParams(C.Structure):

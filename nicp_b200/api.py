@@ -540,6 +540,7 @@ class CorrespondenceFinderProjective:
         self._demotedToGICP = False
         self._rows = self._cols = 0
         self.parityThreads = 1
+        self._rowSearchRegion = self._colSearchRegion = 0  # correspondencefinderprojective.cpp:12-13
         self._referenceIndexImage = None
         self._currentIndexImage = None
         self._referenceDepthImage = None
@@ -556,6 +557,11 @@ class CorrespondenceFinderProjective:
     def setInlierCurvatureRatioThreshold(self, v): self._inlierCurvatureRatioThreshold = float(v)
     def inlierCurvatureRatioThreshold(self): return self._inlierCurvatureRatioThreshold
     def setDemotedToGICP(self, v): self._demotedToGICP = bool(v)
+    # correspondencefinderprojective.h:146-150: a search window (0 0 = the pixel itself)
+    def rowSearchRegion(self): return self._rowSearchRegion
+    def colSearchRegion(self): return self._colSearchRegion
+    def setRowSearchRegion(self, v): self._rowSearchRegion = int(v)
+    def setColSearchRegion(self, v): self._colSearchRegion = int(v)
     def demotedToGICP_(self): return self._demotedToGICP
     def setImageSize(self, rows, cols): self._rows, self._cols = int(rows), int(cols)
     def imageRows(self): return self._rows
@@ -575,6 +581,8 @@ class CorrespondenceFinderProjective:
         p.inlier_curvature_ratio_threshold = self._inlierCurvatureRatioThreshold
         p.demoted_to_gicp = 1 if self._demotedToGICP else 0
         p.parity_threads = self.parityThreads
+        p.row_search_region = self._rowSearchRegion
+        p.col_search_region = self._colSearchRegion
         return p
 
     def compute(self, referenceScene, currentScene, T):
@@ -691,6 +699,8 @@ class AlignerProjective:
         self._debug = False
         self._solutionValid = False
         self._translationalEigenRatio = self._rotationalEigenRatio = 0.0
+        self._omega = np.zeros((6, 6))
+        self._mean = np.zeros(6)
         self.computeStatistics = True
         self.earlyExitEps = 0.0
         self.last_result = None
@@ -739,6 +749,8 @@ class AlignerProjective:
     def setLambda(self, v): self._lambda = float(v)
     def lambda_(self): return self._lambda
     def solutionValid(self): return self._solutionValid
+    def omega(self): return self._omega.copy()  # aligner.h:325, 6x6 in (t, quaternion-vector)
+    def mean(self): return self._mean.copy()
     def error(self): return self._error
     def inliers(self): return self._inliers
     def totalTime(self): return self._totalTime
@@ -780,6 +792,8 @@ class AlignerProjective:
         self._translationalEigenRatio = r.translational_ratio
         self._rotationalEigenRatio = r.rotational_ratio
         self._solutionValid = bool(r.solution_valid == 1)
+        self._omega = np.array(r.omega).reshape(6, 6)
+        self._mean = np.array(r.mean)
         self.last_result = r
         return self._T
 
@@ -832,6 +846,8 @@ class AlignerNN(AlignerProjective):
         self._translationalEigenRatio = r.translational_ratio
         self._rotationalEigenRatio = r.rotational_ratio
         self._solutionValid = bool(r.solution_valid == 1)
+        self._omega = np.array(r.omega).reshape(6, 6)
+        self._mean = np.array(r.mean)
         self.last_result = r
         return self._T
 

@@ -248,6 +248,8 @@ static CorrParams corr_params(const nicp_corr_params &p) {
   c.max_ratio = p.inlier_curvature_ratio_threshold;
   c.demoted = p.demoted_to_gicp;
   c.row_limit_threads = std::max(1, p.parity_threads);
+  c.row_search = std::max(0, p.row_search_region);
+  c.col_search = std::max(0, p.col_search_region);
   return c;
 }
 
@@ -300,6 +302,7 @@ extern "C" void nicp_default_corr_params(nicp_corr_params *p) {
   p->inlier_curvature_ratio_threshold = 1.3f;
   p->demoted_to_gicp = 0;
   p->parity_threads = 1;
+  p->row_search_region = p->col_search_region = 0;
 }
 
 extern "C" void nicp_default_lin_params(nicp_lin_params *p) {
@@ -1154,6 +1157,9 @@ extern "C" int nicp_correspond(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_
   NICP_ON_DEVICE(ctx);
   if (!ctx || !ref || !cur || !ref_index || !cur_index || rows <= 0 || cols <= 0 || !T16 || !prm || !num_out)
     return NICP_EINVAL;
+  if (prm->row_search_region < 0 || prm->col_search_region < 0 || prm->row_search_region > 16 ||
+      prm->col_search_region > 16)
+    return fail(ctx, NICP_EINVAL, "search regions must lie in [0, 16]");
   nicp_camera cam;
   nicp_default_camera(&cam);
   cam.rows = rows;
@@ -1566,8 +1572,10 @@ extern "C" int nicp_align_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cl
   out->status = st.status;
   out->translational_ratio = out->rotational_ratio = 0;
   out->solution_valid = -1;
+  std::memset(out->omega, 0, sizeof(out->omega));
+  std::memset(out->mean, 0, sizeof(out->mean));
   if (prm->compute_statistics) {
-    solution_statistics(st.Hstat, st.T, &out->translational_ratio, &out->rotational_ratio);
+    solution_statistics(st.Hstat, st.T, &out->translational_ratio, &out->rotational_ratio, out->omega, out->mean);
     out->solution_valid = !(out->rotational_ratio > prm->rotational_min_eigen_ratio ||
                             out->translational_ratio > prm->translational_min_eigen_ratio);
   }
@@ -1938,7 +1946,12 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
     if (!a.foreign_clouds && (a.refs[i]->ctx != ctx || a.curs[i]->ctx != ctx))
       return fail(ctx, NICP_EINVAL, "cloud of another context");
   }
-  bool list_mode = a.corr->parity_threads > 1;
+  if (a.corr->row_search_region < 0 || a.corr->col_search_region < 0 || a.corr->row_search_region > 16 ||
+      a.corr->col_search_region > 16)
+    return fail(ctx, NICP_EINVAL, "search regions must lie in [0, 16]");
+  // windowed correspondences and the reference's partition drops run on
+  // the correspondence-list kernels
+  bool list_mode = a.corr->parity_threads > 1 || a.corr->row_search_region > 0 || a.corr->col_search_region > 0;
   bool keep_ref = p.inner_iterations > 1 || p.compute_statistics;
   // point tiles cover the larger of the two clouds: the current cloud is
   // projected once with the same grid as the reference cloud
@@ -2049,8 +2062,10 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
     r.status = st[i].status;
     r.translational_ratio = r.rotational_ratio = 0;
     r.solution_valid = -1;
+    std::memset(r.omega, 0, sizeof(r.omega));
+    std::memset(r.mean, 0, sizeof(r.mean));
     if (p.compute_statistics) {
-      solution_statistics(st[i].Hstat, st[i].T, &r.translational_ratio, &r.rotational_ratio);
+      solution_statistics(st[i].Hstat, st[i].T, &r.translational_ratio, &r.rotational_ratio, r.omega, r.mean);
       r.solution_valid = !(r.rotational_ratio > p.rotational_min_eigen_ratio ||
                            r.translational_ratio > p.translational_min_eigen_ratio);
     }

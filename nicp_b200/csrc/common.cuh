@@ -134,6 +134,7 @@ struct CorrParams {
   float sq_thr, cos_thr, flat_thr, min_ratio, max_ratio;
   int demoted;
   int row_limit_threads;  // parity threads T (rows beyond T*(rows/T) skipped)
+  int row_search, col_search;  // search window half-sizes (0 0: the pixel itself)
 };
 
 struct LinParams {

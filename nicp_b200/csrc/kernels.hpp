@@ -88,9 +88,10 @@ void launch_intervals(const float *d_depth, int P, const float *d_K9, float min_
                       cudaStream_t s, Profiler *prof);
 
 // Host-side Aligner::_computeStatistics (FP64): translational / rotational
-// eigen-ratios of the solution information matrix.
+// eigen-ratios of the solution information matrix, the matrix itself
+// (Aligner::omega(), row-major 6x6) and the reconstructed mean.
 void solution_statistics(const double H36[36], const double T16[16], double *translational_ratio,
-                         double *rotational_ratio);
+                         double *rotational_ratio, double omega36[36], double mean6[6]);
 
 // Grid (max_pt_tiles, npairs): max_pt_tiles = the largest number of
 // 1024-point tiles of any pair's projected cloud.

@@ -152,9 +152,12 @@ double block_ratio(const double *A6x6, int o) {
 
 }  // namespace
 
-void solution_statistics(const double H36[36], const double T16[16], double *tr, double *rr) {
+void solution_statistics(const double H36[36], const double T16[16], double *tr, double *rr, double omega36[36],
+                         double mean6[6]) {
   *tr = std::numeric_limits<double>::max();
   *rr = std::numeric_limits<double>::max();
+  for (int i = 0; i < 36; i++) omega36[i] = 0;
+  for (int i = 0; i < 6; i++) mean6[i] = 0;
   double A[36], V[36], w[6];
   for (int i = 0; i < 6; i++)
     for (int j = 0; j < 6; j++) A[i * 6 + j] = 0.5 * (H36[i * 6 + j] + H36[j * 6 + i]);
@@ -206,10 +209,12 @@ void solution_statistics(const double H36[36], const double T16[16], double *tr,
   for (int k = 0; k < np; k++)
     for (int r = 0; r < 6; r++)
       for (int c = 0; c < 6; c++) cov[r * 6 + c] += wc[k] * (samp[k][r] - mean[r]) * (samp[k][c] - mean[c]);
+  for (int i = 0; i < 6; i++) mean6[i] = mean[i];
   double Om[36];
   if (!inverse6(cov, Om)) return;
   for (int i = 0; i < 6; i++)
     for (int j = 0; j < 6; j++) A[i * 6 + j] = 0.5 * (Om[i * 6 + j] + Om[j * 6 + i]);
+  for (int i = 0; i < 36; i++) omega36[i] = A[i];
   *tr = block_ratio(A, 0);
   *rr = block_ratio(A, 3);
 }

@@ -761,9 +761,16 @@ template <> inline double curv_ratio<double>(double kr, double kc) { return (kr 
 // With `threads` = T, rows [T*(rows/T), rows) are never visited (the
 // reference's partition); the output is row-major over the visited rows.
 template <class S>
+static int correspond_multi(const Cloud<S> &ref, const Cloud<S> &cur, const int32_t *ri, const int32_t *ci,
+                            int rows, int cols, M4<S> T, const orc_align_params &prm, int32_t *pairs,
+                            bool f64mode);
+
+template <class S>
 static int correspond(const Cloud<S> &ref, const Cloud<S> &cur, const int32_t *ri, const int32_t *ci,
                       int rows, int cols, M4<S> T, const orc_align_params &prm, int32_t *pairs,
                       bool f64mode) {
+  if (prm.row_search_region != 0 || prm.col_search_region != 0)  // compute(), :16-21
+    return correspond_multi(ref, cur, ri, ci, rows, cols, T, prm, pairs, f64mode);
   set_row3(T);
   S thr = S(prm.inlier_distance_threshold);
   S sq = thr * thr;
@@ -804,6 +811,88 @@ static int correspond(const Cloud<S> &ref, const Cloud<S> &cur, const int32_t *r
         out.push_back(a);
         out.push_back(b);
       }
+  }
+  int k = 0;
+  for (int t = 0; t < nth; t++)
+    for (size_t i = 0; i < local[t].size(); i += 2) {
+      pairs[2 * k] = local[t][i];
+      pairs[2 * k + 1] = local[t][i + 1];
+      k++;
+    }
+  return k;
+}
+
+// CorrespondenceFinderProjective::_computeMulti
+// (correspondencefinderprojective.cpp:119-257), used by compute() when a
+// search region is set (:16-21): every reference pixel looks for the best
+// current pixel in the (2 rsr + 1) x (2 csr + 1) window around it (clamped
+// to the image), scanned row-major; gates in the order normal present,
+// normal angle, distance, curvature ratio; a later candidate replaces the
+// kept one only if it is both strictly closer and strictly better aligned.
+// Row partition and thread-order assembly as _computeSingle (rows % T
+// dropped).
+template <class S>
+static int correspond_multi(const Cloud<S> &ref, const Cloud<S> &cur, const int32_t *ri, const int32_t *ci,
+                            int rows, int cols, M4<S> T, const orc_align_params &prm, int32_t *pairs,
+                            bool f64mode) {
+  set_row3(T);
+  S thr = S(prm.inlier_distance_threshold);
+  S sq = thr * thr;
+  S minr = S(1) / S(prm.inlier_curvature_ratio_threshold);
+  S maxr = S(prm.inlier_curvature_ratio_threshold);
+  S cosT = S(prm.inlier_normal_angular_threshold);
+  S flat = S(prm.flat_curvature_threshold);
+  const int R = prm.row_search_region, Cc = prm.col_search_region;
+  int nth = (f64mode || prm.threads < 1) ? 1 : prm.threads;
+  int rpt = rows / nth;
+  std::vector<std::vector<int32_t>> local(nth);
+#pragma omp parallel for num_threads(nth) schedule(static, 1)
+  for (int t = 0; t < nth; t++) {
+    std::vector<int32_t> &out = local[t];
+    for (int r = t * rpt; r < (t + 1) * rpt; r++) {
+      const int rmin = std::max(r - R, 0), rmax = std::min(r + R + 1, rows);
+      for (int c = 0; c < cols; c++) {
+        const int a = ri[(size_t)r * cols + c];
+        if (a < 0) continue;
+        const V4<S> &rn0 = ref.normals[a];
+        if (dot4(rn0, rn0) == S(0)) continue;
+        V4<S> rp = mv(T, ref.points[a]);
+        rp[3] = S(1);
+        V4<S> rn = mv(T, rn0);
+        rn[3] = S(0);
+        S kr = ref.curvature[a];
+        if (kr < flat) kr = flat;
+        const int cmin = std::max(c - Cc, 0), cmax = std::min(c + Cc + 1, cols);
+        int best = -1;
+        S bestN = S(0), bestD = S(1e20);
+        for (int r2 = rmin; r2 < rmax; r2++)
+          for (int c2 = cmin; c2 < cmax; c2++) {
+            const int b = ci[(size_t)r2 * cols + c2];
+            if (b < 0) continue;
+            const V4<S> &cn = cur.normals[b];
+            if (dot4(cn, cn) == S(0)) continue;
+            const V4<S> &cp = cur.points[b];
+            const S nd = dot4(cn, rn);
+            if (nd < cosT) continue;
+            V4<S> dv = {{cp[0] - rp[0], cp[1] - rp[1], cp[2] - rp[2], cp[3] - rp[3]}};
+            const S d = dot4(dv, dv);
+            if (d > sq) continue;
+            S kc = cur.curvature[b];
+            if (kc < flat) kc = flat;
+            const S ratio = curv_ratio<S>(kr, kc);
+            if (ratio < minr || ratio > maxr) continue;
+            if (best == -1 || (d < bestD && nd > bestN)) {
+              best = b;
+              bestN = nd;
+              bestD = d;
+            }
+          }
+        if (best > -1) {
+          out.push_back(a);
+          out.push_back(best);
+        }
+      }
+    }
   }
   int k = 0;
   for (int t = 0; t < nth; t++)

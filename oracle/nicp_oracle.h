@@ -73,6 +73,8 @@ typedef struct {
   int threads;               /* emulated omp_get_max_threads() */
   double early_exit_eps;     /* stop once an outer iteration moves the pose by less
                                 (max |t2v(T T_start^-1)|); 0 = the reference's fixed count */
+  int row_search_region, col_search_region;  /* CorrespondenceFinderProjective search window
+                                                (correspondencefinderprojective.h:146-150); 0 0 = single */
 } orc_align_params;
 
 typedef struct orc_cloud orc_cloud;

@@ -42,7 +42,8 @@ class AlignParams(C.Structure):
                 ("z_scaling", C.c_int), ("lin_scale", C.c_float), ("lin_demoted_to_gicp", C.c_int),
                 ("outer_iterations", C.c_int), ("inner_iterations", C.c_int), ("lambda_", C.c_float),
                 ("translational_min_eigen_ratio", C.c_float), ("rotational_min_eigen_ratio", C.c_float),
-                ("threads", C.c_int), ("early_exit_eps", C.c_double)]
+                ("threads", C.c_int), ("early_exit_eps", C.c_double), ("row_search_region", C.c_int),
+                ("col_search_region", C.c_int)]
 
 
 class AlignResult(C.Structure):
@@ -158,6 +159,7 @@ def align_params(**kw):
     p.translational_min_eigen_ratio = p.rotational_min_eigen_ratio = 50.0
     p.threads = 1
     p.early_exit_eps = 0.0
+    p.row_search_region = p.col_search_region = 0
     for k, v in kw.items():
         setattr(p, k, v)
     return p

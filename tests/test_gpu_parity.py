@@ -104,6 +104,16 @@ def test_normals_curvature_vs_f64(ctx, pair):
     # information matrices (relative to their scale, 1000)
     dop = np.abs(f.get("omega_p").reshape(-1, 3, 3)[fi] - g["omega_p"][gi])[ok]
     assert np.max(dop) / 1000.0 < 1e-5, np.max(dop)
+    don = np.abs(f.get("omega_n").reshape(-1, 3, 3)[fi] - g["omega_n"][gi])[ok]
+    assert np.max(don) / 1000.0 < 1e-5, np.max(don)
+    # the class code the fused kernel rebuilds Omega from (point w) agrees
+    # with the stored matrices: Omega_p / Omega_n flat exactly where F64 is flat
+    fk = f.get("curvature")[fi][ok]
+    clear = np.abs(fk - 0.02) > 1e-5  # away from the flat/non-flat threshold
+    fflat = (fk < 0.02)[clear]
+    gflat_p = (np.trace(g["omega_p"][gi][ok], axis1=1, axis2=2) > 100.0)[clear]
+    gflat_n = (np.trace(g["omega_n"][gi][ok], axis1=1, axis2=2) > 100.0)[clear]
+    assert np.array_equal(fflat, gflat_p) and np.array_equal(fflat, gflat_n)
     # REF32 (the reference's own float arithmetic) is reported, not gated
     ri2, fi2 = match_by_pixel(ridx, fidx, stable)
     rn, fn2 = r.get("normals")[ri2, :3], f.get("normals")[fi2, :3]
@@ -216,6 +226,56 @@ def test_correspond_bitexact(ctx, pair, threads):
     assert np.array_equal(gp, op)
 
 
+@pytest.mark.parametrize("region", [(1, 1), (2, 2), (0, 2)], ids=["1x1", "2x2", "0x2"])
+@pytest.mark.parametrize("threads", [1, 4])
+def test_correspond_multi_bitexact(ctx, pair, region, threads):
+    """The windowed search (setRowSearchRegion / setColSearchRegion,
+    CorrespondenceFinderProjective::_computeMulti,
+    correspondencefinderprojective.cpp:119-257): the list equals the REF32
+    oracle's on identical clouds, index images and T, partition drops
+    included, and it differs from the single-pixel search."""
+    proj, ref, cur, ri, ci, T = _pipeline_inputs(ctx, pair, perturb(pair["seed"], 1.0, 0.02))
+    cf = api.CorrespondenceFinderProjective(ctx)
+    cf.parityThreads = threads
+    cf.setRowSearchRegion(region[0])
+    cf.setColSearchRegion(region[1])
+    cf.setReferenceIndexImage(ri)
+    cf.setCurrentIndexImage(ci)
+    Tinv = np.linalg.inv(float_T(T)).astype(np.float32)
+    gp = cf.compute(ref, cur, Tinv)
+    oref = oracle_cloud_from_gpu(O.REF32, ref.download())
+    ocur = oracle_cloud_from_gpu(O.REF32, cur.download())
+    prm = O.align_params(threads=threads, row_search_region=region[0], col_search_region=region[1])
+    op = O.correspond(O.REF32, oref, ocur, ri, ci, Tinv.astype(np.float64), prm)
+    single = O.correspond(O.REF32, oref, ocur, ri, ci, Tinv.astype(np.float64), O.align_params(threads=threads))
+    assert len(gp) > 1000
+    assert np.array_equal(gp, op)
+    assert not np.array_equal(gp, single)
+
+
+def test_align_with_search_region_vs_f64(ctx, pair):
+    """AlignerProjective with a 1 x 1 search window (list path on the device)
+    against the FP64 oracle loop with the same window on the same float
+    clouds: within 1e-5 rad / 0.05 mm."""
+    proj, conv = converter(pair["cam"], ctx)
+    ref, _ = gpu_cloud(ctx, conv, pair["d1"], keep_index=False)
+    cur, _ = gpu_cloud(ctx, conv, pair["d2"], keep_index=False)
+    cf = api.CorrespondenceFinderProjective(ctx)
+    cf.setRowSearchRegion(1)
+    cf.setColSearchRegion(1)
+    al = api.AlignerProjective(proj, api.Linearizer(ctx), cf, ctx)
+    al.computeStatistics = False
+    al.setReferenceCloud(ref)
+    al.setCurrentCloud(cur)
+    al.align()
+    pc, oc = cams(pair["cam"])
+    r = O.align(O.F64, oracle_cloud_from_gpu(O.F64, ref.download()), oracle_cloud_from_gpu(O.F64, cur.download()),
+                oc, prm=O.align_params(row_search_region=1, col_search_region=1))
+    er, et = synth.pose_error(al.T(), r["T"])
+    print("search region 1x1: GPU vs F64 %.3g rad %.3g m" % (er, et))
+    assert er < 1e-5 and et < 5e-5, (er, et)
+
+
 def _rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
@@ -284,6 +344,29 @@ def test_align_same_inputs_vs_f64(ctx, pair):
     r = O.align(O.F64, oref, ocur, oc)
     er, et = synth.pose_error(al.T(), r["T"])
     assert er < 1e-5 and et < 5e-5, (er, et)
+
+
+def test_solution_statistics_vs_f64(ctx, pair):
+    """Aligner::_computeStatistics (aligner.cpp:82-135): the solution's 6x6
+    information matrix Omega (Aligner::omega(), aligner.h:325), the unscented
+    mean, the two eigen-ratios and solutionValid, against the FP64 oracle loop
+    run on the same float clouds.  Omega and the ratios within 1e-4 relative
+    (they come from H at a final pose that itself agrees within 1e-5 rad),
+    the mean within 1e-5, solutionValid equal."""
+    al, ref, cur = _align_gpu(ctx, pair)
+    pc, oc = cams(pair["cam"])
+    oref = oracle_cloud_from_gpu(O.F64, ref.download())
+    ocur = oracle_cloud_from_gpu(O.F64, cur.download())
+    r = O.align(O.F64, oref, ocur, oc, statistics=True)
+    om, fom = al.omega(), r["omega"]
+    assert np.allclose(om, om.T) and np.linalg.norm(fom) > 0
+    rel_om = _rel(om, fom)
+    rel_tr = abs(al.translationalEigenRatio() - r["translational_ratio"]) / r["translational_ratio"]
+    rel_rr = abs(al.rotationalEigenRatio() - r["rotational_ratio"]) / r["rotational_ratio"]
+    dmean = np.max(np.abs(al.mean() - r["mean"]))
+    print("Omega rel %.3g, ratios rel %.3g / %.3g, mean %.3g" % (rel_om, rel_tr, rel_rr, dmean))
+    assert rel_om < 1e-4 and rel_tr < 1e-4 and rel_rr < 1e-4 and dmean < 1e-5
+    assert al.solutionValid() == bool(r["solution_valid"])
 
 
 def test_inner_iterations_and_parity_threads(ctx, pair):

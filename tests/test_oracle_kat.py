@@ -288,3 +288,63 @@ def test_unprojection_gaussian_analytic():
         exp = J @ np.diag([3.0, 3.0, zv]) @ J.T
         assert np.allclose(cov[k], exp, rtol=1e-9, atol=1e-15), (r, c)
         assert np.array_equal(mean[k], cl.get("points").reshape(-1, 4)[k, :3])
+
+
+def test_correspond_multi_matches_brute_force():
+    """_computeMulti (correspondencefinderprojective.cpp:119-257) restated:
+    for a sample of reference pixels, a plain-Python scan of the clamped
+    window (row-major; gates: current normal present, normal angle, distance,
+    curvature ratio; a later candidate replaces the kept one only if strictly
+    closer and strictly better aligned) picks the current point the oracle
+    lists; regions 0 0 give the single-pixel list."""
+    d1, d2, Tgt, cam = synth.render_pair(13, "160x120")
+    oc = O.camera(cam["rows"], cam["cols"], cam["fx"], cam["fy"], cam["cx"], cam["cy"])
+    ref, _ = O.build_cloud(O.F64, d1, oc)
+    cur, _ = O.build_cloud(O.F64, d2, oc)
+    ri, _ = O.project(O.F64, ref, oc, Tgt)
+    ci, _ = O.project(O.F64, cur, oc, np.eye(4))
+    T = np.linalg.inv(Tgt)
+    R, Cw = 2, 1
+    prm = O.align_params(row_search_region=R, col_search_region=Cw)
+    pairs = O.correspond(O.F64, ref, cur, ri, ci, T, prm)
+    assert len(pairs) > 1000
+    got = {int(a): int(b) for a, b in pairs}
+    P, N, K = ref.get("points"), ref.get("normals"), ref.get("curvature")
+    cP, cN, cK = cur.get("points"), cur.get("normals"), cur.get("curvature")
+    p0 = O.align_params()
+    sq = np.float64(np.float32(p0.inlier_distance_threshold)) ** 2
+    cos_t, flat = p0.inlier_normal_angular_threshold, np.float64(np.float32(p0.flat_curvature_threshold))
+    thr = np.float64(np.float32(p0.inlier_curvature_ratio_threshold))
+    rows, cols = ri.shape
+    rng = np.random.default_rng(3)
+    checked = 0
+    cand = np.argwhere((ri >= 0) & (np.abs(N[np.maximum(ri, 0), :3]).sum(-1) > 0))
+    for r, c in cand[rng.choice(len(cand), size=min(300, len(cand)), replace=False)]:
+        r, c = int(r), int(c)
+        a = ri[r, c]
+        rp = T[:3, :3] @ P[a, :3] + T[:3, 3]
+        rn = T[:3, :3] @ N[a, :3]
+        kr = max(K[a], flat)
+        best, bn, bd = -1, 0.0, 1e20
+        for r2 in range(max(r - R, 0), min(r + R + 1, rows)):
+            for c2 in range(max(c - Cw, 0), min(c + Cw + 1, cols)):
+                b = ci[r2, c2]
+                if b < 0 or not cN[b, :3].any():
+                    continue
+                nd = float(cN[b, :3] @ rn)
+                if nd < cos_t:
+                    continue
+                d = float(np.sum((cP[b, :3] - rp) ** 2))
+                if d > sq:
+                    continue
+                ratio = (kr + 1e-5) / (max(cK[b], flat) + 1e-5)
+                if ratio < 1.0 / thr or ratio > thr:
+                    continue
+                if best == -1 or (d < bd and nd > bn):
+                    best, bn, bd = b, nd, d
+        assert got.get(int(a), -1) == best, (r, c)
+        checked += 1
+    assert checked > 100
+    single = O.correspond(O.F64, ref, cur, ri, ci, T, O.align_params())
+    zero = O.correspond(O.F64, ref, cur, ri, ci, T, O.align_params(row_search_region=0, col_search_region=0))
+    assert np.array_equal(single, zero)
