@@ -295,6 +295,7 @@ class DepthImageConverterIntegralImage {
                const Isometry3f &sensorOffset = Isometry3f::Identity()) {
     nicp_cloud_params p = params();
     proj_->setImageSize(rows, cols);
+    proj_->setTransform(Isometry3f::Identity());  // depthimageconverterintegralimage.cpp:42
     nicp_camera c = proj_->camera();
     check(cloud.context().handle(), nicp_cloud_from_depth_u16(cloud.context().handle(), depth, rows, cols, 0, 0, &c,
                                                               &p, sensorOffset.data(), cloud.handle(), nullptr));
@@ -304,6 +305,7 @@ class DepthImageConverterIntegralImage {
                const Isometry3f &sensorOffset = Isometry3f::Identity()) {
     nicp_cloud_params p = params();
     proj_->setImageSize(rows, cols);
+    proj_->setTransform(Isometry3f::Identity());  // depthimageconverterintegralimage.cpp:42
     nicp_camera c = proj_->camera();
     check(cloud.context().handle(), nicp_cloud_from_depth_f32(cloud.context().handle(), depth, rows, cols, 0, 0, &c,
                                                               &p, sensorOffset.data(), cloud.handle(), nullptr));

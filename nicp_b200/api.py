@@ -435,6 +435,9 @@ class DepthImageConverterIntegralImage:
         d = np.ascontiguousarray(depthImage)
         rows, cols = d.shape
         self._projector.setImageSize(rows, cols)
+        # the converter unprojects in the camera frame and leaves the
+        # projector there (depthimageconverterintegralimage.cpp:42)
+        self._projector.setTransform(np.eye(4))
         cam = self._projector.camera(rows, cols)
         prm = self.params()
         idx = np.zeros((rows, cols), np.int32) if keep_index else None

@@ -159,18 +159,56 @@ __global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restr
   for (int q = t; q < tile; q += blockDim.x) before += f.tile_counts[q];
   before = block_sum_int(before, red);
   const int base = tile * kUnprojTilePixels + t;
-  // every round's depth is loaded before the first ballot (one branch on the
-  // depth type for all of them), so the loads are in flight together
+  // The tile's depths come in with 128-bit loads (thread t: bytes 16 t,
+  // 16 (t + 256), ... of the tile) into shared memory, from where thread t
+  // takes pixels t, t + 256, ...; unaligned or partial tiles load per pixel.
+  __shared__ __align__(16) unsigned char sdepth[kUnprojTilePixels * 4];
+  const int tile0 = tile * kUnprojTilePixels;
+  const int n_in = min(kUnprojTilePixels, P - tile0);
   float d[kUnprojRounds];
   if (f.depth_u16) {
-    unsigned short u[kUnprojRounds];
+    const uint16_t *src = f.depth_u16 + tile0;
+    uint16_t *dst = reinterpret_cast<uint16_t *>(sdepth);
+    if (n_in == kUnprojTilePixels && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+      const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+      uint4 v[kUnprojTilePixels / 8 / 256];
 #pragma unroll
-    for (int k = 0; k < kUnprojRounds; k++) u[k] = base + k * 256 < P ? f.depth_u16[base + k * 256] : 0;
+      for (int k = 0; k < kUnprojTilePixels / 8 / 256; k++) v[k] = __ldg(s4 + t + 256 * k);
 #pragma unroll
-    for (int k = 0; k < kUnprojRounds; k++) d[k] = u[k] ? fm(f.depth_scale, (float)(int)u[k]) : 0.0f;
+      for (int k = 0; k < kUnprojTilePixels / 8 / 256; k++) reinterpret_cast<uint4 *>(dst)[t + 256 * k] = v[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < kUnprojRounds; k++) {
+        const int q = t + 256 * k;
+        dst[q] = q < n_in ? src[q] : (uint16_t)0;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kUnprojRounds; k++) {
+      const uint16_t u = dst[t + 256 * k];
+      d[k] = u ? fm(f.depth_scale, (float)(int)u) : 0.0f;
+    }
   } else {
+    const float *src = f.depth_f32 + tile0;
+    float *dst = reinterpret_cast<float *>(sdepth);
+    if (n_in == kUnprojTilePixels && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+      const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+      uint4 v[kUnprojTilePixels / 4 / 256];
 #pragma unroll
-    for (int k = 0; k < kUnprojRounds; k++) d[k] = base + k * 256 < P ? f.depth_f32[base + k * 256] : 0.0f;
+      for (int k = 0; k < kUnprojTilePixels / 4 / 256; k++) v[k] = __ldg(s4 + t + 256 * k);
+#pragma unroll
+      for (int k = 0; k < kUnprojTilePixels / 4 / 256; k++) reinterpret_cast<uint4 *>(dst)[t + 256 * k] = v[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < kUnprojRounds; k++) {
+        const int q = t + 256 * k;
+        dst[q] = q < n_in ? src[q] : 0.0f;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kUnprojRounds; k++) d[k] = dst[t + 256 * k];
   }
   unsigned mask = 0;
 #pragma unroll

@@ -348,3 +348,38 @@ def test_correspond_multi_matches_brute_force():
     single = O.correspond(O.F64, ref, cur, ri, ci, T, O.align_params())
     zero = O.correspond(O.F64, ref, cur, ri, ci, T, O.align_params(row_search_region=0, col_search_region=0))
     assert np.array_equal(single, zero)
+
+
+def test_pose_sensitivity_to_one_ulp_of_depth():
+    """How well the FP64 pose of the config-1 pair (the golden pair: 320x240,
+    2 deg + 3 cm, reference defaults, 10 outer x 1 inner) is determined by
+    its input: moving every float depth of the reference's DepthImage by one
+    ulp, up or down at random, moves the FP64 pipeline's pose by more than
+    1e-5 rad -- discrete decisions (window radii, validity, gates, pixel
+    rounding) flip and the unconverged loop carries the difference on.  A
+    float pipeline cannot be held closer to FP64 than this on this pair, so
+    the pose gate of this pair is quoted together with these figures."""
+    d1, d2, _, cam = synth.render_pair(1, "320x240", deg=2.0, meters=0.03)
+    oc = O.camera(cam["rows"], cam["cols"], cam["fx"], cam["fy"], cam["cx"], cam["cy"])
+    f1, f2 = O.convert_u16(d1), O.convert_u16(d2)
+    a, _ = O.build_cloud_f32(O.F64, f1, oc)
+    b, _ = O.build_cloud_f32(O.F64, f2, oc)
+    T0 = O.align(O.F64, a, b, oc)["T"]
+    # the u16 path starts from the same float image
+    a16, _ = O.build_cloud(O.F64, d1, oc)
+    b16, _ = O.build_cloud(O.F64, d2, oc)
+    assert np.array_equal(O.align(O.F64, a16, b16, oc)["T"], T0)
+    moves = []
+    for seed in (1, 2, 3):
+        rng = np.random.default_rng(seed)
+
+        def ulp(f):
+            up = rng.integers(0, 2, size=f.shape).astype(bool)
+            g = np.where(up, np.nextafter(f, np.float32(np.inf)), np.nextafter(f, np.float32(-np.inf)))
+            return np.where(f > 0, g, f).astype(np.float32)
+
+        pa, _ = O.build_cloud_f32(O.F64, ulp(f1), oc)
+        pb, _ = O.build_cloud_f32(O.F64, ulp(f2), oc)
+        moves.append(synth.pose_error(O.align(O.F64, pa, pb, oc)["T"], T0))
+    print("FP64 pose moved by one-ulp depth perturbations: %s" % ["%.2e rad %.2e m" % m for m in moves])
+    assert max(m[0] for m in moves) > 1e-5

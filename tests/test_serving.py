@@ -3,7 +3,9 @@ keyframes.  Each stream's results must be the same whether the stream is
 served alone or mixed with other streams (batches differ in composition and
 size; the kernels' per-pair sums do not depend on either), frames of one
 stream are handled in order against the keyframe the previous frame left,
-and a request that can never fit the memory budget is refused."""
+a request that can never fit the memory budget is refused, one that fits
+only after in-flight work completes waits for it, and requests submitted
+while batches run join later batches with unchanged results."""
 import numpy as np
 import pytest
 
@@ -104,3 +106,54 @@ def test_request_beyond_budget_is_refused(ctx, streams):
     res = srv.drain(1, timeout_s=30)
     srv.close()
     assert len(res) == 1 and res[0]["status"] == L.NICP_EBUDGET
+
+
+def test_request_waits_for_memory_and_keeps_its_result(ctx, streams):
+    """A request that fits the budget only once in-flight work has finished
+    is held back, admitted when that work completes, and gives the same
+    result as with room to spare.  Two 640x480 streams, a budget of 365
+    bytes per pixel: both first frames fit together, but once both keyframes
+    are resident (84 B/pixel each) only one more request (181 B/pixel) can
+    be in flight, so the second stream's next frame must wait for the first
+    stream's (two workers: room, not a free worker, is what it waits for)."""
+    frames, poses, cam = streams[2]
+    P = cam["rows"] * cam["cols"]
+
+    def run(budget):
+        srv = api.Server(hbm_budget_bytes=budget, max_batch=4, workers=2)
+        for f in range(3):
+            for s in (0, 1):
+                srv.submit(s, 10 * s + f, frames[f + 2 * s], _camera(cam))
+        res = srv.drain(6, timeout_s=60)
+        srv.close()
+        return {r["request_id"]: r for r in res}
+
+    tight = run(365 * P)
+    roomy = run(60 << 30)
+    assert len(tight) == len(roomy) == 6
+    for k, r in tight.items():
+        assert r["status"] == 0, (k, r["status"])
+        assert np.array_equal(r["T"], roomy[k]["T"]) and r["inliers"] == roomy[k]["inliers"], k
+        assert r["keyframe_replaced"] == roomy[k]["keyframe_replaced"], k
+
+
+def test_request_submitted_while_a_batch_runs(ctx, streams):
+    """Frames submitted while other requests are on the device join later
+    batches and give the results they give alone."""
+    alone = {**_serve(streams, [2], max_batch=8, workers=1), **_serve(streams, [0], max_batch=8, workers=1)}
+    srv = api.Server(max_batch=8, workers=2)
+    f2, _, cam2 = streams[2]
+    f0, _, cam0 = streams[0]
+    for f in range(6):
+        srv.submit(2, 2000 + f, f2[f], _camera(cam2))
+    late = 0
+    for f in range(6):
+        pending, _ = srv.status()
+        late += pending > 0  # stream 2's requests still queued or on the device
+        srv.submit(0, f, f0[f], _camera(cam0))
+    res = {r["request_id"]: r for r in srv.drain(12, timeout_s=60)}
+    srv.close()
+    assert late > 0 and len(res) == 12
+    for k, r in res.items():
+        assert r["status"] == 0
+        assert np.array_equal(r["T"], alone[k]["T"]) and r["inliers"] == alone[k]["inliers"], k
