@@ -217,13 +217,18 @@ int nicp_ctx_set_profiling(nicp_ctx *ctx, int enable);
  * iteration counts) times the Gauss-Newton loop with each candidate launch
  * shape -- z-buffer points per thread 1/2/4/8, fused correspondence +
  * linearizer CTAs per SM 2/3/as many as fit -- and keeps the fastest for
- * that mix.  Results do not depend on the launch shape (bitwise).  The
- * trials run on the context stream before the call's own loop. */
+ * that mix; the first build of a new frame-size mix likewise times the
+ * stats kernel (normals, curvature, information matrices) at 256 x 3,
+ * 128 x 6, 64 x 12 and 256 x 2 (threads per CTA x CTAs per SM) and keeps
+ * the fastest.  Results do not depend on the launch shapes (bitwise).  The
+ * trials run on the context stream before the call's own work and
+ * synchronize it once. */
 int nicp_ctx_set_autotune(nicp_ctx *ctx, int enable);
 /* Launch shape used by the last alignment call (corr_ctas_per_sm 0 = as many
- * as fit) and the number of resolution mixes tuned so far. */
+ * as fit), the number of resolution mixes tuned so far, and the stats
+ * kernel's shape in the last build.  Any pointer may be NULL. */
 int nicp_ctx_launch_shape(const nicp_ctx *ctx, int *zbuffer_points_per_thread, int *corr_ctas_per_sm,
-                          int *tuned_mixes);
+                          int *tuned_mixes, int *stats_threads, int *stats_ctas_per_sm);
 /* Kernels this context has launched so far (graph replays included). */
 unsigned long long nicp_ctx_kernel_launches(const nicp_ctx *ctx);
 /* Host->device and device->host bytes the context has copied so far. */
@@ -236,6 +241,9 @@ int nicp_cloud_create(nicp_ctx *ctx, nicp_cloud **out);
 int nicp_cloud_destroy(nicp_cloud *c);
 /* Number of points (synchronizes). */
 int nicp_cloud_size(nicp_cloud *c, int *n);
+/* Number of points with a normal, counted by the build (no reference
+ * counterpart; the serving loop's keyframe test uses it; synchronizes). */
+int nicp_cloud_normal_count(nicp_cloud *c, int *n);
 
 /* Cloud::gaussians() (cloud.h:107; filled by unProject,
  * pinholepointprojector.cpp:93-134, moved by Gaussian3fVector::

@@ -99,13 +99,15 @@ SIGNATURES = {
     "nicp_ctx_set_profiling": (C.c_int, [P, C.c_int]),
     "nicp_ctx_kernel_launches": (C.c_ulonglong, [P]),
     "nicp_ctx_set_autotune": (C.c_int, [P, C.c_int]),
-    "nicp_ctx_launch_shape": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "nicp_ctx_launch_shape": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "nicp_ctx_transfer_bytes": (C.c_int, [P, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
     "nicp_ctx_read_profile": (C.c_int, [P, C.c_int, f64p, C.POINTER(C.c_int)]),
     "nicp_kernel_name": (C.c_char_p, [C.c_int]),
     "nicp_cloud_create": (C.c_int, [P, C.POINTER(P)]),
     "nicp_cloud_destroy": (C.c_int, [P]),
     "nicp_cloud_size": (C.c_int, [P, C.POINTER(C.c_int)]),
+    "nicp_cloud_normal_count": (C.c_int, [P, C.POINTER(C.c_int)]),
     "nicp_cloud_download": (C.c_int, [P, f32p, f32p, f32p, f32p, f32p, f32p, f32p]),
     "nicp_cloud_download_gaussians": (C.c_int, [P, f32p, f32p]),
     "nicp_cloud_download_stats": (C.c_int, [P, f32p, f32p, f32p, i32p]),

@@ -75,8 +75,14 @@ class Context:
         """(z-buffer points per thread, fused-kernel CTAs per SM (0 = all that
         fit), resolution mixes tuned) of the last alignment call."""
         a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
-        self.check(self.lib.nicp_ctx_launch_shape(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        self.check(self.lib.nicp_ctx_launch_shape(self.h, C.byref(a), C.byref(b), C.byref(c), None, None))
         return a.value, b.value, c.value
+
+    def stats_shape(self):
+        """(threads per CTA, CTAs per SM) of the stats kernel in the last build."""
+        a, b = C.c_int(0), C.c_int(0)
+        self.check(self.lib.nicp_ctx_launch_shape(self.h, None, None, None, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def read_profile(self, kernel):
         ms = C.c_double(0)
@@ -118,6 +124,12 @@ class Cloud:
         return n.value
 
     __len__ = size
+
+    def normal_count(self):
+        """Points with a normal (counted on the device by the build)."""
+        n = C.c_int(0)
+        self.ctx.check(self.ctx.lib.nicp_cloud_normal_count(self.h, C.byref(n)))
+        return n.value
 
     def download(self, stats=False):
         n = self.size()

@@ -74,6 +74,10 @@ struct nicp_ctx {
   Launch launch;
   bool autotune = false;
   std::map<std::string, Launch> tuned;
+  // k_stats launch shape per frame-size mix of a build chunk (autotuned),
+  // and the shape of the last build
+  std::map<std::string, int> stats_tuned;
+  int stats_shape = 0;
   std::map<std::string, std::vector<float>> tune_ms;  // trial times per resolution mix
 };
 
@@ -423,11 +427,13 @@ extern "C" int nicp_ctx_set_autotune(nicp_ctx *ctx, int enable) {
 }
 
 extern "C" int nicp_ctx_launch_shape(const nicp_ctx *ctx, int *zbuffer_points_per_thread, int *corr_ctas_per_sm,
-                                     int *tuned_mixes) {
+                                     int *tuned_mixes, int *stats_threads, int *stats_ctas_per_sm) {
   NICP_ABI_TRY
   NICP_ON_DEVICE(ctx);
   if (!ctx) return NICP_EINVAL;
   if (zbuffer_points_per_thread) *zbuffer_points_per_thread = ctx->launch.zb_ppt;
+  if (stats_threads) *stats_threads = stats_shape_threads(ctx->stats_shape);
+  if (stats_ctas_per_sm) *stats_ctas_per_sm = stats_shape_min_ctas(ctx->stats_shape);
   if (corr_ctas_per_sm) *corr_ctas_per_sm = ctx->launch.corr_ctas;
   if (tuned_mixes) *tuned_mixes = (int)ctx->tuned.size();
   return NICP_OK;
@@ -512,6 +518,18 @@ extern "C" int nicp_cloud_size(nicp_cloud *c, int *n) {
   if (!c->mem) { *n = 0; return NICP_OK; }
   nicp_ctx *ctx = c->ctx;
   CK(ctx, cudaMemcpyAsync(n, c->count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return NICP_OK;
+  NICP_ABI_CATCH
+}
+
+extern "C" int nicp_cloud_normal_count(nicp_cloud *c, int *n) {
+  NICP_ABI_TRY
+  NICP_ON_DEVICE(c ? c->ctx : nullptr);
+  if (!c || !n) return NICP_EINVAL;
+  if (!c->mem) { *n = 0; return NICP_OK; }
+  nicp_ctx *ctx = c->ctx;
+  CK(ctx, cudaMemcpyAsync(n, c->count + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return NICP_OK;
   NICP_ABI_CATCH
@@ -677,6 +695,45 @@ struct FrameIn {
 };
 }  // namespace
 
+// Times k_stats on a chunk (its moments complete) with every launch shape
+// and returns the fastest.  The kernel writes the same outputs under every
+// shape; only its count of points with a normal accumulates, so that count
+// is zeroed before each run (and before the real run that follows).
+static int tune_stats(nicp_ctx *ctx, int precision, const FrameDev *dfr, int nf, int max_pixels, int *best) {
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t e0, e1;
+  CK(ctx, cudaEventCreate(&e0));
+  CK(ctx, cudaEventCreate(&e1));
+  const bool prof = ctx->prof.enabled;
+  ctx->prof.enabled = false;
+  float best_ms = 0;
+  *best = 0;
+  int rc = NICP_OK;
+  for (int rep = 0; rep < 2 && rc == NICP_OK; rep++)  // the first pass also loads the kernels
+    for (int shape = 0; shape < kStatsShapes; shape++) {
+      launch_reset_normal_counts(dfr, nf, s);
+      cudaEventRecord(e0, s);
+      launch_stats(precision, dfr, nf, max_pixels, shape, s, &ctx->prof);
+      cudaEventRecord(e1, s);
+      float ms = 0;
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) {
+        rc = fail(ctx, NICP_ECUDA, std::string("stats autotune: ") + cudaGetErrorString(e));
+        break;
+      }
+      if (rep == 1 && (shape == 0 || ms < best_ms)) {
+        best_ms = ms;
+        *best = shape;
+      }
+    }
+  launch_reset_normal_counts(dfr, nf, s);
+  ctx->prof.enabled = prof;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
 // Builds clouds for frames [0, n) in chunks that bound the integral-image
 // scratch.  The descriptors of every chunk are filled first and uploaded in
 // one copy.  Frames that need staging (host frames, or device frames that
@@ -782,7 +839,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   char *pin;
   if ((rc = pin_up(ctx, frames_bytes, &pin))) return rc;
   int *tab_all = reinterpret_cast<int *>(pin + sizeof(FrameDev) * n);
-  struct Grid { int tiles, bands, carryctas, max_bands, max_stiles; };
+  struct Grid { int tiles, bands, carryctas, max_bands, max_pixels; };
   std::vector<Grid> grids(chunks.size());
   for (size_t ci = 0; ci < chunks.size(); ci++) {
     const int i0 = chunks[ci].first, nf = chunks[ci].second - i0;
@@ -800,7 +857,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     }
     FrameDev *fd = reinterpret_cast<FrameDev *>(pin) + i0;
     int *tab_t = tab_all + tab_off[ci], *tab_b = tab_t + tab_tiles[ci], *tab_k = tab_b + tab_bands[ci];
-    int tiles = 0, bands = 0, carryctas = 0, max_bands = 0, max_stiles = 0;
+    int tiles = 0, bands = 0, carryctas = 0, max_bands = 0, max_pixels = 0;
     for (int k = 0; k < nf; k++) {
       const FrameIn &f = fin[i0 + k];
       const nicp_camera &cam = cams[i0 + k];
@@ -822,7 +879,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       tiles += (int)((P + kUnprojTilePixels - 1) / kUnprojTilePixels);
       bands += (f.rows + nb_rows - 1) / nb_rows;
       max_bands = std::max(max_bands, (f.rows + nb_rows - 1) / nb_rows);
-      max_stiles = std::max(max_stiles, (int)((P + kStatsThreads - 1) / kStatsThreads));
+      max_pixels = std::max(max_pixels, (int)P);
       carryctas += (10 * f.cols + 127) / 128;
       d.depth_scale = prm->depth_scale;
       d.min_d = cam.min_distance;
@@ -871,7 +928,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       d.band_tot = unproject_only ? nullptr : (void *)(ctx->ws + o_band[k]);
       d.rowpre = o_rowpre[k] ? (void *)(ctx->ws + o_rowpre[k]) : nullptr;
     }
-    grids[ci] = {tiles, bands, carryctas, max_bands, max_stiles};
+    grids[ci] = {tiles, bands, carryctas, max_bands, max_pixels};
   }
   FrameDev *dfr_all = (FrameDev *)(ctx->ws + o_frames_all);
   CK(ctx, cudaMemcpyAsync(dfr_all, pin, frames_bytes, cudaMemcpyHostToDevice, s));
@@ -932,7 +989,28 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     launch_unproject(dfr, nf, g.tiles, ft, s, &ctx->prof);
     if (!unproject_only) {
       launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, g.max_bands, fb, fk, s, &ctx->prof);
-      launch_stats(prm->moments_precision, dfr, nf, g.max_stiles, s, &ctx->prof);
+      int shape = 0;
+      if (ctx->autotune) {
+        // the chunk's frame sizes and the moment precision select the shape
+        std::map<std::pair<int, int>, int> hist;
+        for (int i = i0; i < i0 + nf; i++) hist[{fin[i].rows, fin[i].cols}]++;
+        std::string key = std::to_string(prm->moments_precision) + ":";
+        for (auto &h : hist)
+          key += std::to_string(h.first.first) + "x" + std::to_string(h.first.second) + "*" +
+                 std::to_string(h.second) + " ";
+        auto it = ctx->stats_tuned.find(key);
+        if (it == ctx->stats_tuned.end()) {
+          int best = 0, rc = tune_stats(ctx, prm->moments_precision, dfr, nf, g.max_pixels, &best);
+          if (rc) {
+            if (any_staged) cudaStreamSynchronize(ctx->copy_stream);
+            return rc;
+          }
+          it = ctx->stats_tuned.emplace(key, best).first;
+        }
+        shape = it->second;
+      }
+      ctx->stats_shape = shape;
+      launch_stats(prm->moments_precision, dfr, nf, g.max_pixels, shape, s, &ctx->prof);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail_staged(e, "build launch");
   }

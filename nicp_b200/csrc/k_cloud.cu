@@ -597,10 +597,13 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const Fra
 // ------------------------------------------------------------ stats + omegas
 // Grid (pixel tile, frame): the frame is blockIdx.y, no search over the frame
 // descriptors.
-template <class M>
-__global__ void __launch_bounds__(kStatsThreads, 3) k_stats(const FrameDev *__restrict__ frames, int nframes) {
+// One thread per pixel: the CTA size and the CTAs per SM the compiler
+// budgets registers for are launch shapes only (the autotuner picks one per
+// frame-size mix); every pixel's result is the same under all of them.
+template <class M, int kThreads, int kMinCtas>
+__global__ void __launch_bounds__(kThreads, kMinCtas) k_stats(const FrameDev *__restrict__ frames, int nframes) {
   const FrameDev &f = frames[blockIdx.y];
-  int pix = blockIdx.x * kStatsThreads + threadIdx.x;
+  int pix = blockIdx.x * kThreads + threadIdx.x;
   int rows = f.rows, cols = f.cols;
   int P = rows * cols;
   if (pix >= P) return;
@@ -985,13 +988,43 @@ void launch_moments(int precision, const FrameDev *d_frames, int nframes, int to
                          prof);
 }
 
-void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_tiles, cudaStream_t s, Profiler *prof) {
+// Stats launch shapes: (threads per CTA, CTAs per SM of the register budget).
+static const int kStatsShape[kStatsShapes][2] = {{256, 3}, {128, 6}, {64, 12}, {256, 2}};
+
+int stats_shape_threads(int shape) { return kStatsShape[shape][0]; }
+int stats_shape_min_ctas(int shape) { return kStatsShape[shape][1]; }
+
+template <class M>
+static void stats_launch(int shape, dim3 g, const FrameDev *d_frames, int nframes, cudaStream_t s) {
+  switch (shape) {
+    case 1: k_stats<M, 128, 6><<<g, 128, 0, s>>>(d_frames, nframes); break;
+    case 2: k_stats<M, 64, 12><<<g, 64, 0, s>>>(d_frames, nframes); break;
+    case 3: k_stats<M, 256, 2><<<g, 256, 0, s>>>(d_frames, nframes); break;
+    default: k_stats<M, 256, 3><<<g, 256, 0, s>>>(d_frames, nframes); break;
+  }
+}
+
+void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_pixels, int shape, cudaStream_t s,
+                  Profiler *prof) {
+  if (shape < 0 || shape >= kStatsShapes) shape = 0;
   prof->begin(NICP_K_STATS, s);
-  const dim3 g(max_tiles, nframes);
-  if (precision == NICP_MOMENTS_F32) k_stats<MomF32><<<g, kStatsThreads, 0, s>>>(d_frames, nframes);
-  else if (precision == NICP_MOMENTS_TWOFLOAT) k_stats<MomTwoFloat><<<g, kStatsThreads, 0, s>>>(d_frames, nframes);
-  else k_stats<MomF64><<<g, kStatsThreads, 0, s>>>(d_frames, nframes);
+  const int threads = kStatsShape[shape][0];
+  const dim3 g((max_pixels + threads - 1) / threads, nframes);
+  if (precision == NICP_MOMENTS_F32) stats_launch<MomF32>(shape, g, d_frames, nframes, s);
+  else if (precision == NICP_MOMENTS_TWOFLOAT) stats_launch<MomTwoFloat>(shape, g, d_frames, nframes, s);
+  else stats_launch<MomF64>(shape, g, d_frames, nframes, s);
   prof->end(NICP_K_STATS, s);
+}
+
+// Zeroes the frames' counts of points with a normal (k_stats adds to them),
+// so that the stats kernel can run again with another launch shape.
+__global__ void k_reset_normal_counts(const FrameDev *__restrict__ frames, int nframes) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nframes) frames[i].count[1] = 0;
+}
+
+void launch_reset_normal_counts(const FrameDev *d_frames, int nframes, cudaStream_t s) {
+  if (nframes > 0) k_reset_normal_counts<<<(nframes + 127) / 128, 128, 0, s>>>(d_frames, nframes);
 }
 
 void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,

@@ -77,10 +77,14 @@ size_t moment_acc_bytes(int precision);
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
                     int max_bands, const int *frame_of_band, const int *frame_of_carry, cudaStream_t s,
                     Profiler *prof);
-// (tile, frame) grid: max_tiles = the largest number of kStatsThreads-pixel
-// tiles of any frame of the launch; nframes <= 65535.
-void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_tiles, cudaStream_t s,
+// (pixel tile, frame) grid over max_pixels, the largest frame of the launch;
+// nframes <= 65535.  shape: one of kStatsShapes (CTA size, CTAs per SM).
+constexpr int kStatsShapes = 4;  // k_stats launch shapes the autotuner chooses from (0: default)
+int stats_shape_threads(int shape);
+int stats_shape_min_ctas(int shape);
+void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_pixels, int shape, cudaStream_t s,
                   Profiler *prof);
+void launch_reset_normal_counts(const FrameDev *d_frames, int nframes, cudaStream_t s);
 void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,
                             int capacity, const float *d_m12, cudaStream_t s, Profiler *prof);
 size_t moment_bytes(int precision);

@@ -105,3 +105,40 @@ def test_wide_batch_default_shape_matches_single_pairs(ctx):
         assert ctx.launch_shape()[:2] == (4, 0)
         assert np.array_equal(np.array(one[0].T), np.array(wide[i].T))
         assert one[0].inliers == wide[i].inliers
+
+
+def test_autotuned_stats_shape_gives_identical_clouds(ctx):
+    """The build's autotuner (stats kernel: threads per CTA x CTAs per SM)
+    leaves every cloud bitwise as the default shape builds it, the count of
+    points with a normal included (the trials run the kernel several times)."""
+    frames, cam_list = [], []
+    for seed, name in [(61, "640x480"), (62, "320x240"), (63, "640x480")]:
+        d1, _, _, cam = synth.render_pair(seed, name)
+        proj, conv = converter(cam, ctx, keep_stats=True)
+        frames.append(d1)
+        cam_list.append(proj.camera(cam["rows"], cam["cols"]))
+        prm = conv.params()
+
+    def build():
+        outs = [api.Cloud(ctx) for _ in frames]
+        api.build_batch(ctx, frames, cam_list, prm, outs)
+        return [(o.download(stats=True), ctx.lib) for o in outs], outs
+
+    ctx.set_autotune(False)
+    base, keep0 = build()
+    assert ctx.stats_shape() == (256, 3)
+    ctx.set_autotune(True)
+    try:
+        tuned, keep1 = build()
+        shape = ctx.stats_shape()
+        assert shape in ((256, 3), (128, 6), (64, 12), (256, 2))
+        again, keep2 = build()  # cached choice
+        assert ctx.stats_shape() == shape
+    finally:
+        ctx.set_autotune(False)
+    for (a, _), (b, _), (c, _) in zip(base, tuned, again):
+        for k in ("points", "normals", "curvature", "omega_p", "omega_n", "eigenvalues", "eigenvectors"):
+            assert np.array_equal(a[k], b[k]) and np.array_equal(a[k], c[k]), k
+    counts = [[o.normal_count() for o in outs] for outs in (keep0, keep1, keep2)]
+    assert counts[0] == counts[1] == counts[2]
+    assert counts[0] == [int((np.abs(a["normals"][:, :3]).sum(1) > 0).sum()) for a, _ in base]
