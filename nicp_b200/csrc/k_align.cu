@@ -329,194 +329,6 @@ __device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const 
   lin_terms_structured_xf(lp, omd, xform_point(T12, rp0), xform_normal(T12, rn0), cpt, cn, acc);
 }
 
-// ---- two pixels per instruction (sm_100 packed FP32: FMUL2 / FADD2 / FFMA2).
-// A float2 holds the same quantity of two pixels, A in .x and B in .y; each
-// half is rounded exactly as the scalar __fmul_rn / __fadd_rn / fmaf would
-// round it, so the packed gate takes the scalar gate's decisions bit for bit.
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-// a - b with one rounding: fma(b, -1, a) is exactly __fsub_rn(a, b)
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
-__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
-
-struct P3 {
-  float2 x, y, z;
-};
-__device__ __forceinline__ P3 pk3(float4 a, float4 b) { return P3{pk(a.x, b.x), pk(a.y, b.y), pk(a.z, b.z)}; }
-// ((a0 b0 + a1 b1) + a2 b2): dot3x without its trailing "+ 0", which can
-// change only the sign of a zero -- no comparison below can tell
-__device__ __forceinline__ float2 dot2(const P3 &a, const P3 &b) {
-  float2 s = mul2(a.x, b.x);
-  s = add2(s, mul2(a.y, b.y));
-  return add2(s, mul2(a.z, b.z));
-}
-// rows 0..2 of a 4x4 (as duplicated pairs A[0..11]) applied to a point (w = 1:
-// the "+ A3 * 1" of row4 adds A3 exactly) or to a normal (w = 0: "+ A3 * 0"
-// changes at most the sign of a zero)
-__device__ __forceinline__ float2 row2(const float2 *A, const P3 &v) {
-  float2 s = mul2(A[0], v.x);
-  s = add2(s, mul2(A[1], v.y));
-  return add2(s, mul2(A[2], v.z));
-}
-__device__ __forceinline__ P3 xform_point2(const float2 *A, const P3 &v) {
-  return P3{add2(row2(A, v), A[3]), add2(row2(A + 4, v), A[7]), add2(row2(A + 8, v), A[11])};
-}
-__device__ __forceinline__ P3 xform_normal2(const float2 *A, const P3 &v) {
-  return P3{row2(A, v), row2(A + 4, v), row2(A + 8, v)};
-}
-
-// The curvature-ratio gate of correspondencefinderprojective.cpp:84-96 for
-// one pixel (kr, kc: reference and current curvature).
-__device__ __forceinline__ bool ratio_ok(const CorrParams &cp, float kr, float kc) {
-  if (kr < cp.flat_thr) kr = cp.flat_thr;
-  if (kc < cp.flat_thr) kc = cp.flat_thr;
-  if (kr == kc) return true;  // ratio exactly 1
-  const float ratio = __double2float_rn(__ddiv_rn(__dadd_rn((double)kr, 1e-5), __dadd_rn((double)kc, 1e-5)));
-  return !(ratio < cp.min_ratio || ratio > cp.max_ratio);
-}
-
-// gate_t for two pixels at once (T2: the gating transform as duplicated
-// pairs); returns the decisions in okA / okB and the moved reference point
-// and normal (rn only when the normal gates run).
-__device__ __forceinline__ void gate2(const CorrParams &cp, const float2 *T2, const P3 &rp0, const P3 &rn0,
-                                      float krA, float krB, const P3 &cpt, const P3 &cn, float kcA, float kcB,
-                                      P3 &rp, P3 &rn, bool &okA, bool &okB) {
-  rp = xform_point2(T2, rp0);
-  const P3 d{sub2(cpt.x, rp.x), sub2(cpt.y, rp.y), sub2(cpt.z, rp.z)};
-  const float2 dd = dot2(d, d);
-  okA = !(dd.x > cp.sq_thr);
-  okB = !(dd.y > cp.sq_thr);
-  if (!cp.demoted) {
-    const float2 ncc = dot2(cn, cn), nrr = dot2(rn0, rn0);
-    rn = xform_normal2(T2, rn0);
-    const float2 cs = dot2(cn, rn);
-    okA = okA && !(ncc.x == 0.0f) && !(nrr.x == 0.0f) && !(cs.x < cp.cos_thr);
-    okB = okB && !(ncc.y == 0.0f) && !(nrr.y == 0.0f) && !(cs.y < cp.cos_thr);
-    okA = okA && ratio_ok(cp, krA, kcA);
-    okB = okB && ratio_ok(cp, krB, kcB);
-  }
-}
-
-// Accumulators of two pixel streams (A in .x, B in .y) for elements 0..27 of
-// Acc; the three counts (inliers, candidates, accepted -- at most 8 per thread
-// and tile each) share one word: bits 0-7, 8-15 and 16-23.
-struct Acc2 {
-  float2 v[28];
-  unsigned counts;
-};
-
-// lin_terms_structured_xf for two pixels.  mA / mB: 1 where the pixel was
-// accepted by the gate, 0 where it adds nothing (its inputs are finite, so
-// a zero weight zeroes every term exactly).  omd: (d0, d1) of the current
-// cloud's four information-matrix classes.
-__device__ __forceinline__ void lin_terms_structured_x2(const LinParams &lp, const float *omd, const P3 &rp,
-                                                       const P3 &rn, const P3 &cpt, float wA, float wB, const P3 &u,
-                                                       float mA, float mB, Acc2 &acc) {
-  float alA = 0.0f, beA = 0.0f, anA = 0.0f, bnA = 0.0f, alB = 0.0f, beB = 0.0f, anB = 0.0f, bnB = 0.0f;
-  if (point_has_normal(wA)) {
-    const int c = (int)wA - 1;
-    const float *dp = omd + 2 * (c & 1), *dn = omd + 4 + 2 * ((c >> 1) & 1);
-    alA = dp[1];
-    beA = dp[0] - dp[1];
-    anA = lp.scale * dn[1];
-    bnA = lp.scale * dn[0] - anA;
-  }
-  if (point_has_normal(wB)) {
-    const int c = (int)wB - 1;
-    const float *dp = omd + 2 * (c & 1), *dn = omd + 4 + 2 * ((c >> 1) & 1);
-    alB = dp[1];
-    beB = dp[0] - dp[1];
-    anB = lp.scale * dn[1];
-    bnB = lp.scale * dn[0] - anB;
-  }
-  float2 alp = pk(alA, alB), bep = pk(beA, beB), aln = pk(anA, anB), ben = pk(bnA, bnB);
-  if (lp.z_scaling) {
-    const float2 f = pk(1.0f / fabsf(cpt.z.x), 1.0f / fabsf(cpt.z.y));
-    alp = mul2(alp, f);
-    bep = mul2(bep, f);
-    aln = mul2(aln, f);
-    ben = mul2(ben, f);
-  }
-  if (lp.demoted) {
-    aln = pk(0.0f, 0.0f);
-    ben = aln;
-  }
-  const P3 pe{sub2(rp.x, cpt.x), sub2(rp.y, cpt.y), sub2(rp.z, cpt.z)};
-  const P3 ne{sub2(rn.x, u.x), sub2(rn.y, u.y), sub2(rn.z, u.z)};
-  const float2 up = fma2(u.z, pe.z, fma2(u.y, pe.y, mul2(u.x, pe.x)));
-  const float2 un = fma2(u.z, ne.z, fma2(u.y, ne.y, mul2(u.x, ne.x)));
-  const float2 bu = mul2(bep, up), bn_ = mul2(ben, un);
-  const P3 ep{fma2(bu, u.x, mul2(alp, pe.x)), fma2(bu, u.y, mul2(alp, pe.y)), fma2(bu, u.z, mul2(alp, pe.z))};
-  const P3 en{fma2(bn_, u.x, mul2(aln, ne.x)), fma2(bn_, u.y, mul2(aln, ne.y)), fma2(bn_, u.z, mul2(aln, ne.z))};
-  const float2 le = add2(fma2(pe.z, ep.z, fma2(pe.y, ep.y, mul2(pe.x, ep.x))),
-                         fma2(ne.z, en.z, fma2(ne.y, en.y, mul2(ne.x, en.x))));
-  // robust kernel (linearizer.cpp:80-87): weight max_chi2 / le beyond the
-  // threshold, or drop the correspondence when the kernel is off
-  float ksA = mA, ksB = mB, inA = mA, inB = mB;
-  if (le.x > lp.max_chi2) {
-    ksA = lp.robust ? mA * (lp.max_chi2 / le.x) : 0.0f;
-    inA = lp.robust ? mA : 0.0f;
-  }
-  if (le.y > lp.max_chi2) {
-    ksB = lp.robust ? mB * (lp.max_chi2 / le.y) : 0.0f;
-    inB = lp.robust ? mB : 0.0f;
-  }
-  const float2 ks = pk(ksA, ksB);
-  acc.v[27] = fma2(ks, le, acc.v[27]);
-  acc.counts += (unsigned)(inA + inB);
-  const float2 two = pk(2.0f, 2.0f);
-  const float2 a = mul2(two, rp.x), b = mul2(two, rp.y), c = mul2(two, rp.z);
-  const float2 an = mul2(two, rn.x), bn = mul2(two, rn.y), cn2 = mul2(two, rn.z);
-  const float2 ka = mul2(ks, alp), kb = mul2(ks, bep), kan = mul2(ks, aln), kbn = mul2(ks, ben);
-  // Htt += ks Omega_p
-  const float2 t0 = mul2(kb, u.x), t1 = mul2(kb, u.y), t2 = mul2(kb, u.z);
-  acc.v[0] = add2(acc.v[0], fma2(t0, u.x, ka));
-  acc.v[1] = fma2(t0, u.y, acc.v[1]);
-  acc.v[2] = add2(acc.v[2], fma2(t1, u.y, ka));
-  acc.v[3] = fma2(t0, u.z, acc.v[3]);
-  acc.v[4] = fma2(t1, u.z, acc.v[4]);
-  acc.v[5] = add2(acc.v[5], fma2(t2, u.z, ka));
-  // Htr += ks Omega_p S (S = [[0, c, -b], [-c, 0, a], [b, -a, 0]])
-  const float2 wp0 = sub2(mul2(b, u.z), mul2(c, u.y)), wp1 = sub2(mul2(c, u.x), mul2(a, u.z)),
-               wp2 = sub2(mul2(a, u.y), mul2(b, u.x));
-  const float2 wn0 = sub2(mul2(bn, u.z), mul2(cn2, u.y)), wn1 = sub2(mul2(cn2, u.x), mul2(an, u.z)),
-               wn2 = sub2(mul2(an, u.y), mul2(bn, u.x));
-  const float2 qa = mul2(ka, a), qb = mul2(ka, b), qc = mul2(ka, c);
-  acc.v[6] = fma2(t0, wp0, acc.v[6]);
-  acc.v[7] = fma2(t0, wp1, add2(acc.v[7], qc));
-  acc.v[8] = fma2(t0, wp2, sub2(acc.v[8], qb));
-  acc.v[9] = fma2(t1, wp0, sub2(acc.v[9], qc));
-  acc.v[10] = fma2(t1, wp1, acc.v[10]);
-  acc.v[11] = fma2(t1, wp2, add2(acc.v[11], qa));
-  acc.v[12] = fma2(t2, wp0, add2(acc.v[12], qb));
-  acc.v[13] = fma2(t2, wp1, sub2(acc.v[13], qa));
-  acc.v[14] = fma2(t2, wp2, acc.v[14]);
-  // Hrr += ka (|v|^2 I - v v^T) + kan (|vn|^2 I - vn vn^T) + kb wp wp^T + kbn wn wn^T
-  const float2 qan = mul2(kan, an), qbn = mul2(kan, bn), qcn = mul2(kan, cn2);
-  const float2 D = fma2(ka, fma2(c, c, fma2(b, b, mul2(a, a))), mul2(kan, fma2(cn2, cn2, fma2(bn, bn, mul2(an, an)))));
-  const float2 pw0 = mul2(kb, wp0), pw1 = mul2(kb, wp1), pw2 = mul2(kb, wp2);
-  const float2 nw0 = mul2(kbn, wn0), nw1 = mul2(kbn, wn1), nw2 = mul2(kbn, wn2);
-  const float2 nqa = pk(-qa.x, -qa.y), nqb = pk(-qb.x, -qb.y), nqc = pk(-qc.x, -qc.y);
-  const float2 nqan = pk(-qan.x, -qan.y), nqbn = pk(-qbn.x, -qbn.y), nqcn = pk(-qcn.x, -qcn.y);
-  acc.v[15] = fma2(nw0, wn0, fma2(pw0, wp0, fma2(nqan, an, fma2(nqa, a, add2(acc.v[15], D)))));
-  acc.v[16] = fma2(nw1, wn0, fma2(pw1, wp0, fma2(nqbn, an, fma2(nqb, a, acc.v[16]))));
-  acc.v[17] = fma2(nw1, wn1, fma2(pw1, wp1, fma2(nqbn, bn, fma2(nqb, b, add2(acc.v[17], D)))));
-  acc.v[18] = fma2(nw2, wn0, fma2(pw2, wp0, fma2(nqcn, an, fma2(nqc, a, acc.v[18]))));
-  acc.v[19] = fma2(nw2, wn1, fma2(pw2, wp1, fma2(nqcn, bn, fma2(nqc, b, acc.v[19]))));
-  acc.v[20] = fma2(nw2, wn2, fma2(pw2, wp2, fma2(nqcn, cn2, fma2(nqc, c, add2(acc.v[20], D)))));
-  // bt += ks ep; br += ks (S^T ep + Sn^T en), S^T e = (2v) x e
-  acc.v[21] = fma2(ks, ep.x, acc.v[21]);
-  acc.v[22] = fma2(ks, ep.y, acc.v[22]);
-  acc.v[23] = fma2(ks, ep.z, acc.v[23]);
-  const float2 r0 = add2(sub2(mul2(b, ep.z), mul2(c, ep.y)), sub2(mul2(bn, en.z), mul2(cn2, en.y)));
-  const float2 r1 = add2(sub2(mul2(c, ep.x), mul2(a, ep.z)), sub2(mul2(cn2, en.x), mul2(an, en.z)));
-  const float2 r2 = add2(sub2(mul2(a, ep.y), mul2(b, ep.x)), sub2(mul2(an, en.y), mul2(bn, en.x)));
-  acc.v[24] = fma2(ks, r0, acc.v[24]);
-  acc.v[25] = fma2(ks, r1, acc.v[25]);
-  acc.v[26] = fma2(ks, r2, acc.v[26]);
-}
-
 // Reduces every thread's Acc to one FP64 partial of the CTA (fixed order).
 template <int kThreads>
 __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) {
@@ -527,39 +339,6 @@ __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) 
   for (int k = 0; k < 31; k++) v[k] = (double)acc.v[k];
   v[31] = 0.0;
   // butterfly reduce-scatter: lane L ends with the warp total of element L
-#pragma unroll
-  for (int off = 16; off >= 1; off >>= 1) {
-    bool upper = (lane & off) != 0;
-#pragma unroll
-    for (int j = 0; j < off; j++) {
-      double send = upper ? v[j] : v[j + off];
-      double keep = upper ? v[j + off] : v[j];
-      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
-    }
-  }
-  wsum[wid][lane] = v[0];
-  __syncthreads();
-  if (wid == 0) {
-    double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; w++) s += wsum[w][lane];
-    out[lane] = s;
-  }
-}
-
-// block_reduce_store for two pixel streams: each element enters the FP64
-// reduction as (double)A + (double)B.
-template <int kThreads>
-__device__ __forceinline__ void block_reduce_store2(const Acc2 &acc, double *out) {
-  __shared__ double wsum[kThreads / 32][32];
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double v[32];
-#pragma unroll
-  for (int k = 0; k < 28; k++) v[k] = (double)acc.v[k].x + (double)acc.v[k].y;
-  v[28] = (double)(acc.counts & 255u);
-  v[29] = (double)((acc.counts >> 8) & 255u);
-  v[30] = (double)((acc.counts >> 16) & 255u);
-  v[31] = 0.0;
 #pragma unroll
   for (int off = 16; off >= 1; off >>= 1) {
     bool upper = (lane & off) != 0;
@@ -605,16 +384,11 @@ constexpr int kCorrStages = 3;  // general Omega: gather, gate + Omega gather, l
 // Structure-of-arrays stage: thread t owns slots t + k kFusedThreads of
 // every array, so a warp's accesses to one field are consecutive 16-byte
 // words (no bank conflicts).
-// Structured Omega (rebuilt from the current normal): a warp's candidate
-// pixels are compacted into its 2 x 32 slots (nwarp[w] of them, in pixel
-// order), so that lane l linearizes slots l and l + 32 as one packed pair.
-struct GatherStageS {
-  float4 rp[kSubPix], rn[kSubPix], cp[kSubPix], cn[kSubPix];
-  int nwarp[kFusedThreads / 32];
-};
-struct GatherStageG {  // general Omega: gathered for accepted pixels
+struct GatherStageS {  // structured Omega: rebuilt from the current normal
   float4 rp[kSubPix], rn[kSubPix], cp[kSubPix], cn[kSubPix];
   int valid[kSubPix];
+};
+struct GatherStageG : GatherStageS {  // general Omega: gathered for accepted pixels
   float4 o0[kSubPix], o1[kSubPix], o2[kSubPix];
   int ci[kSubPix];
 };
@@ -655,7 +429,6 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   // [0..11] gating T, [12..23] linearizer T, [24..31] the current cloud's
   // Omega parameters, then pair index, skip flag and structured-Omega flag
   __shared__ float sT[2][32];
-  __shared__ float2 sT2[2][24];  // the two transforms as (v, v) pairs for the packed gate and linearizer
   __shared__ int sPair[2], sSkip[2], sStruct[2], sSame[2];
   const bool stats_pass = flags & 8;
   if ((int)blockIdx.x >= total_tiles) return;
@@ -710,19 +483,16 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   // gather points and normals of both clouds.
   auto issue_g1 = [&](int j) {
     Stage &g = stage_of(j);
-    int ri[kFusedPX], ci[kFusedPX], valid[kFusedPX];
+    int ci[kFusedPX], valid[kFusedPX];
 #pragma unroll
     for (int k = 0; k < kFusedPX; k++) {
-      ri[k] = -1;
       ci[k] = -1;
       valid[k] = 0;
     }
-    const PairDev *gpd = pairs;
     if (j < nsub) {
       int tile = tile_of(j);
       lookup(tile, gt_tile, gt_pi, gt_skip);
       const PairDev &pd = pairs[gt_pi];
-      gpd = &pd;
       if (!gt_skip) {
         if (gt_ctile != tile) {  // point counts, read once per tile
           gt_ctile = tile;
@@ -733,58 +503,35 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
         const int p0 = (tile - pd.tile_base) * kCorrTilePixels + (j % kSubsPerTile) * kSubPix + t;
 #pragma unroll
         for (int k = 0; k < kFusedPX; k++) {
-          const int p = p0 + k * kFusedThreads;
+          const int p = p0 + k * kFusedThreads, sl = t + k * kFusedThreads;
           if (p < P) {
+            int ri;
             if (flags & 1) {
-              ri[k] = zbuf_index(zI[k], drop_no_normal);
+              ri = zbuf_index(zI[k], drop_no_normal);
               ci[k] = cI[k];
               if (flags & 2) pd.zbuf[p] = ~0ull;
-              if (flags & 4) pd.ref_index[p] = ri[k];
+              if (flags & 4) pd.ref_index[p] = ri;
             } else {
-              ri[k] = cI[k];
+              ri = cI[k];
               ci[k] = (int)(unsigned)zI[k];
             }
-            valid[k] = ri[k] >= 0 && ci[k] >= 0 && ri[k] < gt_rc && ci[k] < gt_cc;
+            valid[k] = ri >= 0 && ci[k] >= 0 && ri < gt_rc && ci[k] < gt_cc;
             if (valid[k] && cp.row_limit_threads > 1)
               valid[k] = p / pd.cols < (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
+            if (valid[k]) {
+              cp_async16(&g.rp[sl], pd.ref_pts + ri);
+              cp_async16(&g.rn[sl], pd.ref_nrm + ri);
+              cp_async16(&g.cp[sl], pd.cur_pts + ci[k]);
+              cp_async16(&g.cn[sl], pd.cur_nrm + ci[k]);
+            }
           }
         }
       }
     }
-    if constexpr (kStructured) {
-      // compact the warp's candidates (pixel order: slot-0 pixels, then
-      // slot-1 pixels) into its 64 slots; the warp's lanes must be done
-      // reading this stage's slots (consumed two sub-tiles ago) first
-      __syncwarp();
-      const int lane = t & 31, w = t >> 5;
-      const unsigned lt = (1u << lane) - 1u;
-      int base = 0;
 #pragma unroll
-      for (int k = 0; k < kFusedPX; k++) {
-        const unsigned m = __ballot_sync(0xffffffffu, valid[k]);
-        if (valid[k]) {
-          const int sl = w * 32 * kFusedPX + base + __popc(m & lt);
-          cp_async16(&g.rp[sl], gpd->ref_pts + ri[k]);
-          cp_async16(&g.rn[sl], gpd->ref_nrm + ri[k]);
-          cp_async16(&g.cp[sl], gpd->cur_pts + ci[k]);
-          cp_async16(&g.cn[sl], gpd->cur_nrm + ci[k]);
-        }
-        base += __popc(m);
-      }
-      if (lane == 0) g.nwarp[w] = base;
-    } else {
-#pragma unroll
-      for (int k = 0; k < kFusedPX; k++) {
-        const int sl = t + k * kFusedThreads;
-        if (valid[k]) {
-          cp_async16(&g.rp[sl], gpd->ref_pts + ri[k]);
-          cp_async16(&g.rn[sl], gpd->ref_nrm + ri[k]);
-          cp_async16(&g.cp[sl], gpd->cur_pts + ci[k]);
-          cp_async16(&g.cn[sl], gpd->cur_nrm + ci[k]);
-        }
-        g.ci[sl] = ci[k];
-        g.valid[sl] = valid[k];
-      }
+    for (int k = 0; k < kFusedPX; k++) {
+      if constexpr (!kStructured) g.ci[t + k * kFusedThreads] = ci[k];
+      g.valid[t + k * kFusedThreads] = valid[k];
     }
     cp_async_commit();
   };
@@ -796,12 +543,10 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
     lookup(tile_of(j), gt_tile, gt_pi, gt_skip);
     const int pi = gt_pi;
     const PairState *st = pairs[pi].state;
-    if (threadIdx.x < 24) {
-      const float v = threadIdx.x < 12 ? (stats_pass ? st->Tgate_used : st->Tgate)[threadIdx.x]
-                                       : st->Tlin[threadIdx.x - 12];
-      sT[e][threadIdx.x] = v;
-      sT2[e][threadIdx.x] = make_float2(v, v);
-    } else if (threadIdx.x < 32)
+    if (threadIdx.x < 24)
+      sT[e][threadIdx.x] = threadIdx.x < 12 ? (stats_pass ? st->Tgate_used : st->Tgate)[threadIdx.x]
+                                            : st->Tlin[threadIdx.x - 12];
+    else if (threadIdx.x < 32)
       sT[e][threadIdx.x] = pairs[pi].cur_omd[threadIdx.x - 24];
     if (threadIdx.x == 0) {
       sPair[e] = pi;
@@ -827,13 +572,14 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
         // linearizer in the main step
         cp_async_commit();
         return;
-      } else {
+      }
 #pragma unroll
-        for (int k = 0; k < kFusedPX; k++) {
-          const int sl = t + k * kFusedThreads;
-          acc_ok = 0;
-          if (g.valid[sl] && !sSkip[e]) {
-            acc_ok = gate(cp, sT[e], g.rp[sl], g.rn[sl], g.cp[sl], g.cn[sl]) ? 2 : 1;
+      for (int k = 0; k < kFusedPX; k++) {
+        const int sl = t + k * kFusedThreads;
+        acc_ok = 0;
+        if (g.valid[sl] && !sSkip[e]) {
+          acc_ok = gate(cp, sT[e], g.rp[sl], g.rn[sl], g.cp[sl], g.cn[sl]) ? 2 : 1;
+          if constexpr (!kStructured) {
             if (acc_ok == 2 && !sStruct[e]) {
               const float4 *o = pairs[sPair[e]].cur_omg + 3 * (size_t)g.ci[sl];
               cp_async16(&g.o0[sl], o);
@@ -841,20 +587,16 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
               cp_async16(&g.o2[sl], o + 2);
             }
           }
-          g.valid[sl] = acc_ok;  // 0 none, 1 candidate rejected, 2 accepted
         }
+        g.valid[sl] = acc_ok;  // 0 none, 1 candidate rejected, 2 accepted
       }
     }
     cp_async_commit();
   };
 
-  Acc acc;    // general Omega: one pixel at a time
-  Acc2 acc2;  // structured Omega: two pixels per packed instruction
+  Acc acc;
 #pragma unroll
   for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
-#pragma unroll
-  for (int k = 0; k < 28; k++) acc2.v[k] = make_float2(0.0f, 0.0f);
-  acc2.counts = 0u;
   // Linearizes sub-tile j (its gather -- and, for general Omega, its gate --
   // complete); at a tile's last sub-tile the CTA stores the tile's partial.
   auto consume = [&](int j) {
@@ -863,44 +605,27 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
     if (sub == 0) {
 #pragma unroll
       for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
-#pragma unroll
-      for (int k = 0; k < 28; k++) acc2.v[k] = make_float2(0.0f, 0.0f);
-      acc2.counts = 0u;
     }
     if (!sSkip[e]) {
       const Stage &g = stage_of(j);
-      if constexpr (kStructured) {
-        // lane l: the warp's compacted candidates l (A) and l + 32 (B); a
-        // lane without a B candidate repeats A's inputs with a zero weight
-        const int lane = t & 31, w = t >> 5;
-        const int n = g.nwarp[w];
-        if (lane < n) {
-          const int sA = w * 32 * kFusedPX + lane;
-          const bool hasB = lane + 32 < n;
-          const int sB = hasB ? sA + 32 : sA;
-          const float4 rpA = g.rp[sA], rnA = g.rn[sA], cpA = g.cp[sA], cnA = g.cn[sA];
-          const float4 rpB = g.rp[sB], rnB = g.rn[sB], cpB = g.cp[sB], cnB = g.cn[sB];
-          const P3 rp0 = pk3(rpA, rpB), rn0 = pk3(rnA, rnB), cpt = pk3(cpA, cpB), cn = pk3(cnA, cnB);
-          P3 rp, rn;
-          bool okA, okB;
-          gate2(cp, sT2[e], rp0, rn0, rnA.w, rnB.w, cpt, cn, cnA.w, cnB.w, rp, rn, okA, okB);
-          okB = okB && hasB;
-          acc2.counts += (hasB ? 2u : 1u) << 8;
-          if (okA || okB) {
-            acc2.counts += ((okA ? 1u : 0u) + (okB ? 1u : 0u)) << 16;
-            if (!(sSame[e] && !cp.demoted)) {  // the linearizer's own transform: inputs reloaded
-              rp = xform_point2(sT2[e] + 12, pk3(g.rp[sA], g.rp[sB]));
-              rn = xform_normal2(sT2[e] + 12, pk3(g.rn[sA], g.rn[sB]));
-            }
-            lin_terms_structured_x2(lp, sT[e] + 24, rp, rn, cpt, cpA.w, cpB.w, cn, okA ? 1.0f : 0.0f,
-                                    okB ? 1.0f : 0.0f, acc2);
-          }
-        }
-      } else {
 #pragma unroll
-        for (int k = 0; k < kFusedPX; k++) {
-          const int sl = t + k * kFusedThreads;
-          const int v = g.valid[sl];
+      for (int k = 0; k < kFusedPX; k++) {
+        const int sl = t + k * kFusedThreads;
+        const int v = g.valid[sl];
+        if constexpr (kStructured) {
+          if (v) {
+            acc.v[29] += 1.0f;
+            const float4 rp0 = g.rp[sl], rn0 = g.rn[sl], cpt = g.cp[sl], cn = g.cn[sl];
+            float3 rp, rn;
+            if (gate_t(cp, sT[e], rp0, rn0, cpt, cn, rp, rn)) {
+              acc.v[30] += 1.0f;
+              if (sSame[e] && !cp.demoted)
+                lin_terms_structured_xf(lp, sT[e] + 24, rp, rn, cpt, cn, acc);
+              else
+                lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, rp0, rn0, cpt, cn, acc);
+            }
+          }
+        } else {
           if (v) acc.v[29] += 1.0f;
           if (v == 2) {
             acc.v[30] += 1.0f;
@@ -914,9 +639,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
       }
       if (sub == kSubsPerTile - 1) {
         const PairDev &pd = pairs[sPair[e]];
-        double *out = pd.partials + (size_t)(tile_of(j) - pd.tile_base) * kPartialWords;
-        if constexpr (kStructured) block_reduce_store2<kFusedThreads>(acc2, out);
-        else block_reduce_store<kFusedThreads>(acc, out);
+        block_reduce_store<kFusedThreads>(acc, pd.partials + (size_t)(tile_of(j) - pd.tile_base) * kPartialWords);
       }
     }
   };
@@ -932,7 +655,6 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
       load_indices(j + 2);
       __syncthreads();        // tile constants visible
       cp_async_wait<1>();     // G1(j) complete (G1(j+1) may be in flight)
-      __syncwarp();           // ... for every lane of the warp (compacted slots are read by other lanes)
       consume(j);
     }
   } else {
