@@ -455,9 +455,9 @@ int nicp_align_batch(nicp_ctx *ctx, int n, const nicp_cloud *const *refs,
  * keyframe is replaced by the current frame when inliers fall below
  * keyframe_min_inlier_ratio x the keyframe's points (points with a normal);
  * the first frame of a stream becomes its keyframe (result T = identity).
- * Each alignment starts from the stream's previous estimate against the
- * same keyframe (identity right after a replacement), the constant-position
- * guess of a tracker. */
+ * Each alignment starts from a constant-velocity prediction against the
+ * same keyframe: last * prev^-1 * last over the stream's last two estimates
+ * (the last estimate after one, the identity right after a replacement). */
 typedef struct nicp_server nicp_server;
 
 typedef struct {

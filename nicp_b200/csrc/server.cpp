@@ -67,7 +67,49 @@ struct StreamState {
   int key_rows = 0, key_cols = 0;
   nicp_camera key_cam{};
   int key_points = 0;  // keyframe points with a normal
-  float guess[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};  // last estimate against the keyframe
+  // the last two estimates against the keyframe (frame -> keyframe) and
+  // how many there are since the keyframe was set (at most 2 kept)
+  double last[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  double prev[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  int estimates = 0;
+  // Initial guess of the next frame: a constant-velocity prediction,
+  // last * prev^-1 * last (the motion between the last two frames applied
+  // once more), with one estimate the last one, with none the identity.
+  void guess(float *g) const {
+    double G[16];
+    if (estimates >= 2) {
+      double pi[16], m[16];
+      iso_inverse(prev, pi);
+      mm4(last, pi, m);
+      mm4(m, last, G);
+    } else {
+      for (int k = 0; k < 16; k++) G[k] = estimates ? last[k] : (k % 5 == 0 ? 1.0 : 0.0);
+    }
+    for (int k = 0; k < 16; k++) g[k] = (float)G[k];
+    g[12] = g[13] = g[14] = 0.0f;
+    g[15] = 1.0f;
+  }
+  void push(const double *T) {
+    std::memcpy(prev, last, sizeof(last));
+    std::memcpy(last, T, sizeof(last));
+    estimates = std::min(estimates + 1, 2);
+  }
+  void reset() { estimates = 0; }
+  static void mm4(const double *A, const double *B, double *C) {
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 4; j++) {
+        double s = 0;
+        for (int k = 0; k < 4; k++) s += A[i * 4 + k] * B[k * 4 + j];
+        C[i * 4 + j] = s;
+      }
+  }
+  static void iso_inverse(const double *T, double *R) {
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) R[i * 4 + j] = T[j * 4 + i];
+    for (int i = 0; i < 3; i++) R[i * 4 + 3] = -(R[i * 4 + 0] * T[3] + R[i * 4 + 1] * T[7] + R[i * 4 + 2] * T[11]);
+    R[12] = R[13] = R[14] = 0;
+    R[15] = 1;
+  }
   bool busy = false;
 };
 
@@ -205,7 +247,9 @@ void nicp_server::worker(int w) {
           refs.push_back(ss.keyframe);
           curs.push_back(cur_clouds[i]);
           pcams.push_back(cams[i]);
-          guesses.insert(guesses.end(), ss.guess, ss.guess + 16);
+          float g[16];
+          ss.guess(g);
+          guesses.insert(guesses.end(), g, g + 16);
         }
       }
     }
@@ -239,7 +283,7 @@ void nicp_server::worker(int w) {
           r.inliers = a.inliers;
           r.keyframe_points = ss.key_points;
           replace = (double)a.inliers < (double)prm.keyframe_min_inlier_ratio * ss.key_points;
-          for (int k = 0; k < 16; k++) ss.guess[k] = (float)a.T[k];  // the next frame starts from here
+          ss.push(a.T);  // the next frame's guess builds on this estimate
         }
         size_t px = (size_t)rq.rows * rq.cols;
         if (rc == NICP_OK && replace) {
@@ -252,7 +296,7 @@ void nicp_server::worker(int w) {
           ss.key_cols = rq.cols;
           ss.key_cam = rq.cam;
           ss.key_points = cur_counts[i];
-          for (int k = 0; k < 16; k++) ss.guess[k] = (k % 5 == 0) ? 1.0f : 0.0f;
+          ss.reset();
           keyframe_bytes += kKeyframeBytesPerPixel * px;
           r.keyframe_replaced = 1;
         } else if (cur_clouds[i]) {
