@@ -699,7 +699,8 @@ struct FrameIn {
 // and returns the fastest.  The kernel writes the same outputs under every
 // shape; only its count of points with a normal accumulates, so that count
 // is zeroed before each run (and before the real run that follows).
-static int tune_stats(nicp_ctx *ctx, int precision, const FrameDev *dfr, int nf, int max_pixels, int *best) {
+static int tune_stats(nicp_ctx *ctx, int precision, bool lean, const FrameDev *dfr, int nf, int max_pixels,
+                      int *best) {
   cudaStream_t s = ctx->stream;
   cudaEvent_t e0, e1;
   CK(ctx, cudaEventCreate(&e0));
@@ -713,7 +714,7 @@ static int tune_stats(nicp_ctx *ctx, int precision, const FrameDev *dfr, int nf,
     for (int shape = 0; shape < kStatsShapes; shape++) {
       launch_reset_normal_counts(dfr, nf, s);
       cudaEventRecord(e0, s);
-      launch_stats(precision, dfr, nf, max_pixels, shape, s, &ctx->prof);
+      launch_stats(precision, dfr, nf, max_pixels, shape, lean, s, &ctx->prof);
       cudaEventRecord(e1, s);
       float ms = 0;
       cudaError_t e = cudaEventSynchronize(e1);
@@ -989,6 +990,11 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     launch_unproject(dfr, nf, g.tiles, ft, s, &ctx->prof);
     if (!unproject_only) {
       launch_moments(prm->moments_precision, dfr, nf, g.bands, g.carryctas, g.max_bands, fb, fk, s, &ctx->prof);
+      // only the smallest eigenpair is needed unless Stats are kept or an
+      // information matrix has distinct second and third diagonal entries
+      const bool lean = !prm->keep_stats && prm->pim_flat[1] == prm->pim_flat[2] &&
+                        prm->pim_nonflat[1] == prm->pim_nonflat[2] && prm->nim_flat[1] == prm->nim_flat[2] &&
+                        prm->nim_nonflat[1] == prm->nim_nonflat[2];
       int shape = 0;
       if (ctx->autotune) {
         // the chunk's frame sizes and the moment precision select the shape
@@ -1000,7 +1006,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
                  std::to_string(h.second) + " ";
         auto it = ctx->stats_tuned.find(key);
         if (it == ctx->stats_tuned.end()) {
-          int best = 0, rc = tune_stats(ctx, prm->moments_precision, dfr, nf, g.max_pixels, &best);
+          int best = 0, rc = tune_stats(ctx, prm->moments_precision, lean, dfr, nf, g.max_pixels, &best);
           if (rc) {
             if (any_staged) cudaStreamSynchronize(ctx->copy_stream);
             return rc;
@@ -1010,7 +1016,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
         shape = it->second;
       }
       ctx->stats_shape = shape;
-      launch_stats(prm->moments_precision, dfr, nf, g.max_pixels, shape, s, &ctx->prof);
+      launch_stats(prm->moments_precision, dfr, nf, g.max_pixels, shape, lean, s, &ctx->prof);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail_staged(e, "build launch");
   }

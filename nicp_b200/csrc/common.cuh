@@ -303,16 +303,20 @@ __device__ inline void d_plane_vector(const double *B, const double *e, double m
 // eigenvalues are m + 2 p cos(phi + 2 pi k / 3), phi = acos(det((B - m I) / p) / 2) / 3;
 // the largest (k = 0) and the smallest (k = 1) come from one sincos:
 // cos(phi + 2 pi / 3) = -cos(phi) / 2 - sin(phi) sqrt(3) / 2.
-__device__ inline void d_eig3(const double *A, double *lam, double *U) {
-  double amax = fabs(A[0]);
+// The eigenvalues of a symmetric 3x3 A (lower triangle 00 10 11 20 21 22 as
+// 00 01 02 11 12 22): returns true with lam and U filled for the degenerate
+// cases (A = 0, or A a multiple of the identity); otherwise false with B =
+// A / amax and its ascending eigenvalues l0 <= l1 <= l2 (of B).
+__device__ inline bool d_eig3_values(const double *A, double *B, double &amax, double &l0, double &l1, double &l2,
+                                     double *lam, double *U) {
+  amax = fabs(A[0]);
   for (int i = 1; i < 6; i++) amax = fmax(amax, fabs(A[i]));
   if (!(amax > 0.0)) {
     lam[0] = lam[1] = lam[2] = 0;
     for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? 1.0 : 0.0;
-    return;
+    return true;
   }
   const double is = 1.0 / amax;
-  double B[6];
   for (int i = 0; i < 6; i++) B[i] = A[i] * is;
   const double third = 1.0 / 3.0;
   const double m = (B[0] + B[3] + B[5]) * third;
@@ -322,7 +326,7 @@ __device__ inline void d_eig3(const double *A, double *lam, double *U) {
   if (!(p2 > 0.0)) {
     lam[0] = lam[1] = lam[2] = m * amax;
     for (int i = 0; i < 9; i++) U[i] = (i % 4 == 0) ? 1.0 : 0.0;
-    return;
+    return true;
   }
   const double p26 = p2 * (1.0 / 6.0);
   const double ip = rsqrt(p26), p = p26 * ip;
@@ -333,14 +337,21 @@ __device__ inline void d_eig3(const double *A, double *lam, double *U) {
   double sphi, cphi;
   sincos(phi, &sphi, &cphi);
   const double half_sqrt3 = 0.86602540378443864676;
-  double l2 = m + 2.0 * p * cphi;
-  double l0 = m - p * cphi - 2.0 * half_sqrt3 * p * sphi;
-  double l1 = 3.0 * m - l0 - l2;
+  l2 = m + 2.0 * p * cphi;
+  l0 = m - p * cphi - 2.0 * half_sqrt3 * p * sphi;
+  l1 = 3.0 * m - l0 - l2;
   double t;
   if (l1 < l0) { t = l1; l1 = l0; l0 = t; }
   if (l2 < l1) { t = l2; l2 = l1; l1 = t; }
   if (l1 < l0) { t = l1; l1 = l0; l0 = t; }
-  double v0[3], v1[3], v2[3];
+  return false;
+}
+
+// The orthonormal eigenvectors of B for its eigenvalues l0 <= l1 <= l2: the
+// best separated end eigenvalue's vector from a null vector, the middle one
+// in the plane orthogonal to it, the third by a cross product.
+__device__ inline void d_eig3_vectors(const double *B, double l0, double l1, double l2, double *v0, double *v1,
+                                      double *v2) {
   if (l1 - l0 >= l2 - l1) {
     d_null_vector(B, l0, v0);
     d_plane_vector(B, v0, l1, v1);
@@ -350,6 +361,13 @@ __device__ inline void d_eig3(const double *A, double *lam, double *U) {
     d_plane_vector(B, v2, l1, v1);
     d_cross(v1, v2, v0);
   }
+}
+
+__device__ inline void d_eig3(const double *A, double *lam, double *U) {
+  double B[6], amax, l0, l1, l2;
+  if (d_eig3_values(A, B, amax, l0, l1, l2, lam, U)) return;
+  double v0[3], v1[3], v2[3];
+  d_eig3_vectors(B, l0, l1, l2, v0, v1, v2);
   lam[0] = l0 * amax; lam[1] = l1 * amax; lam[2] = l2 * amax;
   for (int r = 0; r < 3; r++) { U[r * 3 + 0] = v0[r]; U[r * 3 + 1] = v1[r]; U[r * 3 + 2] = v2[r]; }
 }

@@ -600,7 +600,9 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const Fra
 // One thread per pixel: the CTA size and the CTAs per SM the compiler
 // budgets registers for are launch shapes only (the autotuner picks one per
 // frame-size mix); every pixel's result is the same under all of them.
-template <class M, int kThreads, int kMinCtas>
+// kLean: Stats are not kept and the information matrices have the
+// converter's form U diag(d0, d1, d1) U^T (decided on the host for the launch).
+template <class M, int kThreads, int kMinCtas, bool kLean>
 __global__ void __launch_bounds__(kThreads, kMinCtas) k_stats(const FrameDev *__restrict__ frames, int nframes) {
   const FrameDev &f = frames[blockIdx.y];
   int pix = blockIdx.x * kThreads + threadIdx.x;
@@ -652,18 +654,39 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) k_stats(const FrameDev *__
       double C[6] = {S[4] * dn - mu0 * mu0, S[5] * dn - mu0 * mu1, S[6] * dn - mu0 * mu2,
                      S[7] * dn - mu1 * mu1, S[8] * dn - mu1 * mu2, S[9] * dn - mu2 * mu2};
       // FP64 solve.  (An FP32 trigonometric solve refined in FP64 was
-      // measured: no faster -- this kernel is bound by its 40 scattered FP64
-      // moment reads per pixel, not by the eigensolve -- and its refinement
-      // could still settle on the wrong root when the two smallest
-      // eigenvalues are close.)
-      d_eig3(C, lam, U);
+      // measured: no faster, and its refinement could settle on the wrong
+      // root when the two smallest eigenvalues are close.)  Without kept
+      // Stats and with information matrices of the converter's form
+      // U diag(d0, d1, d1) U^T, only the smallest eigenpair matters: the
+      // eigenvalues come first, and the normal's eigenvector is computed only
+      // for a flat pixel, from its null vector when the smallest eigenvalue is
+      // the better separated one -- the same arithmetic as the full solve, so
+      // the normal is bitwise the full solve's.
+      constexpr bool lean = kLean;
+      double B[6], amax = 1.0, l0 = 0, l1 = 0, l2 = 0;
+      bool degenerate = true;
+      if (lean) {
+        degenerate = d_eig3_values(C, B, amax, l0, l1, l2, lam, U);
+        if (!degenerate) { lam[0] = l0 * amax; lam[1] = l1 * amax; lam[2] = l2 * amax; }
+      } else {
+        d_eig3(C, lam, U);
+      }
       if (lam[0] < 0) lam[0] = 0;
       reached = true;
       double kappa = lam[0] / (((lam[0] + lam[1]) + lam[2]) + 1e-9);
       nout.w = (float)kappa;
       if (kappa < (double)f.curv_thr) {
+        double u0[3] = {U[0], U[3], U[6]};
+        if (lean && !degenerate) {
+          if (l1 - l0 >= l2 - l1) {
+            d_null_vector(B, l0, u0);
+          } else {
+            double v1[3], v2[3];
+            d_eig3_vectors(B, l0, l1, l2, u0, v1, v2);
+          }
+        }
         float4 p = unproject_pixel(f.iKRt, c, r, d);
-        double nx = U[0], ny = U[3], nz = U[6];
+        double nx = u0[0], ny = u0[1], nz = u0[2];
         if (nx * p.x + ny * p.y + nz * p.z > 0) { nx = -nx; ny = -ny; nz = -nz; }
         nout.x = (float)nx; nout.y = (float)ny; nout.z = (float)nz;
         // information matrices: Omega = U diag(D) U^T
@@ -675,18 +698,29 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) k_stats(const FrameDev *__
         }
         omega_class = (kappa < (double)f.pim_thr ? 0 : 1) + (kappa < (double)f.nim_thr ? 0 : 2);
         const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
+        if (lean) {
+          // U diag(d0, d1, d1) U^T = d1 I + (d0 - d1) u0 u0^T
 #pragma unroll
-        for (int e = 0; e < 6; e++) {
-          int i = ii[e], j = jj[e];
-          double sp = 0, sn = 0;
-#pragma unroll
-          for (int k = 0; k < 3; k++) {
-            double uu = U[i * 3 + k] * U[j * 3 + k];
-            sp += Dp[k] * uu;
-            sn += Dn[k] * uu;
+          for (int e = 0; e < 6; e++) {
+            const int i = ii[e], j = jj[e];
+            const double uu = u0[i] * u0[j];
+            om[e] = (float)((i == j ? Dp[1] : 0.0) + (Dp[0] - Dp[1]) * uu);
+            om[6 + e] = (float)((i == j ? Dn[1] : 0.0) + (Dn[0] - Dn[1]) * uu);
           }
-          om[e] = (float)sp;
-          om[6 + e] = (float)sn;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 6; e++) {
+            int i = ii[e], j = jj[e];
+            double sp = 0, sn = 0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              double uu = U[i * 3 + k] * U[j * 3 + k];
+              sp += Dp[k] * uu;
+              sn += Dn[k] * uu;
+            }
+            om[e] = (float)sp;
+            om[6 + e] = (float)sn;
+          }
         }
       }
     }
@@ -994,25 +1028,31 @@ static const int kStatsShape[kStatsShapes][2] = {{256, 3}, {128, 6}, {64, 12}, {
 int stats_shape_threads(int shape) { return kStatsShape[shape][0]; }
 int stats_shape_min_ctas(int shape) { return kStatsShape[shape][1]; }
 
-template <class M>
+template <class M, bool kLean>
 static void stats_launch(int shape, dim3 g, const FrameDev *d_frames, int nframes, cudaStream_t s) {
   switch (shape) {
-    case 1: k_stats<M, 128, 6><<<g, 128, 0, s>>>(d_frames, nframes); break;
-    case 2: k_stats<M, 64, 12><<<g, 64, 0, s>>>(d_frames, nframes); break;
-    case 3: k_stats<M, 256, 2><<<g, 256, 0, s>>>(d_frames, nframes); break;
-    default: k_stats<M, 256, 3><<<g, 256, 0, s>>>(d_frames, nframes); break;
+    case 1: k_stats<M, 128, 6, kLean><<<g, 128, 0, s>>>(d_frames, nframes); break;
+    case 2: k_stats<M, 64, 12, kLean><<<g, 64, 0, s>>>(d_frames, nframes); break;
+    case 3: k_stats<M, 256, 2, kLean><<<g, 256, 0, s>>>(d_frames, nframes); break;
+    default: k_stats<M, 256, 3, kLean><<<g, 256, 0, s>>>(d_frames, nframes); break;
   }
 }
 
-void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_pixels, int shape, cudaStream_t s,
-                  Profiler *prof) {
+template <class M>
+static void stats_launch(int shape, bool lean, dim3 g, const FrameDev *d_frames, int nframes, cudaStream_t s) {
+  if (lean) stats_launch<M, true>(shape, g, d_frames, nframes, s);
+  else stats_launch<M, false>(shape, g, d_frames, nframes, s);
+}
+
+void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_pixels, int shape, bool lean,
+                  cudaStream_t s, Profiler *prof) {
   if (shape < 0 || shape >= kStatsShapes) shape = 0;
   prof->begin(NICP_K_STATS, s);
   const int threads = kStatsShape[shape][0];
   const dim3 g((max_pixels + threads - 1) / threads, nframes);
-  if (precision == NICP_MOMENTS_F32) stats_launch<MomF32>(shape, g, d_frames, nframes, s);
-  else if (precision == NICP_MOMENTS_TWOFLOAT) stats_launch<MomTwoFloat>(shape, g, d_frames, nframes, s);
-  else stats_launch<MomF64>(shape, g, d_frames, nframes, s);
+  if (precision == NICP_MOMENTS_F32) stats_launch<MomF32>(shape, lean, g, d_frames, nframes, s);
+  else if (precision == NICP_MOMENTS_TWOFLOAT) stats_launch<MomTwoFloat>(shape, lean, g, d_frames, nframes, s);
+  else stats_launch<MomF64>(shape, lean, g, d_frames, nframes, s);
   prof->end(NICP_K_STATS, s);
 }
 

@@ -82,8 +82,10 @@ void launch_moments(int precision, const FrameDev *d_frames, int nframes, int to
 constexpr int kStatsShapes = 4;  // k_stats launch shapes the autotuner chooses from (0: default)
 int stats_shape_threads(int shape);
 int stats_shape_min_ctas(int shape);
-void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_pixels, int shape, cudaStream_t s,
-                  Profiler *prof);
+// lean: no Stats kept and information matrices U diag(d0, d1, d1) U^T (only
+// the smallest eigenpair is computed).
+void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_pixels, int shape, bool lean,
+                  cudaStream_t s, Profiler *prof);
 void launch_reset_normal_counts(const FrameDev *d_frames, int nframes, cudaStream_t s);
 void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,
                             int capacity, const float *d_m12, cudaStream_t s, Profiler *prof);
