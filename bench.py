@@ -598,14 +598,28 @@ def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=4
 
     # warm-up: a burst of 3 requests per stream (sizes the pools and
     # workspaces, sets every stream's keyframe), then a settle
+    out = []
+    samples = []  # served requests checked against the FP64 oracle (CPU leg)
+    track = {}  # per stream: (keyframe frame, last two estimates against it), in request order
+
+    def follow(results, meta):
+        """Advances the per-stream keyframe tracking through a phase's results."""
+        for r in sorted(results, key=lambda r: r["request_id"]):
+            if r["status"] != 0:
+                continue
+            key, hist = track.get(r["stream_id"], (None, []))
+            f = meta[r["request_id"]][1]
+            if r["keyframe_replaced"]:
+                key, hist = f, []
+            elif key is not None:
+                hist = (hist + [np.asarray(r["T"], float).reshape(4, 4)])[-2:]
+            track[r["stream_id"]] = (key, hist)
+
     wmeta, wt = {}, {}
     for _ in range(3):
         for s in range(len(streams)):
             submit(s, wt, wmeta)
-    srv.drain(len(wmeta), timeout_s=300)
-
-    out = []
-    samples = []  # served requests checked against the FP64 oracle (CPU leg)
+    follow(srv.drain(len(wmeta), timeout_s=300), wmeta)
     # unmeasured Poisson phases first: 1 s at 2000 requests/s (every worker
     # meets every resolution: pools, first launches), then 1 s at 10000
     # requests/s (batches reach max size: workspaces and pools grow to their
@@ -661,7 +675,9 @@ def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=4
         for r in sorted(ok, key=lambda r: r["request_id"]):
             per_stream.setdefault(r["stream_id"], []).append(r)
         for s, rs in per_stream.items():
-            key, hist = None, []
+            # the stream's keyframe and estimates carry over from the earlier
+            # phases (every phase drains before the next starts)
+            key, hist = track.get(s, (None, []))
             poses = streams[s][2]
             for r in rs:
                 f = meta[r["request_id"]][1]
@@ -679,7 +695,8 @@ def serve_leg(device, rates, seconds, seed, frames_per_stream=16, max_requests=4
                     key, hist = f, []
                     replaced += 1
                 elif key is not None:
-                    hist.append(np.asarray(r["T"], float).reshape(4, 4))
+                    hist = (hist + [np.asarray(r["T"], float).reshape(4, 4)])[-2:]
+            track[s] = (key, hist)
         er = np.array([e[0] for e in errs]) if errs else np.zeros(1)
         et = np.array([e[1] for e in errs]) if errs else np.zeros(1)
         if not measured:
