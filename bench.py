@@ -173,7 +173,8 @@ def run_step(ctx, frames_ptrs, cam_c, prm_c, clouds, corr, lin, prm, on_device):
 
 # Algorithmic bytes per unit (the per-stage figures of the scope table):
 #   S1 unproject     2P + 4P + 12V          S2 moments   bands: 2P + 3 (10 s P / 16); sweep: 2P + 10 s P / 16 + 10 s P
-#   S3 stats + Omega 10 s P + 6P + 76V      S4 z-buffer  12V + 8V (+ 8P init, 8P resolve read, 4P write)
+#   S3 stats + Omega 10 s P + 6P + 76V      S4 z-buffer  16V (the point and its w, which carries the
+#                                                        "has a normal" bit of the key) + 8V atomics
 #   S5 corr + lin    8P + 56 C: both index images, then per correspondence
 #                    point xyz, normal xyz and curvature of both clouds; the
 #                    information matrices are rebuilt from the current normal
@@ -186,16 +187,16 @@ def build_bytes(P, V, s=8):
 
 
 def align_bytes(P, V, C, outer, inner):
-    """One alignment: the current cloud's projection (z-buffer 12V + 8V) and
-    resolve (z-buffer read 8P, index write 4P, z-buffer reset 8P), then per
-    outer iteration the reference projection (20V) and per inner iteration
+    """One alignment: the current cloud's projection (points 16V, atomics 8V)
+    and resolve (z-buffer read 8P, index write 4P, z-buffer reset 8P), then
+    per outer iteration the reference projection (24V) and per inner iteration
     the fused pass: z-buffer read and reset (16P) + current index (4P) on the
     first, plus the reference index written (4P) when more follow; later
     inner iterations read both index images (8P); 56 bytes per accepted
     correspondence (points, normals, curvatures of both clouds)."""
     first = 20 * P + (4 * P if inner > 1 else 0) + 56 * C
     later = (inner - 1) * (8 * P + 56 * C)
-    return 20 * V + 20 * P + outer * (20 * V + first + later)
+    return 24 * V + 20 * P + outer * (24 * V + first + later)
 
 
 def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
@@ -209,7 +210,7 @@ def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     if kernel == "stats_omega":
         return (10 * s * P + 6 * P + 76 * V) * pairs
     if kernel == "zbuffer":
-        return (12 * V + 8 * V) * pairs
+        return (16 * V + 8 * V) * pairs
     if kernel == "corr_lin":
         return (20 * P + 56 * C) * pairs
     if kernel == "resolve":
@@ -871,7 +872,7 @@ def main():
     launches_per_step = top_n
     per_launch_bytes = {
         "corr_lin": (20 * P + 56 * C) * npairs,
-        "zbuffer": (12 * V + 8 * V) * npairs,
+        "zbuffer": (16 * V + 8 * V) * npairs,
         "stats_omega": (10 * 8 * P + 6 * P + 76 * V) * F,
         "moments_bands": (2 * P + 3 * 80 * P / 16) * F / 2,  # two kernels per stage launch
         "moments_sweep": (2 * P + 80 * P / 16 + 80 * P) * F,
