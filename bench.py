@@ -214,7 +214,7 @@ def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     if kernel == "corr_lin":
         return (20 * P + 56 * C) * pairs
     if kernel == "resolve":
-        return (8 * P + 4 * P) * pairs
+        return (8 * P + 4 * P + 8 * P) * pairs
     return 0
 
 
@@ -877,7 +877,7 @@ def main():
         "moments_bands": (2 * P + 3 * 80 * P / 16) * F / 2,  # two kernels per stage launch
         "moments_sweep": (2 * P + 80 * P / 16 + 80 * P) * F,
         "unproject": (2 * P + 4 * P + 12 * V) * F / 2,  # two kernels per stage launch
-        "resolve": (12 * P) * npairs,
+        "resolve": (20 * P) * npairs,  # z-buffer read 8P, index write 4P, z-buffer reset 8P
     }.get(top, 0.0)
     achieved = per_launch_bytes / (top_ms / top_n / 1e3) / 1e9
     roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
