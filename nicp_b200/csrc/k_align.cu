@@ -135,6 +135,25 @@ struct Acc {
   float v[31];
 };
 
+// The gate's arithmetic: dot3x and xform_normal without the reference's
+// zero w terms ("+ 0 * 0" of the 4-vector dot products, "+ A3 * 0" of the
+// normal transform), which change at most the sign of a zero -- no
+// comparison of the gates can tell, so the decisions stay bitwise the
+// reference's.
+__device__ __forceinline__ float dot3g(float ax, float ay, float az, float bx, float by, float bz) {
+  float s = fm(ax, bx);
+  s = fa(s, fm(ay, by));
+  return fa(s, fm(az, bz));
+}
+__device__ __forceinline__ float rowg(const float *A, float x, float y, float z) {
+  float s = fm(A[0], x);
+  s = fa(s, fm(A[1], y));
+  return fa(s, fm(A[2], z));
+}
+__device__ __forceinline__ float3 xform_normal_g(const float *A, float4 n) {
+  return make_float3(rowg(A, n.x, n.y, n.z), rowg(A + 4, n.x, n.y, n.z), rowg(A + 8, n.x, n.y, n.z));
+}
+
 // correspondencefinderprojective.cpp:59-101.  T12: rows 0..2 of the gating
 // transform (the aligner passes _T.inverse()).
 // The transformed reference point and normal are returned in rp / rn (rn
@@ -142,15 +161,15 @@ struct Acc {
 __device__ __forceinline__ bool gate_t(const CorrParams &cp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
                                        float4 cn, float3 &rp, float3 &rn) {
   if (!cp.demoted) {
-    if (dot3x(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) return false;
-    if (dot3x(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return false;
+    if (dot3g(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) return false;
+    if (dot3g(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return false;
   }
   rp = xform_point(T12, rp0);
   float dx = fsb(cpt.x, rp.x), dy = fsb(cpt.y, rp.y), dz = fsb(cpt.z, rp.z);
-  if (dot3x(dx, dy, dz, dx, dy, dz) > cp.sq_thr) return false;
+  if (dot3g(dx, dy, dz, dx, dy, dz) > cp.sq_thr) return false;
   if (!cp.demoted) {
-    rn = xform_normal(T12, rn0);
-    if (dot3x(cn.x, cn.y, cn.z, rn.x, rn.y, rn.z) < cp.cos_thr) return false;
+    rn = xform_normal_g(T12, rn0);
+    if (dot3g(cn.x, cn.y, cn.z, rn.x, rn.y, rn.z) < cp.cos_thr) return false;
     float kr = rn0.w, kc = cn.w;
     if (kr < cp.flat_thr) kr = cp.flat_thr;
     if (kc < cp.flat_thr) kc = cp.flat_thr;
@@ -173,7 +192,7 @@ __device__ __forceinline__ bool gate(const CorrParams &cp, const float *T12, flo
 __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
                                          float4 cn, float4 o0, float4 o1, float4 o2, Acc &acc) {
   float3 rp = xform_point(T12, rp0);
-  float3 rn = xform_normal(T12, rn0);
+  float3 rn = xform_normal_g(T12, rn0);
   // symmetric 3x3 as (00 01 02 11 12 22)
   float Op[6] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y};
   float On[6] = {o1.z, o1.w, o2.x, o2.y, o2.z, o2.w};
@@ -326,30 +345,33 @@ __device__ __forceinline__ void lin_terms_structured_xf(const LinParams &lp, con
 
 __device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const float *T12, const float *omd,
                                                     float4 rp0, float4 rn0, float4 cpt, float4 cn, Acc &acc) {
-  lin_terms_structured_xf(lp, omd, xform_point(T12, rp0), xform_normal(T12, rn0), cpt, cn, acc);
+  lin_terms_structured_xf(lp, omd, xform_point(T12, rp0), xform_normal_g(T12, rn0), cpt, cn, acc);
 }
 
-// Reduces every thread's Acc to one FP64 partial of the CTA (fixed order).
+// Reduces every thread's Acc to one FP64 partial of the CTA (fixed order):
+// inside a warp a pairwise FP32 tree (each warp sums 32 threads' partial
+// sums of at most 8 terms: the tree adds log2(32) roundings, far below the
+// FP32 rounding of the terms themselves), across warps and tiles FP64.
 template <int kThreads>
 __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) {
   __shared__ double wsum[kThreads / 32][32];
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double v[32];
+  float v[32];
 #pragma unroll
-  for (int k = 0; k < 31; k++) v[k] = (double)acc.v[k];
-  v[31] = 0.0;
+  for (int k = 0; k < 31; k++) v[k] = acc.v[k];
+  v[31] = 0.0f;
   // butterfly reduce-scatter: lane L ends with the warp total of element L
 #pragma unroll
   for (int off = 16; off >= 1; off >>= 1) {
     bool upper = (lane & off) != 0;
 #pragma unroll
     for (int j = 0; j < off; j++) {
-      double send = upper ? v[j] : v[j + off];
-      double keep = upper ? v[j + off] : v[j];
+      float send = upper ? v[j] : v[j + off];
+      float keep = upper ? v[j + off] : v[j];
       v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
     }
   }
-  wsum[wid][lane] = v[0];
+  wsum[wid][lane] = (double)v[0];
   __syncthreads();
   if (wid == 0) {
     double s = 0.0;
@@ -691,9 +713,9 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
 // (strictly closer AND strictly better aligned); -1 when none passes.
 __device__ int multi_best(const PairDev &pd, const CorrParams &cp, const float *Tg, int p, int ri, int ncur) {
   const float4 rn0 = pd.ref_nrm[ri];
-  if (dot3x(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return -1;
+  if (dot3g(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return -1;
   const float3 rp = xform_point(Tg, pd.ref_pts[ri]);
-  const float3 rn = xform_normal(Tg, rn0);
+  const float3 rn = xform_normal_g(Tg, rn0);
   float kr = rn0.w;
   if (kr < cp.flat_thr) kr = cp.flat_thr;
   const int r = p / pd.cols, c = p - r * pd.cols;
@@ -706,12 +728,12 @@ __device__ int multi_best(const PairDev &pd, const CorrParams &cp, const float *
       const int ci = pd.cur_index[r2 * pd.cols + c2];
       if (ci < 0 || ci >= ncur) continue;
       const float4 cn = pd.cur_nrm[ci];
-      if (dot3x(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) continue;
-      const float nd = dot3x(cn.x, cn.y, cn.z, rn.x, rn.y, rn.z);
+      if (dot3g(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) continue;
+      const float nd = dot3g(cn.x, cn.y, cn.z, rn.x, rn.y, rn.z);
       if (nd < cp.cos_thr) continue;
       const float4 cpt = pd.cur_pts[ci];
       const float dx = fsb(cpt.x, rp.x), dy = fsb(cpt.y, rp.y), dz = fsb(cpt.z, rp.z);
-      const float d = dot3x(dx, dy, dz, dx, dy, dz);
+      const float d = dot3g(dx, dy, dz, dx, dy, dz);
       if (d > cp.sq_thr) continue;
       float kc = cn.w;
       if (kc < cp.flat_thr) kc = cp.flat_thr;
