@@ -257,32 +257,61 @@ __global__ void __launch_bounds__(256) k_unproject_write(const FrameDev *__restr
 }
 
 // ------------------------------------------------------------ moments
-// Storage policies for the integral image.
+// Storage policies for the integral image.  The ten moment planes are kept
+// as five interleaved plane pairs: pair k holds planes 2k and 2k + 1 of
+// pixel i side by side (element 2 (k P + i) + (m & 1)), so that the stats
+// kernel reads a corner's ten sums with five paired loads and the sweep
+// writes them with five paired stores.
 struct MomF64 {
   typedef double T;
   __device__ static double val(double v) { return v; }
-  __device__ static double load(const void *base, size_t i) { return static_cast<const double *>(base)[i]; }
-  __device__ static void store(void *base, size_t i, double v) { static_cast<double *>(base)[i] = v; }
+  __device__ static void store(void *base, size_t P, int m, size_t i, double v) {
+    static_cast<double *>(base)[2 * ((size_t)(m >> 1) * P + i) + (m & 1)] = v;
+  }
+  __device__ static void store2(void *base, size_t P, int k, size_t i, double a, double b) {
+    static_cast<double2 *>(base)[(size_t)k * P + i] = make_double2(a, b);
+  }
+  __device__ static void load2(const void *base, size_t P, int k, size_t i, double &a, double &b) {
+    const double2 v = static_cast<const double2 *>(base)[(size_t)k * P + i];
+    a = v.x;
+    b = v.y;
+  }
 };
 struct MomF32 {
   typedef float T;
   __device__ static double val(float v) { return (double)v; }
-  __device__ static double load(const void *base, size_t i) { return (double)static_cast<const float *>(base)[i]; }
-  __device__ static void store(void *base, size_t i, double v) { static_cast<float *>(base)[i] = (float)v; }
+  __device__ static void store(void *base, size_t P, int m, size_t i, double v) {
+    static_cast<float *>(base)[2 * ((size_t)(m >> 1) * P + i) + (m & 1)] = (float)v;
+  }
+  __device__ static void store2(void *base, size_t P, int k, size_t i, double a, double b) {
+    static_cast<float2 *>(base)[(size_t)k * P + i] = make_float2((float)a, (float)b);
+  }
+  __device__ static void load2(const void *base, size_t P, int k, size_t i, double &a, double &b) {
+    const float2 v = static_cast<const float2 *>(base)[(size_t)k * P + i];
+    a = (double)v.x;
+    b = (double)v.y;
+  }
 };
 // Two-float: an unevaluated sum hi + lo of two floats (about 48 significant
 // bits); values travel as double inside the kernels and are split on store.
 struct MomTwoFloat {
   typedef float2 T;
   __device__ static double val(float2 v) { return (double)v.x + (double)v.y; }
-  __device__ static double load(const void *base, size_t i) {
-    float2 v = static_cast<const float2 *>(base)[i];
-    return (double)v.x + (double)v.y;
+  __device__ static float2 split(double v) {
+    const float hi = (float)v;
+    return make_float2(hi, (float)(v - (double)hi));
   }
-  __device__ static void store(void *base, size_t i, double v) {
-    float hi = (float)v;
-    float lo = (float)(v - (double)hi);
-    static_cast<float2 *>(base)[i] = make_float2(hi, lo);
+  __device__ static void store(void *base, size_t P, int m, size_t i, double v) {
+    static_cast<float2 *>(base)[2 * ((size_t)(m >> 1) * P + i) + (m & 1)] = split(v);
+  }
+  __device__ static void store2(void *base, size_t P, int k, size_t i, double a, double b) {
+    const float2 x = split(a), y = split(b);
+    static_cast<float4 *>(base)[(size_t)k * P + i] = make_float4(x.x, x.y, y.x, y.y);
+  }
+  __device__ static void load2(const void *base, size_t P, int k, size_t i, double &a, double &b) {
+    const float4 v = static_cast<const float4 *>(base)[(size_t)k * P + i];
+    a = (double)v.x + (double)v.y;
+    b = (double)v.z + (double)v.w;
   }
 };
 
@@ -583,11 +612,13 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const Fra
       __syncthreads();
       const size_t row0 = (size_t)r * cols + x0;
 #pragma unroll
-      for (int m = 0; m < 10; m++)
+      for (int k = 0; k < 5; k++)
 #pragma unroll
         for (int j = 0; j < kRowPix; j++) {
           const int q = j * kRowThreads + t;
-          if (q < n) M::store(f.moments, m * P + row0 + q, (double)state[m * kChunkPix + q]);
+          if (q < n)
+            M::store2(f.moments, P, k, row0 + q, (double)state[2 * k * kChunkPix + q],
+                      (double)state[(2 * k + 1) * kChunkPix + q]);
         }
     }
     __syncthreads();  // the last copy-out has read the state before the next chunk's carry row
@@ -633,17 +664,19 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) k_stats(const FrameDev *__
     size_t iA = (size_t)yM * cols + xM, iB = (size_t)ym * cols + xm;
     size_t iC = (size_t)yM * cols + xm, iD = (size_t)ym * cols + xM;
     double S[10];
-    // one pointer per corner, advanced plane by plane
-    const typename M::T *pA = static_cast<const typename M::T *>(f.moments) + iA;
-    const typename M::T *pB = pA + ((ptrdiff_t)iB - (ptrdiff_t)iA), *pC = pA + ((ptrdiff_t)iC - (ptrdiff_t)iA),
-                        *pD = pA + ((ptrdiff_t)iD - (ptrdiff_t)iA);
+    // the four corners of each plane pair: 20 paired loads
 #pragma unroll
-    for (int m = 0; m < 10; m++) {
-      double s = M::val(pA[0]) + M::val(pB[0]);
-      s = s - M::val(pC[0]);
-      s = s - M::val(pD[0]);
-      S[m] = s;
-      pA += P; pB += P; pC += P; pD += P;
+    for (int k = 0; k < 5; k++) {
+      double a0, a1, b0, b1, c0, c1, d0, d1;
+      M::load2(f.moments, P, k, iA, a0, a1);
+      M::load2(f.moments, P, k, iB, b0, b1);
+      M::load2(f.moments, P, k, iC, c0, c1);
+      M::load2(f.moments, P, k, iD, d0, d1);
+      double s0 = a0 + b0, s1 = a1 + b1;
+      s0 = s0 - c0;
+      s1 = s1 - c1;
+      S[2 * k] = s0 - d0;
+      S[2 * k + 1] = s1 - d1;
     }
     int n = (int)S[0];
     if (n >= f.min_points) {
@@ -959,7 +992,7 @@ __global__ void __launch_bounds__(128) k_moments_colsum(const FrameDev *__restri
   for (int k = 0; k < kBandRows; k++) {
     if (r0 + k < r1) {
       s = s + v[k];
-      M::store(f.moments, m * P + (size_t)(r0 + k) * cols + c, (double)s);
+      M::store(f.moments, P, m, (size_t)(r0 + k) * cols + c, (double)s);
     }
   }
 }
@@ -1023,19 +1056,22 @@ void launch_moments(int precision, const FrameDev *d_frames, int nframes, int to
 }
 
 // Stats launch shapes: (threads per CTA, CTAs per SM of the register budget).
+#ifdef NICP_STATS_WIDE_DEFAULT
+static const int kStatsShape[kStatsShapes][2] = {{256, 2}, {128, 6}, {64, 12}, {256, 3}};
+#else
 static const int kStatsShape[kStatsShapes][2] = {{256, 3}, {128, 6}, {64, 12}, {256, 2}};
+#endif
 
 int stats_shape_threads(int shape) { return kStatsShape[shape][0]; }
 int stats_shape_min_ctas(int shape) { return kStatsShape[shape][1]; }
 
 template <class M, bool kLean>
 static void stats_launch(int shape, dim3 g, const FrameDev *d_frames, int nframes, cudaStream_t s) {
-  switch (shape) {
-    case 1: k_stats<M, 128, 6, kLean><<<g, 128, 0, s>>>(d_frames, nframes); break;
-    case 2: k_stats<M, 64, 12, kLean><<<g, 64, 0, s>>>(d_frames, nframes); break;
-    case 3: k_stats<M, 256, 2, kLean><<<g, 256, 0, s>>>(d_frames, nframes); break;
-    default: k_stats<M, 256, 3, kLean><<<g, 256, 0, s>>>(d_frames, nframes); break;
-  }
+  const int threads = kStatsShape[shape][0], ctas = kStatsShape[shape][1];
+  if (threads == 128) k_stats<M, 128, 6, kLean><<<g, 128, 0, s>>>(d_frames, nframes);
+  else if (threads == 64) k_stats<M, 64, 12, kLean><<<g, 64, 0, s>>>(d_frames, nframes);
+  else if (ctas == 2) k_stats<M, 256, 2, kLean><<<g, 256, 0, s>>>(d_frames, nframes);
+  else k_stats<M, 256, 3, kLean><<<g, 256, 0, s>>>(d_frames, nframes);
 }
 
 template <class M>
