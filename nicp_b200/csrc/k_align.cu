@@ -348,30 +348,30 @@ __device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const 
   lin_terms_structured_xf(lp, omd, xform_point(T12, rp0), xform_normal_g(T12, rn0), cpt, cn, acc);
 }
 
-// Reduces every thread's Acc to one FP64 partial of the CTA (fixed order):
-// inside a warp a pairwise FP32 tree (each warp sums 32 threads' partial
-// sums of at most 8 terms: the tree adds log2(32) roundings, far below the
-// FP32 rounding of the terms themselves), across warps and tiles FP64.
+// Reduces every thread's Acc to one FP64 partial of the CTA (fixed order).
+// (A pairwise FP32 tree inside the warp measured 3 % faster but moved an
+// ill-conditioned pose -- a frame against a subscene rendered from a merged
+// scene -- from 1e-5 to 2e-5 rad of the FP64 oracle: the warp sums stay FP64.)
 template <int kThreads>
 __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) {
   __shared__ double wsum[kThreads / 32][32];
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  float v[32];
+  double v[32];
 #pragma unroll
-  for (int k = 0; k < 31; k++) v[k] = acc.v[k];
-  v[31] = 0.0f;
+  for (int k = 0; k < 31; k++) v[k] = (double)acc.v[k];
+  v[31] = 0.0;
   // butterfly reduce-scatter: lane L ends with the warp total of element L
 #pragma unroll
   for (int off = 16; off >= 1; off >>= 1) {
     bool upper = (lane & off) != 0;
 #pragma unroll
     for (int j = 0; j < off; j++) {
-      float send = upper ? v[j] : v[j + off];
-      float keep = upper ? v[j + off] : v[j];
+      double send = upper ? v[j] : v[j + off];
+      double keep = upper ? v[j + off] : v[j];
       v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
     }
   }
-  wsum[wid][lane] = (double)v[0];
+  wsum[wid][lane] = v[0];
   __syncthreads();
   if (wid == 0) {
     double s = 0.0;
