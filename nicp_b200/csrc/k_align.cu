@@ -419,6 +419,51 @@ struct GatherStageG : GatherStageS {  // general Omega: gathered for accepted pi
 #endif
 template <bool kStructured>
 using GatherStage = typename std::conditional<kStructured, GatherStageS, GatherStageG>::type;
+
+// block_reduce_store for the fused kernel, with the warp's step done
+// through shared memory instead of a shuffle butterfly: the warp's 32 x 31
+// partial sums are written to the warp's own slots of the stage it has just
+// consumed (rp, rn, cp, cn at slots 32w.. and 128 + 32w..: eight runs of
+// four 32-float rows), and lane L < 31 then sums row L -- the 32 lanes'
+// partials of element L -- in FP64, in a fixed order (each lane starts its
+// row at another 16-byte column, so that the eight lanes of a quarter-warp
+// read eight different bank groups).  The warps' totals are added in FP64
+// as in block_reduce_store.  The barrier inside also orders the row reads
+// before the next gathers into these slots.
+template <int kThreads, class StageT>
+__device__ __forceinline__ void block_reduce_store_staged(const Acc &acc, double *out, StageT &g) {
+  __shared__ double wsum[kThreads / 32][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  float *base = reinterpret_cast<float *>(&g.rp[0]);
+  auto row_of = [&](int k) {  // element k: run k / 4, row k % 4 of the warp's region
+    const int run = k >> 2;
+    return base + 4 * ((run >> 1) * kSubPix + (run & 1) * kFusedThreads + 32 * wid) + 32 * (k & 3);
+  };
+  __syncwarp();  // every lane of the warp is done with its slots of this stage
+#pragma unroll
+  for (int k = 0; k < 31; k++) row_of(k)[lane] = acc.v[k];
+  __syncwarp();
+  double v = 0.0;
+  if (lane < 31) {
+    const float4 *r4 = reinterpret_cast<const float4 *>(row_of(lane));
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const float4 x = r4[(q + lane) & 7];
+      v += (double)x.x;
+      v += (double)x.y;
+      v += (double)x.z;
+      v += (double)x.w;
+    }
+  }
+  wsum[wid][lane] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; w++) s += wsum[w][lane];
+    out[lane] = s;
+  }
+}
 template <bool kStructured>
 __host__ __device__ constexpr int corr_stages() { return kStructured ? NICP_CORR_S_STAGES : kCorrStages; }
 template <bool kStructured>
@@ -661,7 +706,8 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
       }
       if (sub == kSubsPerTile - 1) {
         const PairDev &pd = pairs[sPair[e]];
-        block_reduce_store<kFusedThreads>(acc, pd.partials + (size_t)(tile_of(j) - pd.tile_base) * kPartialWords);
+        block_reduce_store_staged<kFusedThreads>(acc, pd.partials + (size_t)(tile_of(j) - pd.tile_base) * kPartialWords,
+                                                 stage_of(j));
       }
     }
   };
