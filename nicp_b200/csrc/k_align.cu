@@ -139,7 +139,7 @@ struct Acc {
 // zero w terms ("+ 0 * 0" of the 4-vector dot products, "+ A3 * 0" of the
 // normal transform), which change at most the sign of a zero -- no
 // comparison of the gates can tell, so the decisions stay bitwise the
-// reference's.
+// reference's -- and xform_point with its "+ A3 * 1" written as "+ A3".
 __device__ __forceinline__ float dot3g(float ax, float ay, float az, float bx, float by, float bz) {
   float s = fm(ax, bx);
   s = fa(s, fm(ay, by));
@@ -153,6 +153,11 @@ __device__ __forceinline__ float rowg(const float *A, float x, float y, float z)
 __device__ __forceinline__ float3 xform_normal_g(const float *A, float4 n) {
   return make_float3(rowg(A, n.x, n.y, n.z), rowg(A + 4, n.x, n.y, n.z), rowg(A + 8, n.x, n.y, n.z));
 }
+// row4 with w = 1: "+ A3 * 1" adds A3 exactly
+__device__ __forceinline__ float3 xform_point_g(const float *A, float4 p) {
+  return make_float3(fa(rowg(A, p.x, p.y, p.z), A[3]), fa(rowg(A + 4, p.x, p.y, p.z), A[7]),
+                     fa(rowg(A + 8, p.x, p.y, p.z), A[11]));
+}
 
 // correspondencefinderprojective.cpp:59-101.  T12: rows 0..2 of the gating
 // transform (the aligner passes _T.inverse()).
@@ -164,7 +169,7 @@ __device__ __forceinline__ bool gate_t(const CorrParams &cp, const float *T12, f
     if (dot3g(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) return false;
     if (dot3g(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return false;
   }
-  rp = xform_point(T12, rp0);
+  rp = xform_point_g(T12, rp0);
   float dx = fsb(cpt.x, rp.x), dy = fsb(cpt.y, rp.y), dz = fsb(cpt.z, rp.z);
   if (dot3g(dx, dy, dz, dx, dy, dz) > cp.sq_thr) return false;
   if (!cp.demoted) {
@@ -191,7 +196,7 @@ __device__ __forceinline__ bool gate(const CorrParams &cp, const float *T12, flo
 // linearizer.cpp:59-100 for one correspondence, FP32.
 __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
                                          float4 cn, float4 o0, float4 o1, float4 o2, Acc &acc) {
-  float3 rp = xform_point(T12, rp0);
+  float3 rp = xform_point_g(T12, rp0);
   float3 rn = xform_normal_g(T12, rn0);
   // symmetric 3x3 as (00 01 02 11 12 22)
   float Op[6] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y};
@@ -345,7 +350,7 @@ __device__ __forceinline__ void lin_terms_structured_xf(const LinParams &lp, con
 
 __device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const float *T12, const float *omd,
                                                     float4 rp0, float4 rn0, float4 cpt, float4 cn, Acc &acc) {
-  lin_terms_structured_xf(lp, omd, xform_point(T12, rp0), xform_normal_g(T12, rn0), cpt, cn, acc);
+  lin_terms_structured_xf(lp, omd, xform_point_g(T12, rp0), xform_normal_g(T12, rn0), cpt, cn, acc);
 }
 
 // Reduces every thread's Acc to one FP64 partial of the CTA (fixed order).
@@ -760,7 +765,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
 __device__ int multi_best(const PairDev &pd, const CorrParams &cp, const float *Tg, int p, int ri, int ncur) {
   const float4 rn0 = pd.ref_nrm[ri];
   if (dot3g(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return -1;
-  const float3 rp = xform_point(Tg, pd.ref_pts[ri]);
+  const float3 rp = xform_point_g(Tg, pd.ref_pts[ri]);
   const float3 rn = xform_normal_g(Tg, rn0);
   float kr = rn0.w;
   if (kr < cp.flat_thr) kr = cp.flat_thr;
