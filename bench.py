@@ -413,6 +413,7 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
 
     ms, res = timed(prm)
     shape = ctx.launch_shape()
+    stats_shape = ctx.stats_shape()
     prm_fixed = L.AlignParams.from_buffer_copy(prm)
     prm_fixed.early_exit_eps = 0.0
     ms_fixed, res_fixed = timed(prm_fixed)
@@ -472,7 +473,9 @@ def mixed_batch_leg(ctx, stream, device, seed, npairs=512, steps=3, warmup=3, pl
             "resolution_counts": {n: names.count(n) for n in MIXED_CAMS},
             "kernel_shares_and_launches": shares, "profiled_step_ms": total,
             "autotuned_launch_shape": {"zbuffer_points_per_thread": shape[0],
-                                       "corr_lin_ctas_per_sm": shape[1] or "all that fit"}}, checks
+                                       "corr_lin_ctas_per_sm": shape[1] or "all that fit",
+                                       "stats_threads_x_ctas_per_sm": list(stats_shape),
+                                       "resolution_mixes_tuned": shape[2]}}, checks
 
 
 # ------------------------------------------------------------------ scene fusion leg
