@@ -131,9 +131,17 @@ __global__ void k_resolve(const PairDev *__restrict__ pairs, int npairs, int to_
 // ------------------------------------------------------------ gates + terms
 struct Acc {
   // 0..5 Htt lower (00 10 11 20 21 22), 6..14 Htr row-major, 15..20 Hrr lower,
-  // 21..23 bt, 24..26 br, 27 chi2, 28 inliers, 29 candidates, 30 accepted
+  // 21..23 bt, 24..26 br, 27 chi2, 28 inliers, 29 candidates, 30 accepted.
+  // The rotational Jacobian block is skew(2 p) (linearizer.cpp:59-100); the
+  // per-pixel terms use skew(p), so Htr and br hold half and Hrr a quarter of
+  // their values, and the reductions scale the FP64 tile sums by 2 and 4
+  // (exact: powers of two).
   float v[31];
 };
+// Power-of-two factor of each Acc element (see Acc).
+__device__ __forceinline__ double acc_scale(int k) {
+  return (k >= 15 && k <= 20) ? 4.0 : ((k >= 6 && k <= 14) || (k >= 24 && k <= 26)) ? 2.0 : 1.0;
+}
 
 // The gate's arithmetic: dot3x and xform_normal without the reference's
 // zero w terms ("+ 0 * 0" of the 4-vector dot products, "+ A3 * 0" of the
@@ -144,6 +152,17 @@ __device__ __forceinline__ float dot3g(float ax, float ay, float az, float bx, f
   float s = fm(ax, bx);
   s = fa(s, fm(ay, by));
   return fa(s, fm(az, bz));
+}
+// The reference's "normal.squaredNorm() == 0" (correspondencefinderprojective.cpp:69,
+// the normal's w is 0): a sum of non-negative float squares is zero exactly
+// when every square rounds to zero, and x * x rounds to zero (round to
+// nearest even, subnormals kept) exactly when |x| <= 2^-75, since 2^-150 is
+// the tie between 0 and the smallest subnormal 2^-149.  A NaN component
+// makes the squared norm NaN, not zero, and every comparison below false.
+// Three compares instead of three products and two sums.
+__device__ __forceinline__ bool normal_is_zero(float x, float y, float z) {
+  constexpr float t = 0x1p-75f;
+  return fabsf(x) <= t && fabsf(y) <= t && fabsf(z) <= t;
 }
 __device__ __forceinline__ float rowg(const float *A, float x, float y, float z) {
   float s = fm(A[0], x);
@@ -166,8 +185,8 @@ __device__ __forceinline__ float3 xform_point_g(const float *A, float4 p) {
 __device__ __forceinline__ bool gate_t(const CorrParams &cp, const float *T12, float4 rp0, float4 rn0, float4 cpt,
                                        float4 cn, float3 &rp, float3 &rn) {
   if (!cp.demoted) {
-    if (dot3g(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) return false;
-    if (dot3g(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return false;
+    if (normal_is_zero(cn.x, cn.y, cn.z)) return false;
+    if (normal_is_zero(rn0.x, rn0.y, rn0.z)) return false;
   }
   rp = xform_point_g(T12, rp0);
   float dx = fsb(cpt.x, rp.x), dy = fsb(cpt.y, rp.y), dz = fsb(cpt.z, rp.z);
@@ -226,9 +245,10 @@ __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12,
   }
   acc.v[27] += ks * le;
   acc.v[28] += 1.0f;
-  // skew(v) = [[0, c, -b], [-c, 0, a], [b, -a, 0]], (a, b, c) = 2 v
-  float a = 2.0f * rp.x, b = 2.0f * rp.y, c = 2.0f * rp.z;
-  float an = 2.0f * rn.x, bn = 2.0f * rn.y, cn2 = 2.0f * rn.z;
+  // skew(v) = [[0, c, -b], [-c, 0, a], [b, -a, 0]], (a, b, c) = v (the
+  // Jacobian's factor 2 is applied to the tile sums, see Acc)
+  float a = rp.x, b = rp.y, c = rp.z;
+  float an = rn.x, bn = rn.y, cn2 = rn.z;
   // Htt += Op * ks
   acc.v[0] += Op[0] * ks; acc.v[1] += Op[1] * ks; acc.v[2] += Op[3] * ks;
   acc.v[3] += Op[2] * ks; acc.v[4] += Op[4] * ks; acc.v[5] += Op[5] * ks;
@@ -261,7 +281,7 @@ __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12,
   }
   acc.v[15] += R[0][0] * ks; acc.v[16] += R[1][0] * ks; acc.v[17] += R[1][1] * ks;
   acc.v[18] += R[2][0] * ks; acc.v[19] += R[2][1] * ks; acc.v[20] += R[2][2] * ks;
-  // bt += ks ep; br += ks (Sp^T ep + Sn^T en), S^T e = (2v) x e
+  // bt += ks ep; br += ks (Sp^T ep + Sn^T en), S^T e = v x e
   acc.v[21] += ks * ep[0]; acc.v[22] += ks * ep[1]; acc.v[23] += ks * ep[2];
   float u0 = b * ep[2] - c * ep[1], u1 = c * ep[0] - a * ep[2], u2 = a * ep[1] - b * ep[0];
   float w0 = bn * en[2] - cn2 * en[1], w1 = cn2 * en[0] - an * en[2], w2 = an * en[1] - bn * en[0];
@@ -271,12 +291,15 @@ __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12,
 // lin_terms for a current point whose information matrices have the
 // converter's structure Omega = d1 I + (d0 - d1) u u^T, u its normal (the
 // smallest-eigenvalue eigenvector; Omega = U diag(d0, d1, d1) U^T,
-// informationmatrixcalculator.cpp:9-57).  With S = skew(2 v) (S x = x cross 2v)
-// and w = S^T u:  Omega e = a e + b (u.e) u,  Omega S = a S + b u w^T,
-// S^T Omega S = a (|2v|^2 I - (2v)(2v)^T) + b w w^T.  The class code in the
+// informationmatrixcalculator.cpp:9-57).  With S = skew(v) (S x = x cross v,
+// v the moved point; the Jacobian's factor 2 is applied to the tile sums, see
+// Acc) and w = S^T u:  Omega e = a e + b (u.e) u,  Omega S = a S + b u w^T,
+// S^T Omega S = a (|v|^2 I - v v^T) + b w w^T.  The class code in the
 // point's w selects (d0, d1); omd holds them for the four classes.
 // rp, rn: the reference point and normal already moved by the linearizer's
-// transform.
+// transform.  Every accumulator update is one fused chain of FMAs; the
+// robust kernel's weight ks (linearizer.cpp:83-89) is folded into the
+// weights and residual terms only for the pixels beyond the chi2 bound.
 __device__ __forceinline__ void lin_terms_structured_xf(const LinParams &lp, const float *omd, float3 rp, float3 rn,
                                                        float4 cpt, float4 cn, Acc &acc) {
   float alp = 0.0f, bep = 0.0f, aln = 0.0f, ben = 0.0f;
@@ -294,58 +317,62 @@ __device__ __forceinline__ void lin_terms_structured_xf(const LinParams &lp, con
   }
   if (lp.demoted) { aln = 0.0f; ben = 0.0f; }
   const float ux = cn.x, uy = cn.y, uz = cn.z;
-  float pe[3] = {rp.x - cpt.x, rp.y - cpt.y, rp.z - cpt.z};
-  float ne[3] = {rn.x - cn.x, rn.y - cn.y, rn.z - cn.z};
-  float up = ux * pe[0] + uy * pe[1] + uz * pe[2];
-  float un = ux * ne[0] + uy * ne[1] + uz * ne[2];
-  float ep[3] = {alp * pe[0] + bep * up * ux, alp * pe[1] + bep * up * uy, alp * pe[2] + bep * up * uz};
-  float en[3] = {aln * ne[0] + ben * un * ux, aln * ne[1] + ben * un * uy, aln * ne[2] + ben * un * uz};
-  float le = (pe[0] * ep[0] + pe[1] * ep[1] + pe[2] * ep[2]) + (ne[0] * en[0] + ne[1] * en[1] + ne[2] * en[2]);
-  float ks = 1.0f;
+  float pe0 = rp.x - cpt.x, pe1 = rp.y - cpt.y, pe2 = rp.z - cpt.z;
+  float ne0 = rn.x - cn.x, ne1 = rn.y - cn.y, ne2 = rn.z - cn.z;
+  const float bu = bep * fmaf(uz, pe2, fmaf(uy, pe1, ux * pe0));
+  const float bv = ben * fmaf(uz, ne2, fmaf(uy, ne1, ux * ne0));
+  float ep0 = fmaf(bu, ux, alp * pe0), ep1 = fmaf(bu, uy, alp * pe1), ep2 = fmaf(bu, uz, alp * pe2);
+  float en0 = fmaf(bv, ux, aln * ne0), en1 = fmaf(bv, uy, aln * ne1), en2 = fmaf(bv, uz, aln * ne2);
+  float le = fmaf(ne2, en2, fmaf(ne1, en1, fmaf(ne0, en0, fmaf(pe2, ep2, fmaf(pe1, ep1, pe0 * ep0)))));
   if (le > lp.max_chi2) {
-    if (lp.robust) ks = lp.max_chi2 / le;
-    else return;
+    if (!lp.robust) return;
+    const float ks = lp.max_chi2 / le;
+    le *= ks;
+    alp *= ks; bep *= ks; aln *= ks; ben *= ks;
+    ep0 *= ks; ep1 *= ks; ep2 *= ks;
+    en0 *= ks; en1 *= ks; en2 *= ks;
   }
-  acc.v[27] += ks * le;
+  acc.v[27] += le;
   acc.v[28] += 1.0f;
-  const float a = 2.0f * rp.x, b = 2.0f * rp.y, c = 2.0f * rp.z;
-  const float an = 2.0f * rn.x, bn = 2.0f * rn.y, cn2 = 2.0f * rn.z;
-  const float ka = ks * alp, kb = ks * bep, kan = ks * aln, kbn = ks * ben;
-  // Htt += ks Omega_p
-  const float t0 = kb * ux, t1 = kb * uy, t2 = kb * uz;
-  acc.v[0] += ka + t0 * ux; acc.v[1] += t0 * uy; acc.v[2] += ka + t1 * uy;
-  acc.v[3] += t0 * uz; acc.v[4] += t1 * uz; acc.v[5] += ka + t2 * uz;
-  // Htr += ks Omega_p S, S = [[0, c, -b], [-c, 0, a], [b, -a, 0]]
-  const float wp0 = -c * uy + b * uz, wp1 = c * ux - a * uz, wp2 = -b * ux + a * uy;
-  const float wn0 = -cn2 * uy + bn * uz, wn1 = cn2 * ux - an * uz, wn2 = -bn * ux + an * uy;
-  // (ka S = [[0, qc, -qb], [-qc, 0, qa], [qb, -qa, 0]] with q = ka (a, b, c))
-  const float qa = ka * a, qb = ka * b, qc = ka * c;
+  const float a = rp.x, b = rp.y, c = rp.z;
+  const float an = rn.x, bn = rn.y, cn2 = rn.z;
+  // Htt += Omega_p
+  const float t0 = bep * ux, t1 = bep * uy, t2 = bep * uz;
+  acc.v[0] = fmaf(t0, ux, acc.v[0] + alp);
+  acc.v[1] = fmaf(t0, uy, acc.v[1]);
+  acc.v[2] = fmaf(t1, uy, acc.v[2] + alp);
+  acc.v[3] = fmaf(t0, uz, acc.v[3]);
+  acc.v[4] = fmaf(t1, uz, acc.v[4]);
+  acc.v[5] = fmaf(t2, uz, acc.v[5] + alp);
+  // Htr += Omega_p S = alp S + bep u wp^T, S = [[0, c, -b], [-c, 0, a], [b, -a, 0]]
+  const float wp0 = fmaf(b, uz, -c * uy), wp1 = fmaf(c, ux, -a * uz), wp2 = fmaf(a, uy, -b * ux);
+  const float wn0 = fmaf(bn, uz, -cn2 * uy), wn1 = fmaf(cn2, ux, -an * uz), wn2 = fmaf(an, uy, -bn * ux);
   acc.v[6] = fmaf(t0, wp0, acc.v[6]);
-  acc.v[7] = fmaf(t0, wp1, acc.v[7] + qc);
-  acc.v[8] = fmaf(t0, wp2, acc.v[8] - qb);
-  acc.v[9] = fmaf(t1, wp0, acc.v[9] - qc);
+  acc.v[7] = fmaf(t0, wp1, fmaf(alp, c, acc.v[7]));
+  acc.v[8] = fmaf(t0, wp2, fmaf(-alp, b, acc.v[8]));
+  acc.v[9] = fmaf(t1, wp0, fmaf(-alp, c, acc.v[9]));
   acc.v[10] = fmaf(t1, wp1, acc.v[10]);
-  acc.v[11] = fmaf(t1, wp2, acc.v[11] + qa);
-  acc.v[12] = fmaf(t2, wp0, acc.v[12] + qb);
-  acc.v[13] = fmaf(t2, wp1, acc.v[13] - qa);
+  acc.v[11] = fmaf(t1, wp2, fmaf(alp, a, acc.v[11]));
+  acc.v[12] = fmaf(t2, wp0, fmaf(alp, b, acc.v[12]));
+  acc.v[13] = fmaf(t2, wp1, fmaf(-alp, a, acc.v[13]));
   acc.v[14] = fmaf(t2, wp2, acc.v[14]);
-  // Hrr += ks (S^T Omega_p S + Sn^T Omega_n Sn)
-  //      = ka (|v|^2 I - v v^T) + kan (|vn|^2 I - vn vn^T) + kb wp wp^T + kbn wn wn^T
-  const float qan = kan * an, qbn = kan * bn, qcn = kan * cn2;
-  const float D = fmaf(ka, a * a + b * b + c * c, kan * (an * an + bn * bn + cn2 * cn2));
-  const float pw0 = kb * wp0, pw1 = kb * wp1, pw2 = kb * wp2;
-  const float nw0 = kbn * wn0, nw1 = kbn * wn1, nw2 = kbn * wn2;
-  acc.v[15] = fmaf(nw0, wn0, fmaf(pw0, wp0, fmaf(-qan, an, fmaf(-qa, a, acc.v[15] + D))));
+  // Hrr += S^T Omega_p S + Sn^T Omega_n Sn
+  //      = alp (|v|^2 I - v v^T) + aln (|vn|^2 I - vn vn^T) + bep wp wp^T + ben wn wn^T
+  const float qa = alp * a, qb = alp * b, qc = alp * c;
+  const float qan = aln * an, qbn = aln * bn, qcn = aln * cn2;
+  const float pw0 = bep * wp0, pw1 = bep * wp1, pw2 = bep * wp2;
+  const float nw0 = ben * wn0, nw1 = ben * wn1, nw2 = ben * wn2;
+  acc.v[15] = fmaf(nw0, wn0, fmaf(pw0, wp0, fmaf(qcn, cn2, fmaf(qbn, bn, fmaf(qc, c, fmaf(qb, b, acc.v[15]))))));
   acc.v[16] = fmaf(nw1, wn0, fmaf(pw1, wp0, fmaf(-qbn, an, fmaf(-qb, a, acc.v[16]))));
-  acc.v[17] = fmaf(nw1, wn1, fmaf(pw1, wp1, fmaf(-qbn, bn, fmaf(-qb, b, acc.v[17] + D))));
+  acc.v[17] = fmaf(nw1, wn1, fmaf(pw1, wp1, fmaf(qcn, cn2, fmaf(qan, an, fmaf(qc, c, fmaf(qa, a, acc.v[17]))))));
   acc.v[18] = fmaf(nw2, wn0, fmaf(pw2, wp0, fmaf(-qcn, an, fmaf(-qc, a, acc.v[18]))));
   acc.v[19] = fmaf(nw2, wn1, fmaf(pw2, wp1, fmaf(-qcn, bn, fmaf(-qc, b, acc.v[19]))));
-  acc.v[20] = fmaf(nw2, wn2, fmaf(pw2, wp2, fmaf(-qcn, cn2, fmaf(-qc, c, acc.v[20] + D))));
-  // bt += ks ep; br += ks (S^T ep + Sn^T en)
-  acc.v[21] += ks * ep[0]; acc.v[22] += ks * ep[1]; acc.v[23] += ks * ep[2];
-  float u0 = b * ep[2] - c * ep[1], u1 = c * ep[0] - a * ep[2], u2 = a * ep[1] - b * ep[0];
-  float w0 = bn * en[2] - cn2 * en[1], w1 = cn2 * en[0] - an * en[2], w2 = an * en[1] - bn * en[0];
-  acc.v[24] += ks * (u0 + w0); acc.v[25] += ks * (u1 + w1); acc.v[26] += ks * (u2 + w2);
+  acc.v[20] = fmaf(nw2, wn2, fmaf(pw2, wp2, fmaf(qbn, bn, fmaf(qan, an, fmaf(qb, b, fmaf(qa, a, acc.v[20]))))));
+  // bt += ep; br += Sp^T ep + Sn^T en (S^T e = v x e)
+  acc.v[21] += ep0; acc.v[22] += ep1; acc.v[23] += ep2;
+  acc.v[24] = fmaf(bn, en2, fmaf(-cn2, en1, fmaf(b, ep2, fmaf(-c, ep1, acc.v[24]))));
+  acc.v[25] = fmaf(cn2, en0, fmaf(-an, en2, fmaf(c, ep0, fmaf(-a, ep2, acc.v[25]))));
+  acc.v[26] = fmaf(an, en1, fmaf(-bn, en0, fmaf(a, ep1, fmaf(-b, ep0, acc.v[26]))));
 }
 
 __device__ __forceinline__ void lin_terms_structured(const LinParams &lp, const float *T12, const float *omd,
@@ -382,7 +409,7 @@ __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) 
     double s = 0.0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; w++) s += wsum[w][lane];
-    out[lane] = s;
+    out[lane] = s * acc_scale(lane);
   }
 }
 
@@ -398,12 +425,22 @@ __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) 
 // and normal, 3 x Omega) into its own shared-memory slot with cp.async;
 // kCorrStages sub-tiles are in flight while the oldest one is gated and
 // linearized.  Each thread reads back only what it copied itself, so the
-// pipeline needs no barrier.
+// gathered data needs no barrier.
 constexpr int kFusedThreads = 128;
 constexpr int kFusedPX = 2;
 constexpr int kSubPix = kFusedThreads * kFusedPX;        // pixels per sub-tile
 constexpr int kSubsPerTile = kCorrTilePixels / kSubPix;  // 4
 constexpr int kCorrStages = 3;  // general Omega: gather, gate + Omega gather, linearize
+// The only data threads share are a tile's constants (transforms, Omega
+// parameters, pair, skip flags) and the per-tile reduction.  The constants
+// live in a ring of kConstSlots tiles and the CTA meets at a barrier once per
+// tile, in the iteration that writes the next tile's constants: tile U's are
+// written before the barrier of iteration 4U - 1 (4U - 2 with three stages)
+// and read in iterations up to 4U + 3, and their slot is rewritten for tile
+// U + kConstSlots only after the barrier of iteration 4U + 4 kConstSlots - 5
+// (- 6), which every thread reaches after its iteration 4U + 3 when
+// kConstSlots >= 3.  The reduction's own barrier orders its shared sums.
+constexpr int kConstSlots = 4;
 #ifndef NICP_CORR_S_STAGES
 #define NICP_CORR_S_STAGES 2      // structured Omega: gather, gate + linearize
 #endif
@@ -466,7 +503,7 @@ __device__ __forceinline__ void block_reduce_store_staged(const Acc &acc, double
     double s = 0.0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; w++) s += wsum[w][lane];
-    out[lane] = s;
+    out[lane] = s * acc_scale(lane);
   }
 }
 template <bool kStructured>
@@ -500,8 +537,8 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   // per-tile constants for the two tiles the pipeline can span:
   // [0..11] gating T, [12..23] linearizer T, [24..31] the current cloud's
   // Omega parameters, then pair index, skip flag and structured-Omega flag
-  __shared__ float sT[2][32];
-  __shared__ int sPair[2], sSkip[2], sStruct[2], sSame[2];
+  __shared__ float sT[kConstSlots][32];
+  __shared__ int sPair[kConstSlots], sSkip[kConstSlots], sStruct[kConstSlots], sSame[kConstSlots];
   const bool stats_pass = flags & 8;
   if ((int)blockIdx.x >= total_tiles) return;
   const int ntiles = (total_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
@@ -611,7 +648,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   // Per-tile constants, written when the tile's first sub-tile enters G1.
   auto tile_constants = [&](int j) {
     if (j >= nsub || j % kSubsPerTile) return;
-    int e = (j / kSubsPerTile) & 1;
+    int e = (j / kSubsPerTile) % kConstSlots;
     lookup(tile_of(j), gt_tile, gt_pi, gt_skip);
     const int pi = gt_pi;
     const PairState *st = pairs[pi].state;
@@ -637,21 +674,19 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   auto gate_g2 = [&](int j) {
     if (j < nsub) {
       Stage &g = stage_of(j);
-      int e = (j / kSubsPerTile) & 1;
-      int acc_ok = 0;
+      int e = (j / kSubsPerTile) % kConstSlots;
       if constexpr (kStructured) {
         // structured: nothing to gather after the gate; it runs with the
         // linearizer in the main step
-        cp_async_commit();
-        return;
-      }
+        (void)g;
+        (void)e;
+      } else {
 #pragma unroll
-      for (int k = 0; k < kFusedPX; k++) {
-        const int sl = t + k * kFusedThreads;
-        acc_ok = 0;
-        if (g.valid[sl] && !sSkip[e]) {
-          acc_ok = gate(cp, sT[e], g.rp[sl], g.rn[sl], g.cp[sl], g.cn[sl]) ? 2 : 1;
-          if constexpr (!kStructured) {
+        for (int k = 0; k < kFusedPX; k++) {
+          const int sl = t + k * kFusedThreads;
+          int acc_ok = 0;
+          if (g.valid[sl] && !sSkip[e]) {
+            acc_ok = gate(cp, sT[e], g.rp[sl], g.rn[sl], g.cp[sl], g.cn[sl]) ? 2 : 1;
             if (acc_ok == 2 && !sStruct[e]) {
               const float4 *o = pairs[sPair[e]].cur_omg + 3 * (size_t)g.ci[sl];
               cp_async16(&g.o0[sl], o);
@@ -659,8 +694,8 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
               cp_async16(&g.o2[sl], o + 2);
             }
           }
+          g.valid[sl] = acc_ok;  // 0 none, 1 candidate rejected, 2 accepted
         }
-        g.valid[sl] = acc_ok;  // 0 none, 1 candidate rejected, 2 accepted
       }
     }
     cp_async_commit();
@@ -672,7 +707,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   // Linearizes sub-tile j (its gather -- and, for general Omega, its gate --
   // complete); at a tile's last sub-tile the CTA stores the tile's partial.
   auto consume = [&](int j) {
-    const int e = (j / kSubsPerTile) & 1;
+    const int e = (j / kSubsPerTile) % kConstSlots;
     const int sub = j % kSubsPerTile;
     if (sub == 0) {
 #pragma unroll
@@ -722,11 +757,12 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
     tile_constants(0);
     issue_g1(0);
     load_indices(1);
+    __syncthreads();          // tile 0's constants visible
     for (int j = 0; j < nsub; j++) {
       tile_constants(j + 1);
       issue_g1(j + 1);        // uses the indices loaded in the previous iteration
       load_indices(j + 2);
-      __syncthreads();        // tile constants visible
+      if ((j + 1) % kSubsPerTile == 0) __syncthreads();  // the next tile's constants visible
       cp_async_wait<1>();     // G1(j) complete (G1(j+1) may be in flight)
       consume(j);
     }
@@ -746,7 +782,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
       tile_constants(j + 2);
       issue_g1(j + 2);          // uses the indices loaded in the previous iteration
       load_indices(j + 3);
-      __syncthreads();          // tile constants visible; slots of j-1 fully consumed
+      if ((j + 2) % kSubsPerTile == 0) __syncthreads();  // the constants of j + 2's tile visible
       cp_async_wait<2>();       // G1(j+1) complete (groups after it: G2(j), G1(j+2))
       gate_g2(j + 1);
       cp_async_wait<2>();       // G2(j) complete (groups after it: G1(j+2), G2(j+1))
@@ -764,7 +800,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
 // (strictly closer AND strictly better aligned); -1 when none passes.
 __device__ int multi_best(const PairDev &pd, const CorrParams &cp, const float *Tg, int p, int ri, int ncur) {
   const float4 rn0 = pd.ref_nrm[ri];
-  if (dot3g(rn0.x, rn0.y, rn0.z, rn0.x, rn0.y, rn0.z) == 0.0f) return -1;
+  if (normal_is_zero(rn0.x, rn0.y, rn0.z)) return -1;
   const float3 rp = xform_point_g(Tg, pd.ref_pts[ri]);
   const float3 rn = xform_normal_g(Tg, rn0);
   float kr = rn0.w;
@@ -779,7 +815,7 @@ __device__ int multi_best(const PairDev &pd, const CorrParams &cp, const float *
       const int ci = pd.cur_index[r2 * pd.cols + c2];
       if (ci < 0 || ci >= ncur) continue;
       const float4 cn = pd.cur_nrm[ci];
-      if (dot3g(cn.x, cn.y, cn.z, cn.x, cn.y, cn.z) == 0.0f) continue;
+      if (normal_is_zero(cn.x, cn.y, cn.z)) continue;
       const float nd = dot3g(cn.x, cn.y, cn.z, rn.x, rn.y, rn.z);
       if (nd < cp.cos_thr) continue;
       const float4 cpt = pd.cur_pts[ci];

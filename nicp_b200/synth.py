@@ -103,8 +103,12 @@ def rel(pose_ref, pose_cur):
 
 
 def rot_angle(R):
-    c = (np.trace(R[:3, :3]) - 1) / 2
-    return math.acos(max(-1.0, min(1.0, c)))
+    """Rotation angle of R: atan2(|axis term|, trace term), accurate at small
+    angles (acos((tr - 1) / 2) loses half the digits there, and clips to 0
+    when a float32 rotation's rounding puts the trace above 3)."""
+    R = np.asarray(R, float)[:3, :3]
+    s = math.sqrt((R[2, 1] - R[1, 2]) ** 2 + (R[0, 2] - R[2, 0]) ** 2 + (R[1, 0] - R[0, 1]) ** 2)
+    return math.atan2(s, np.trace(R) - 1.0)
 
 
 def pose_error(T_est, T_ref):

@@ -253,6 +253,48 @@ def test_correspond_multi_bitexact(ctx, pair, region, threads):
     assert not np.array_equal(gp, single)
 
 
+def test_correspond_zero_normal_edges(ctx):
+    """The gates' zero-normal test (squaredNorm() == 0 in float,
+    correspondencefinderprojective.cpp:69) on normals at its edge: components
+    at and one ulp either side of 2^-75, subnormals, NaN, infinity.  Points
+    coincide, curvatures are equal and any normal angle is accepted, so the
+    list depends on that test alone; it must equal the REF32 oracle's."""
+    rows, cols = 16, 32
+    n = rows * cols
+    t = np.float32(2.0 ** -75)
+    vals = np.array([0.0, t, -t, np.nextafter(t, np.float32(1)), np.nextafter(t, np.float32(0)), 1e-40, 2.7e-23,
+                     0.6, np.nan, np.inf], np.float32)
+    rng = np.random.default_rng(11)
+
+    def normals():
+        nn = np.zeros((n, 4), np.float32)
+        nn[:, :3] = vals[rng.integers(0, len(vals), (n, 3))]
+        nn[rng.random(n) < 0.2, :3] = 0.0
+        return nn
+
+    pts = np.ones((n, 4), np.float32)
+    pts[:, 0] = np.arange(n) % cols * 0.01
+    pts[:, 1] = np.arange(n) // cols * 0.01
+    pts[:, 2] = 2.0
+    rn, cn = normals(), normals()
+    curv = np.zeros(n, np.float32)
+    ref, cur = api.Cloud(ctx), api.Cloud(ctx)
+    ref.upload(pts, rn, curv)
+    cur.upload(pts, cn, curv)
+    idx = np.arange(n, dtype=np.int32).reshape(rows, cols)
+    cf = api.CorrespondenceFinderProjective(ctx)
+    cf.setInlierNormalAngularThreshold(-2.0)
+    cf.setReferenceIndexImage(idx)
+    cf.setCurrentIndexImage(idx)
+    gp = cf.compute(ref, cur, np.eye(4, dtype=np.float32))
+    oref = O.Cloud.from_arrays(O.REF32, pts.astype(float), rn.astype(float), curv.astype(float))
+    ocur = O.Cloud.from_arrays(O.REF32, pts.astype(float), cn.astype(float), curv.astype(float))
+    prm = O.align_params(inlier_normal_angular_threshold=-2.0)
+    op = O.correspond(O.REF32, oref, ocur, idx, idx, np.eye(4), prm)
+    assert 50 < len(op) < n - 50, len(op)
+    assert np.array_equal(gp, op)
+
+
 def test_align_with_search_region_vs_f64(ctx, pair):
     """AlignerProjective with a 1 x 1 search window (list path on the device)
     against the FP64 oracle loop with the same window on the same float

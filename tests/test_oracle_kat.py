@@ -383,3 +383,29 @@ def test_pose_sensitivity_to_one_ulp_of_depth():
         moves.append(synth.pose_error(O.align(O.F64, pa, pb, oc)["T"], T0))
     print("FP64 pose moved by one-ulp depth perturbations: %s" % ["%.2e rad %.2e m" % m for m in moves])
     assert max(m[0] for m in moves) > 1e-5
+
+
+def test_zero_normal_test_is_a_threshold():
+    """The gates' "squaredNorm() == 0" (correspondencefinderprojective.cpp:69)
+    is decided on the GPU as |x|, |y|, |z| <= 2^-75: a float sum of
+    non-negative squares is zero exactly when every square rounds to zero,
+    and x * x rounds to zero exactly at |x| <= 2^-75 (2^-150 ties to 0).
+    Checked here in float32 arithmetic on the edge values and on random
+    vectors spanning the subnormal range, NaN and infinity included."""
+    t = np.float32(2.0 ** -75)
+    edge = np.array([0.0, -0.0, t, -t, np.nextafter(t, np.float32(1)), np.nextafter(t, np.float32(0)),
+                     np.float32(1e-40), np.float32(2.6e-23), np.float32(2.7e-23), np.float32(1e-20), 1.0,
+                     np.inf, -np.inf, np.nan], np.float32)
+    g = np.array(np.meshgrid(edge, edge, edge)).reshape(3, -1).T
+    rng = np.random.default_rng(7)
+    r = (rng.standard_normal((200000, 3)) * np.float32(2.0) ** rng.integers(-160, 10, (200000, 3))).astype(np.float32)
+    r[rng.random(200000) < 0.3, 0] = 0.0
+    v = np.concatenate([g, r]).astype(np.float32)
+    with np.errstate(over="ignore", under="ignore", invalid="ignore"):
+        x, y, z = v[:, 0], v[:, 1], v[:, 2]
+        sq = ((x * x + y * y) + z * z).astype(np.float32)  # float32 throughout
+        assert sq.dtype == np.float32
+        zero_by_sum = sq == np.float32(0)
+        zero_by_thr = (np.abs(x) <= t) & (np.abs(y) <= t) & (np.abs(z) <= t)
+    assert np.array_equal(zero_by_sum, zero_by_thr)
+    assert zero_by_thr.sum() > 100 and (~zero_by_thr).sum() > 100

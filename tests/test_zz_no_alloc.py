@@ -2,8 +2,9 @@
 device memory (a real-time loop that cannot pay for cudaMalloc's
 synchronisation, or a framework that owns all device memory).  Its partial
 sums live in a fixed array inside the library, so it must give the same
-H, b, error and inliers as nicp_linearize, and two calls in a row must not
-see each other's leftovers in that shared array.
+H, b, error and inliers as nicp_linearize -- and, directly, as the FP64
+oracle's linearizer on the same clouds and correspondences -- and two calls
+in a row must not see each other's leftovers in that shared array.
 
 This file is collected last on purpose: it must pass both alone in a fresh
 process and after every other test."""
@@ -15,7 +16,9 @@ import pytest
 from nicp_b200 import _lib as L
 from nicp_b200 import api, synth
 
-from helpers import converter, float_T, gpu_cloud, perturb
+from oracle import oracle as O
+
+from helpers import converter, float_T, gpu_cloud, oracle_cloud_from_gpu, perturb
 
 pytestmark = pytest.mark.gpu
 
@@ -54,6 +57,8 @@ def test_noalloc_linearize_matches_nicp_linearize(ctx):
     assert len(pairs) > 1000
     lin = api.Linearizer(ctx)
     lp = lin.params()
+    oref = oracle_cloud_from_gpu(O.F64, ref.download())
+    ocur = oracle_cloud_from_gpu(O.F64, cur.download())
     # two calls in a row with different inputs: the second must not inherit
     # anything from the first through the shared partial-sum array
     T2 = (np.linalg.inv(float_T(Tgt)) @ perturb(4, 0.5, 0.01)).astype(np.float32)
@@ -64,6 +69,22 @@ def test_noalloc_linearize_matches_nicp_linearize(ctx):
         assert inl == lin.inliers()
         assert _rel(H, lin.H()) < 1e-5 and _rel(b, lin.b()) < 1e-5
         assert abs(err - lin.error()) <= 1e-5 * abs(lin.error())
+        # against the FP64 oracle (with threads > 1 the last K % threads
+        # correspondences are dropped, as the reference drops them): H and the
+        # error within 1e-5 relative; b within 1e-5 relative away from the
+        # solution (T2), while at the true pose (Tinv) b is the small remainder
+        # of terms that cancel, so there the bar is on what b is for: the
+        # Gauss-Newton step H^-1 b moves by less than 1e-7 (rad, m), a hundredth
+        # of the pose bar
+        kk = (len(sub) // threads) * threads
+        Ho, bo, erro, inlo = O.linearize(O.F64, oref, ocur, sub[:kk], T.astype(np.float64))
+        assert inl == inlo
+        assert _rel(H, Ho) < 1e-5, _rel(H, Ho)
+        assert abs(err - erro) <= 1e-5 * abs(erro)
+        step_diff = np.abs(np.linalg.solve(Ho, b - bo)).max()
+        assert step_diff < 1e-7, step_diff
+        if T is T2:
+            assert _rel(b, bo) < 1e-5, _rel(b, bo)
 
 
 def test_noalloc_rejects_oversized_list(ctx):
