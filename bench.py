@@ -287,21 +287,23 @@ def oracle_pose_check(cases, threads=None):
     metres).  Where the truth is known, a case whose FP64 pose ends more than
     0.05 rad or 5 cm from it is an alignment the algorithm itself does not
     converge on; such cases are counted apart ("diverged") and kept out of
-    the converged maxima."""
+    the converged maxima.  A case outside 1e-5 rad / 0.05 mm is listed with
+    how far the FP64 loop still moved in its last outer iteration (0 when it
+    stopped on its own exit test) and how far the reference's own FP32
+    pipeline (the REF32 oracle) ends from FP64 on it."""
     from oracle import oracle as O
     from nicp_b200 import synth
     threads = threads or os.cpu_count()
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    errs, diverged = [], []
+    errs, diverged, outside = [], [], []
     for c in cases:
         cam = c["cam"]
         oc = O.camera(cam["rows"], cam["cols"], cam["fx"], cam["fy"], cam["cx"], cam["cy"],
                       max_distance=cam.get("max_distance", 6.0))
         a, _ = O.build_cloud(O.F64, c["d1"], oc)
         b, _ = O.build_cloud(O.F64, c["d2"], oc)
-        r = O.align(O.F64, a, b, oc, guess=c["guess"],
-                    prm=O.align_params(outer_iterations=c["outer"], inner_iterations=c["inner"],
-                                       early_exit_eps=c["eps"]))
+        prm = O.align_params(outer_iterations=c["outer"], inner_iterations=c["inner"], early_exit_eps=c["eps"])
+        r = O.align(O.F64, a, b, oc, guess=c["guess"], prm=prm)
         e = synth.pose_error(c["T"], r["T"])
         if c["truth"] is not None:
             tr, tt = synth.pose_error(r["T"], c["truth"])
@@ -309,11 +311,24 @@ def oracle_pose_check(cases, threads=None):
                 diverged.append({"rad": float(e[0]), "m": float(e[1]), "f64_vs_truth_rad": float(tr)})
                 continue
         errs.append(e)
+        if e[0] > 1e-5 or e[1] > 5e-5:
+            last = (0.0, 0.0)
+            if r["outer_iterations_run"] >= c["outer"] and c["outer"] > 1:
+                prm.outer_iterations = c["outer"] - 1
+                last = synth.pose_error(r["T"], O.align(O.F64, a, b, oc, guess=c["guess"], prm=prm)["T"])
+                prm.outer_iterations = c["outer"]
+            a32, _ = O.build_cloud(O.REF32, c["d1"], oc)
+            b32, _ = O.build_cloud(O.REF32, c["d2"], oc)
+            q = synth.pose_error(O.align(O.REF32, a32, b32, oc, guess=c["guess"], prm=prm)["T"], r["T"])
+            outside.append({"rad": float(e[0]), "m": float(e[1]), "f64_last_step_rad": float(last[0]),
+                            "f64_last_step_m": float(last[1]), "ref32_vs_f64_rad": float(q[0]),
+                            "ref32_vs_f64_m": float(q[1])})
     er = np.array([e[0] for e in errs]) if errs else np.zeros(1)
     et = np.array([e[1] for e in errs]) if errs else np.zeros(1)
     return {"pairs": len(errs), "rad_max": float(er.max()), "rad_p99": float(np.percentile(er, 99)),
             "rad_median": float(np.median(er)), "m_max": float(et.max()), "m_p99": float(np.percentile(et, 99)),
-            "within_1e-5rad_0.05mm": int(np.sum((er <= 1e-5) & (et <= 5e-5))), "diverged": diverged}
+            "within_1e-5rad_0.05mm": int(np.sum((er <= 1e-5) & (et <= 5e-5))), "outside_1e-5rad_0.05mm": outside,
+            "diverged": diverged}
 
 
 def reference_arm(args, rank, world):
