@@ -135,8 +135,21 @@ struct Acc {
   // The rotational Jacobian block is skew(2 p) (linearizer.cpp:59-100); the
   // per-pixel terms use skew(p), so Htr and br hold half and Hrr a quarter of
   // their values, and the reductions scale the FP64 tile sums by 2 and 4
-  // (exact: powers of two).
-  float v[31];
+  // (exact: powers of two).  The three counts (28 inliers, 29 candidates,
+  // 30 accepted) share one integer, 10 bits each (a thread adds at most 8
+  // pixels or 4 list entries to a tile partial).
+  float v[28];
+  unsigned cnt;
+  static constexpr unsigned kInlier = 1u, kCandidate = 1u << 10, kAccepted = 1u << 20;
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int k = 0; k < 28; k++) v[k] = 0.0f;
+    cnt = 0u;
+  }
+  // element k of the partial (0..30) as a float
+  __device__ __forceinline__ float get(int k) const {
+    return k < 28 ? v[k] : (float)((cnt >> (10 * (k - 28))) & 1023u);
+  }
 };
 // Power-of-two factor of each Acc element (see Acc).
 __device__ __forceinline__ double acc_scale(int k) {
@@ -244,7 +257,7 @@ __device__ __forceinline__ void lin_terms(const LinParams &lp, const float *T12,
     else return;
   }
   acc.v[27] += ks * le;
-  acc.v[28] += 1.0f;
+  acc.cnt += Acc::kInlier;
   // skew(v) = [[0, c, -b], [-c, 0, a], [b, -a, 0]], (a, b, c) = v (the
   // Jacobian's factor 2 is applied to the tile sums, see Acc)
   float a = rp.x, b = rp.y, c = rp.z;
@@ -333,7 +346,7 @@ __device__ __forceinline__ void lin_terms_structured_xf(const LinParams &lp, con
     en0 *= ks; en1 *= ks; en2 *= ks;
   }
   acc.v[27] += le;
-  acc.v[28] += 1.0f;
+  acc.cnt += Acc::kInlier;
   const float a = rp.x, b = rp.y, c = rp.z;
   const float an = rn.x, bn = rn.y, cn2 = rn.z;
   // Htt += Omega_p
@@ -390,7 +403,7 @@ __device__ __forceinline__ void block_reduce_store(const Acc &acc, double *out) 
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double v[32];
 #pragma unroll
-  for (int k = 0; k < 31; k++) v[k] = (double)acc.v[k];
+  for (int k = 0; k < 31; k++) v[k] = (double)acc.get(k);
   v[31] = 0.0;
   // butterfly reduce-scatter: lane L ends with the warp total of element L
 #pragma unroll
@@ -483,7 +496,7 @@ __device__ __forceinline__ void block_reduce_store_staged(const Acc &acc, double
   };
   __syncwarp();  // every lane of the warp is done with its slots of this stage
 #pragma unroll
-  for (int k = 0; k < 31; k++) row_of(k)[lane] = acc.v[k];
+  for (int k = 0; k < 31; k++) row_of(k)[lane] = acc.get(k);
   __syncwarp();
   double v = 0.0;
   if (lane < 31) {
@@ -616,7 +629,10 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
           if (p < P) {
             int ri;
             if (flags & 1) {
-              ri = zbuf_index(zI[k], drop_no_normal);
+              // an empty word (all ones) decodes to -1 with drop_no_normal
+              // and to 2^31 - 1 without, which the bounds test below rejects
+              const unsigned lo = (unsigned)zI[k];
+              ri = (drop_no_normal && (lo & 1u)) ? -1 : (int)(lo >> 1);
               ci[k] = cI[k];
               if (flags & 2) pd.zbuf[p] = ~0ull;
               if (flags & 4) pd.ref_index[p] = ri;
@@ -624,7 +640,7 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
               ri = cI[k];
               ci[k] = (int)(unsigned)zI[k];
             }
-            valid[k] = ri >= 0 && ci[k] >= 0 && ri < gt_rc && ci[k] < gt_cc;
+            valid[k] = (unsigned)ri < (unsigned)gt_rc && (unsigned)ci[k] < (unsigned)gt_cc;
             if (valid[k] && cp.row_limit_threads > 1)
               valid[k] = p / pd.cols < (pd.rows / cp.row_limit_threads) * cp.row_limit_threads;
             if (valid[k]) {
@@ -702,16 +718,14 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
   };
 
   Acc acc;
-#pragma unroll
-  for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
+  acc.zero();
   // Linearizes sub-tile j (its gather -- and, for general Omega, its gate --
   // complete); at a tile's last sub-tile the CTA stores the tile's partial.
   auto consume = [&](int j) {
     const int e = (j / kSubsPerTile) % kConstSlots;
     const int sub = j % kSubsPerTile;
     if (sub == 0) {
-#pragma unroll
-      for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
+      acc.zero();
     }
     if (!sSkip[e]) {
       const Stage &g = stage_of(j);
@@ -721,11 +735,11 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
         const int v = g.valid[sl];
         if constexpr (kStructured) {
           if (v) {
-            acc.v[29] += 1.0f;
+            acc.cnt += Acc::kCandidate;
             const float4 rp0 = g.rp[sl], rn0 = g.rn[sl], cpt = g.cp[sl], cn = g.cn[sl];
             float3 rp, rn;
             if (gate_t(cp, sT[e], rp0, rn0, cpt, cn, rp, rn)) {
-              acc.v[30] += 1.0f;
+              acc.cnt += Acc::kAccepted;
               if (sSame[e] && !cp.demoted)
                 lin_terms_structured_xf(lp, sT[e] + 24, rp, rn, cpt, cn, acc);
               else
@@ -733,9 +747,9 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
             }
           }
         } else {
-          if (v) acc.v[29] += 1.0f;
+          if (v) acc.cnt += Acc::kCandidate;
           if (v == 2) {
-            acc.v[30] += 1.0f;
+            acc.cnt += Acc::kAccepted;
             if (sStruct[e])
               lin_terms_structured(lp, sT[e] + 12, sT[e] + 24, g.rp[sl], g.rn[sl], g.cp[sl], g.cn[sl], acc);
             else
@@ -959,8 +973,7 @@ __global__ void __launch_bounds__(kCorrThreads) k_lin_list(const PairDev *__rest
   for (int k = 0; k < 12; k++) Tl[k] = src[k];
   const int nref = *pd.ref_count, ncur = *pd.cur_count;
   Acc acc;
-#pragma unroll
-  for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
+  acc.zero();
   int i0 = tile * kCorrTilePixels + threadIdx.x * 4;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
@@ -968,8 +981,8 @@ __global__ void __launch_bounds__(kCorrThreads) k_lin_list(const PairDev *__rest
     if (i >= K) break;
     int ri = pd.pairs[2 * i], ci = pd.pairs[2 * i + 1];
     if (ri < 0 || ci < 0 || ri >= nref || ci >= ncur) continue;
-    acc.v[29] += 1.0f;
-    acc.v[30] += 1.0f;
+    acc.cnt += Acc::kCandidate;
+    acc.cnt += Acc::kAccepted;
     const float4 *o = pd.cur_omg + 3 * (size_t)ci;
     lin_terms(lp, Tl, pd.ref_pts[ri], pd.ref_nrm[ri], pd.cur_pts[ci], pd.cur_nrm[ci], o[0], o[1], o[2], acc);
   }
@@ -1258,8 +1271,7 @@ __global__ void __launch_bounds__(kCorrThreads) k_lin_noalloc(NoAllocLinArgs a, 
   if (a.parity_threads > 1) K = (K / a.parity_threads) * a.parity_threads;
   const int nref = *a.ref_count, ncur = *a.cur_count;
   Acc acc;
-#pragma unroll
-  for (int k = 0; k < 31; k++) acc.v[k] = 0.0f;
+  acc.zero();
   const int i0 = tile * kCorrTilePixels + threadIdx.x * 4;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
@@ -1267,8 +1279,8 @@ __global__ void __launch_bounds__(kCorrThreads) k_lin_noalloc(NoAllocLinArgs a, 
     if (i >= K) break;
     const int ri = a.pairs[2 * i], ci = a.pairs[2 * i + 1];
     if (ri < 0 || ci < 0 || ri >= nref || ci >= ncur) continue;
-    acc.v[29] += 1.0f;
-    acc.v[30] += 1.0f;
+    acc.cnt += Acc::kCandidate;
+    acc.cnt += Acc::kAccepted;
     const float4 *o = a.cur_omg + 3 * (size_t)ci;
     lin_terms(a.lp, a.T, a.ref_pts[ri], a.ref_nrm[ri], a.cur_pts[ci], a.cur_nrm[ci], o[0], o[1], o[2], acc);
   }
