@@ -182,6 +182,22 @@ __device__ __forceinline__ float rowg(const float *A, float x, float y, float z)
   s = fa(s, fm(A[1], y));
   return fa(s, fm(A[2], z));
 }
+// rowg with its first two products in one packed multiply (sm_100 FMUL2;
+// each half is rounded as __fmul_rn rounds it, so the sum is bitwise rowg's):
+// ((A0 x + A1 y) + A2 z).  A is read element by element (it may be a
+// thread's register array as well as a shared row).
+__device__ __forceinline__ float rowg2(const float *A, float2 xy, float z) {
+  const float2 m = __fmul2_rn(make_float2(A[0], A[1]), xy);
+  return fa(fa(m.x, m.y), fm(A[2], z));
+}
+__device__ __forceinline__ float3 xform_point_g2(const float *A, float4 p) {
+  const float2 xy = make_float2(p.x, p.y);
+  return make_float3(fa(rowg2(A, xy, p.z), A[3]), fa(rowg2(A + 4, xy, p.z), A[7]), fa(rowg2(A + 8, xy, p.z), A[11]));
+}
+__device__ __forceinline__ float3 xform_normal_g2(const float *A, float4 n) {
+  const float2 xy = make_float2(n.x, n.y);
+  return make_float3(rowg2(A, xy, n.z), rowg2(A + 4, xy, n.z), rowg2(A + 8, xy, n.z));
+}
 __device__ __forceinline__ float3 xform_normal_g(const float *A, float4 n) {
   return make_float3(rowg(A, n.x, n.y, n.z), rowg(A + 4, n.x, n.y, n.z), rowg(A + 8, n.x, n.y, n.z));
 }
@@ -201,11 +217,11 @@ __device__ __forceinline__ bool gate_t(const CorrParams &cp, const float *T12, f
     if (normal_is_zero(cn.x, cn.y, cn.z)) return false;
     if (normal_is_zero(rn0.x, rn0.y, rn0.z)) return false;
   }
-  rp = xform_point_g(T12, rp0);
+  rp = xform_point_g2(T12, rp0);
   float dx = fsb(cpt.x, rp.x), dy = fsb(cpt.y, rp.y), dz = fsb(cpt.z, rp.z);
   if (dot3g(dx, dy, dz, dx, dy, dz) > cp.sq_thr) return false;
   if (!cp.demoted) {
-    rn = xform_normal_g(T12, rn0);
+    rn = xform_normal_g2(T12, rn0);
     if (dot3g(cn.x, cn.y, cn.z, rn.x, rn.y, rn.z) < cp.cos_thr) return false;
     float kr = rn0.w, kc = cn.w;
     if (kr < cp.flat_thr) kr = cp.flat_thr;
