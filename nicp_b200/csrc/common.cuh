@@ -372,43 +372,84 @@ __device__ inline void d_eig3(const double *A, double *lam, double *U) {
   for (int r = 0; r < 3; r++) { U[r * 3 + 0] = v0[r]; U[r * 3 + 1] = v1[r]; U[r * 3 + 2] = v2[r]; }
 }
 
-// Solve A x = b for a symmetric 6x6 A given by its lower triangle.
-__device__ inline void d_ldlt_solve6(const double *A, const double *b, double *x) {
+// Solve A x = b for a symmetric 6x6 A given by its lower triangle: LDL^T
+// with symmetric diagonal pivoting.  Every index is a compile-time constant
+// (the pivot's row and column swaps are predicated per candidate), so the
+// factor stays in registers.
+__device__ __forceinline__ void d_ldlt_solve6(const double *A, const double *b, double *x) {
   double M[6][6];
   int perm[6];
+#pragma unroll
   for (int i = 0; i < 6; i++) {
     perm[i] = i;
+#pragma unroll
     for (int j = 0; j < 6; j++) M[i][j] = (i >= j) ? A[i * 6 + j] : A[j * 6 + i];
   }
   double d[6];
+#pragma unroll
   for (int k = 0; k < 6; k++) {
     int piv = k;
     double best = fabs(M[k][k]);
+#pragma unroll
     for (int i = k + 1; i < 6; i++)
       if (fabs(M[i][i]) > best) { best = fabs(M[i][i]); piv = i; }
-    if (piv != k) {
-      for (int j = 0; j < 6; j++) { double t = M[k][j]; M[k][j] = M[piv][j]; M[piv][j] = t; }
-      for (int i = 0; i < 6; i++) { double t = M[i][k]; M[i][k] = M[i][piv]; M[i][piv] = t; }
-      int t = perm[k]; perm[k] = perm[piv]; perm[piv] = t;
+#pragma unroll
+    for (int i = k + 1; i < 6; i++) {
+      const bool sw = piv == i;
+#pragma unroll
+      for (int j = 0; j < 6; j++) {
+        const double a = M[k][j], c = M[i][j];
+        M[k][j] = sw ? c : a;
+        M[i][j] = sw ? a : c;
+      }
+#pragma unroll
+      for (int r = 0; r < 6; r++) {
+        const double a = M[r][k], c = M[r][i];
+        M[r][k] = sw ? c : a;
+        M[r][i] = sw ? a : c;
+      }
+      const int a = perm[k], c = perm[i];
+      perm[k] = sw ? c : a;
+      perm[i] = sw ? a : c;
     }
     d[k] = M[k][k];
     double col[6];
+#pragma unroll
     for (int i = k + 1; i < 6; i++) col[i] = M[i][k];
+#pragma unroll
     for (int i = k + 1; i < 6; i++) M[i][k] = col[i] / d[k];
+#pragma unroll
     for (int i = k + 1; i < 6; i++)
+#pragma unroll
       for (int j = k + 1; j <= i; j++) {
         M[i][j] = M[i][j] - M[i][k] * col[j];
         M[j][i] = M[i][j];
       }
   }
   double y[6];
-  for (int i = 0; i < 6; i++) y[i] = b[perm[i]];
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    y[i] = b[0];
+#pragma unroll
+    for (int j = 1; j < 6; j++) y[i] = perm[i] == j ? b[j] : y[i];
+  }
+#pragma unroll
   for (int i = 0; i < 6; i++)
+#pragma unroll
     for (int j = 0; j < i; j++) y[i] = y[i] - M[i][j] * y[j];
+#pragma unroll
   for (int i = 0; i < 6; i++) y[i] = y[i] / d[i];
+#pragma unroll
   for (int i = 5; i >= 0; i--)
+#pragma unroll
     for (int j = i + 1; j < 6; j++) y[i] = y[i] - M[j][i] * y[j];
-  for (int i = 0; i < 6; i++) x[perm[i]] = y[i];
+#pragma unroll
+  for (int j = 0; j < 6; j++) {  // x[perm[i]] = y[i]
+    double v = y[0];
+#pragma unroll
+    for (int i = 1; i < 6; i++) v = perm[i] == j ? y[i] : v;
+    x[j] = v;
+  }
 }
 
 // bm_se3.h:10-52 in FP64.
@@ -431,7 +472,9 @@ __device__ inline void d_v2t(const double *x, double *T) {
 // Shepperd's method, normalised, vector part with w >= 0.
 __device__ inline void d_t2v(const double *T, double *x) {
   double R[3][3];
+#pragma unroll
   for (int i = 0; i < 3; i++)
+#pragma unroll
     for (int j = 0; j < 3; j++) R[i][j] = T[i * 4 + j];
   double qx, qy, qz, qw;
   double tr = R[0][0] + R[1][1] + R[2][2];
@@ -443,18 +486,34 @@ __device__ inline void d_t2v(const double *T, double *x) {
     qy = (R[0][2] - R[2][0]) * s;
     qz = (R[1][0] - R[0][1]) * s;
   } else {
+    // the largest diagonal entry i picks the component computed first, with
+    // (j, k) = (i + 1, i + 2) mod 3 -- written out per i, so that every
+    // index is a compile-time constant
     int i = 0;
     if (R[1][1] > R[0][0]) i = 1;
-    if (R[2][2] > R[i][i]) i = 2;
-    int j = (i + 1) % 3, k = (j + 1) % 3;
-    double s = sqrt(R[i][i] - R[j][j] - R[k][k] + 1.0);
-    double q[3];
-    q[i] = 0.5 * s;
-    s = 0.5 / s;
-    qw = (R[k][j] - R[j][k]) * s;
-    q[j] = (R[j][i] + R[i][j]) * s;
-    q[k] = (R[k][i] + R[i][k]) * s;
-    qx = q[0]; qy = q[1]; qz = q[2];
+    if (R[2][2] > (i == 1 ? R[1][1] : R[0][0])) i = 2;
+    if (i == 0) {
+      double s = sqrt(R[0][0] - R[1][1] - R[2][2] + 1.0);
+      qx = 0.5 * s;
+      s = 0.5 / s;
+      qw = (R[2][1] - R[1][2]) * s;
+      qy = (R[1][0] + R[0][1]) * s;
+      qz = (R[2][0] + R[0][2]) * s;
+    } else if (i == 1) {
+      double s = sqrt(R[1][1] - R[2][2] - R[0][0] + 1.0);
+      qy = 0.5 * s;
+      s = 0.5 / s;
+      qw = (R[0][2] - R[2][0]) * s;
+      qz = (R[2][1] + R[1][2]) * s;
+      qx = (R[0][1] + R[1][0]) * s;
+    } else {
+      double s = sqrt(R[2][2] - R[0][0] - R[1][1] + 1.0);
+      qz = 0.5 * s;
+      s = 0.5 / s;
+      qw = (R[1][0] - R[0][1]) * s;
+      qx = (R[0][2] + R[2][0]) * s;
+      qy = (R[1][2] + R[2][1]) * s;
+    }
   }
   double n = sqrt(qx * qx + qy * qy + qz * qz + qw * qw);
   qx /= n; qy /= n; qz /= n; qw /= n;
@@ -464,15 +523,20 @@ __device__ inline void d_t2v(const double *T, double *x) {
 }
 
 __device__ inline void d_mm4(const double *A, const double *B, double *C) {
+#pragma unroll
   for (int i = 0; i < 4; i++)
+#pragma unroll
     for (int j = 0; j < 4; j++)
       C[i * 4 + j] = A[i * 4 + 0] * B[0 * 4 + j] + A[i * 4 + 1] * B[1 * 4 + j] + A[i * 4 + 2] * B[2 * 4 + j] +
                      A[i * 4 + 3] * B[3 * 4 + j];
 }
 
 __device__ inline void d_iso_inverse(const double *T, double *R) {
+#pragma unroll
   for (int i = 0; i < 3; i++)
+#pragma unroll
     for (int j = 0; j < 3; j++) R[i * 4 + j] = T[j * 4 + i];
+#pragma unroll
   for (int i = 0; i < 3; i++)
     R[i * 4 + 3] = -(R[i * 4 + 0] * T[3] + R[i * 4 + 1] * T[7] + R[i * 4 + 2] * T[11]);
   R[12] = 0; R[13] = 0; R[14] = 0; R[15] = 1;

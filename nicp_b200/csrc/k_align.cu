@@ -1075,32 +1075,49 @@ __global__ void __launch_bounds__(128) k_solve(const PairDev *__restrict__ pairs
     if (threadIdx.x < 32)
       tot[e] = (double)((((float)part[0][e] + (float)part[1][e]) + (float)part[2][e]) + (float)part[3][e]);
   } else {
+    // the fixed order t = g, g + 4, ..., with eight loads in flight
     double s = 0.0;
-    for (int t = g; t < nt; t += 4) s += pd.partials[(size_t)t * kPartialWords + e];
+    int t = g;
+    for (; t + 28 < nt; t += 32) {
+      double v[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) v[q] = pd.partials[(size_t)(t + 4 * q) * kPartialWords + e];
+#pragma unroll
+      for (int q = 0; q < 8; q++) s += v[q];
+    }
+    for (; t < nt; t += 4) s += pd.partials[(size_t)t * kPartialWords + e];
     part[g][e] = s;
     __syncthreads();
     if (threadIdx.x < 32) tot[e] = ((part[0][e] + part[1][e]) + part[2][e]) + part[3][e];
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
-  const int li[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
+  // (every index below is a compile-time constant: H, b and A stay in registers)
+  constexpr int li[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
   double H[36], b[6];
+#pragma unroll
   for (int q = 0; q < 6; q++) {
-    int i = li[q][0], j = li[q][1];
+    const int i = li[q][0], j = li[q][1];
     H[i * 6 + j] = H[j * 6 + i] = tot[q];
     H[(3 + i) * 6 + 3 + j] = H[(3 + j) * 6 + 3 + i] = tot[15 + q];
   }
+#pragma unroll
   for (int i = 0; i < 3; i++)
+#pragma unroll
     for (int j = 0; j < 3; j++) {
       H[i * 6 + 3 + j] = tot[6 + i * 3 + j];
       H[(3 + j) * 6 + i] = tot[6 + i * 3 + j];
     }
+#pragma unroll
   for (int i = 0; i < 3; i++) { b[i] = tot[21 + i]; b[3 + i] = tot[24 + i]; }
   if (mode & 4) {
+#pragma unroll
     for (int k = 0; k < 36; k++) st->Hstat[k] = H[k];
     return;
   }
+#pragma unroll
   for (int k = 0; k < 36; k++) st->H[k] = H[k];
+#pragma unroll
   for (int k = 0; k < 6; k++) st->b[k] = b[k];
   st->error = (float)tot[27];
   st->inliers = (int)tot[28];
@@ -1109,7 +1126,9 @@ __global__ void __launch_bounds__(128) k_solve(const PairDev *__restrict__ pairs
   if (mode & 2) return;
   // H += lambda I; dx = H^-1 (-b); invT = v2t(dx) invT  (alignerprojective.cpp:72-95)
   double A[36], nb[6], dx[6];
+#pragma unroll
   for (int k = 0; k < 36; k++) A[k] = H[k];
+#pragma unroll
   for (int i = 0; i < 6; i++) { A[i * 6 + i] += (double)lambda; nb[i] = -b[i]; }
   d_ldlt_solve6(A, nb, dx);
   double dT[16], nT[16];
