@@ -779,6 +779,7 @@ def main():
     ap.add_argument("--serve-rates", default="500,2000,5000,10000,20000",
                     help="Poisson arrival rates (requests/s) of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per rate")
+    ap.add_argument("--serve-workers", type=int, default=4, help="server worker threads (one context each)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -966,7 +967,7 @@ def main():
     serving, serve_checks = None, []
     if not args.no_serve and rank == 0:
         serving, serve_checks = serve_leg(local, [float(r) for r in args.serve_rates.split(",")], args.serve_seconds,
-                                          args.seed)
+                                          args.seed, workers=args.serve_workers)
 
     cpu, oracle_seq, oracle_mixed, oracle_served = None, None, None, None
     if not args.no_cpu and rank == 0:
