@@ -173,7 +173,10 @@ def run_step(ctx, frames_ptrs, cam_c, prm_c, clouds, corr, lin, prm, on_device):
 
 # Algorithmic bytes per unit (the per-stage figures of the scope table):
 #   S1 unproject     2P + 4P + 12V          S2 moments   bands: 2P + 3 (10 s P / 16); sweep: 2P + 10 s P / 16 + 10 s P
-#   S3 stats + Omega 10 s P + 6P + 76V      S4 z-buffer  16V (the point and its w, which carries the
+#   S3 stats + Omega 10 s P + 6P + 28V      S4 z-buffer  16V (the point and its w, which carries the
+#                    (+ 48V when the information matrices are written out:
+#                    Stats kept or a general form; the headline leaves them
+#                    implicit)
 #                                                        "has a normal" bit of the key) + 8V atomics
 #   S5 corr + lin    8P + 56 C: both index images, then per correspondence
 #                    point xyz, normal xyz and curvature of both clouds; the
@@ -183,7 +186,7 @@ def run_step(ctx, frames_ptrs, cam_c, prm_c, clouds, corr, lin, prm, on_device):
 def build_bytes(P, V, s=8):
     """One frame build: S1 + band totals/carries + sweep + S3 (bytes)."""
     return (2 * P + 4 * P + 12 * V) + (2 * P + 3 * 10 * s * P / 16) + (2 * P + 10 * s * P / 16 + 10 * s * P) + \
-        (10 * s * P + 6 * P + 76 * V)
+        (10 * s * P + 6 * P + 28 * V)
 
 
 def align_bytes(P, V, C, outer, inner):
@@ -208,7 +211,7 @@ def algorithmic_bytes(kernel, P, V, C, launches_per_step, pairs):
     if kernel == "moments_sweep":  # depth, carry rows, every integral value written once
         return (2 * P + 10 * s * P / 16 + 10 * s * P) * pairs
     if kernel == "stats_omega":
-        return (10 * s * P + 6 * P + 76 * V) * pairs
+        return (10 * s * P + 6 * P + 28 * V) * pairs
     if kernel == "zbuffer":
         return (16 * V + 8 * V) * pairs
     if kernel == "corr_lin":
@@ -906,7 +909,7 @@ def main():
     per_launch_bytes = {
         "corr_lin": (20 * P + 56 * C) * npairs,
         "zbuffer": (16 * V + 8 * V) * npairs,
-        "stats_omega": (10 * 8 * P + 6 * P + 76 * V) * F,
+        "stats_omega": (10 * 8 * P + 6 * P + 28 * V) * F,  # implicit Omega
         "moments_bands": (2 * P + 3 * 80 * P / 16) * F / 2,  # two kernels per stage launch
         "moments_sweep": (2 * P + 80 * P / 16 + 80 * P) * F,
         "unproject": (2 * P + 4 * P + 12 * V) * F / 2,  # two kernels per stage launch

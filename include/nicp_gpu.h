@@ -260,7 +260,12 @@ int nicp_cloud_download_stats(nicp_cloud *cloud, float *eigval3, float *eigvec9,
 
 /* Any output may be NULL.  points4/normals4: n*4 floats (w = 1 / 0);
  * curvature: n; omega_p9/omega_n9: n*9 (3x3 blocks); eigval3: n*3;
- * eigvec9: n*9 (columns are eigenvectors; needs keep_stats). */
+ * eigvec9: n*9 (columns are eigenvectors; needs keep_stats).
+ * A cloud built with information matrices of the form U diag(d0, d1, d1) U^T
+ * and without keep_stats holds them implicitly (d1 I + (d0 - d1) n n^T from
+ * its float normal, evaluated in double and rounded once); the first call
+ * that needs them -- this download, the list-mode linearizer, an add of
+ * clouds with different forms -- writes them out on the context's stream. */
 int nicp_cloud_download(nicp_cloud *c, float *points4, float *normals4, float *curvature,
                         float *omega_p9, float *omega_n9, float *eigval3, float *eigvec9);
 int nicp_cloud_upload(nicp_cloud *c, int n, const float *points4, const float *normals4,

@@ -94,6 +94,11 @@ struct nicp_cloud {
   // clouds built with such parameters, false for uploaded ones
   bool omega_structured = false;
   float omd[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // false while Omega is implicit: a structured cloud built without Stats
+  // (the stats kernel leaves omg unwritten; the fused kernel rebuilds Omega
+  // from the normal, the class code and omd).  cloud_ensure_omg writes the
+  // matrices out for a reader that needs them.
+  mutable bool omg_valid = true;
   float4 *pts = nullptr, *nrm = nullptr, *omg = nullptr;
   float *eig = nullptr;
   float4 *gauss = nullptr;  // 3 float4 per point: mean, then the 9 covariance entries row-major
@@ -147,6 +152,16 @@ class DeviceScope {
     cudaError_t e_ = (call);                                                                   \
     if (e_ != cudaSuccess) return fail((ctx), NICP_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+// Writes out a cloud's implicit information matrices (see omg_valid), on the
+// stream of the context whose kernels will read them.
+static int cloud_ensure_omg(nicp_ctx *ctx, const nicp_cloud *c) {
+  if (!c || c->omg_valid) return NICP_OK;
+  launch_materialize_omg(c->pts, c->nrm, c->omg, c->count, c->capacity, c->omd, ctx->stream);
+  CK(ctx, cudaGetLastError());
+  c->omg_valid = true;
+  return NICP_OK;
+}
 
 static int ensure_ws(nicp_ctx *ctx, size_t bytes) {
   if (bytes <= ctx->ws_cap) return NICP_OK;
@@ -546,6 +561,7 @@ extern "C" int nicp_cloud_download(nicp_cloud *c, float *p4, float *n4, float *c
   if (rc) return rc;
   if (n == 0) return NICP_OK;
   if ((ev3 || U9) && !c->eig_valid) return fail(ctx, NICP_ESTATE, "cloud was built without keep_stats");
+  if ((rc = cloud_ensure_omg(ctx, c))) return rc;
   std::vector<float4> nrm(n), omg(3 * (size_t)n);
   std::vector<float> eig;
   if (p4) CK(ctx, cudaMemcpyAsync(p4, c->pts, 16 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
@@ -633,6 +649,7 @@ extern "C" int nicp_cloud_upload(nicp_cloud *c, int n, const float *p4, const fl
   if (rc) return rc;
   c->eig_valid = c->gauss_valid = false;
   c->omega_structured = false;
+  c->omg_valid = true;
   std::vector<float4> pts(n), nrm(n), omg(3 * (size_t)n);
   int counts[2] = {n, 0};
   for (int i = 0; i < n; i++) {
@@ -676,7 +693,8 @@ extern "C" int nicp_cloud_transform(nicp_cloud *c, const float T16[16]) {
   if ((rc = ensure_ws(ctx, L.off))) return rc;
   CK(ctx, cudaMemcpyAsync(ctx->ws + o, pin, 48, cudaMemcpyHostToDevice, ctx->stream));
   CK(ctx, cudaEventRecord(ctx->pin_up_ev, ctx->stream));
-  launch_cloud_transform(c->pts, c->nrm, c->omg, c->eig_valid ? c->eig : nullptr, c->gauss_valid ? c->gauss : nullptr,
+  launch_cloud_transform(c->pts, c->nrm, c->omg_valid ? c->omg : nullptr, c->eig_valid ? c->eig : nullptr,
+                         c->gauss_valid ? c->gauss : nullptr,
                          c->count, c->capacity, (const float *)(ctx->ws + o), ctx->stream, &ctx->prof);
   CK(ctx, cudaGetLastError());
   return NICP_OK;
@@ -913,6 +931,8 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       cl->gauss_valid = d.gauss != nullptr;
       cl->omega_structured = prm->pim_flat[1] == prm->pim_flat[2] && prm->pim_nonflat[1] == prm->pim_nonflat[2] &&
                              prm->nim_flat[1] == prm->nim_flat[2] && prm->nim_nonflat[1] == prm->nim_nonflat[2];
+      // the stats kernel's lean form (below) leaves Omega implicit
+      if (!unproject_only) cl->omg_valid = !(!prm->keep_stats && cl->omega_structured);
       {
         const float od[8] = {prm->pim_flat[0], prm->pim_flat[1], prm->pim_nonflat[0], prm->pim_nonflat[1],
                              prm->nim_flat[0], prm->nim_flat[1], prm->nim_nonflat[0], prm->nim_nonflat[1]};
@@ -1293,6 +1313,7 @@ extern "C" int nicp_linearize(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_c
   if ((rc = plan_pairs(ctx, 1, &cam, &ref, false, true, pl))) return rc;
   char *pin;
   if ((rc = pin_up(ctx, sizeof(PairDev) + 48 + 4, &pin))) return rc;
+  if ((rc = cloud_ensure_omg(ctx, cur))) return rc;  // the list linearizer reads the matrices
   PairDev *pd = (PairDev *)pin;
   fill_pairs(ctx, pl, &cam, &ref, &cur, pd);
   float *T12 = (float *)(pin + sizeof(PairDev));
@@ -1337,6 +1358,11 @@ extern "C" int nicp_linearize_noalloc(nicp_ctx *ctx, const nicp_cloud *ref, cons
   int device = -1;
   if (cudaGetDevice(&device) != cudaSuccess) return NICP_ECUDA;
   if (device != ctx->device) return NICP_ESTATE;
+  if (!cur->omg_valid) {  // an implicit Omega is written out first (no allocation)
+    launch_materialize_omg(cur->pts, cur->nrm, cur->omg, cur->count, cur->capacity, cur->omd, ctx->stream);
+    if (cudaGetLastError() != cudaSuccess) return NICP_ECUDA;
+    cur->omg_valid = true;
+  }
   NoAllocLinArgs a;
   a.ref_pts = ref->pts;
   a.ref_nrm = ref->nrm;
@@ -1605,6 +1631,7 @@ extern "C" int nicp_align_nn(nicp_ctx *ctx, const nicp_cloud *ref, const nicp_cl
   PairDev &d = *(PairDev *)pin;
   std::memset(&d, 0, sizeof(d));
   d.ref_pts = ref->pts; d.ref_nrm = ref->nrm; d.ref_count = ref->count;
+  if ((rc = cloud_ensure_omg(ctx, cur))) return rc;
   d.cur_pts = cur->pts; d.cur_nrm = cur->nrm; d.cur_omg = cur->omg; d.cur_count = cur->count;
   d.rows = 1;
   d.cols = std::max(pl.nr, 1);
@@ -1746,9 +1773,17 @@ extern "C" int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[
     if ((rc = cloud_grow(dst, cap, nd))) return rc;
   }
   cudaStream_t s = ctx->stream;
+  // the result keeps an implicit Omega when both parts have one (and the same
+  // parameters); otherwise both parts' matrices are written out first
+  const bool implicit = structured && !src->omg_valid && (empty || !dst->omg_valid);
+  if (!implicit) {
+    if ((rc = cloud_ensure_omg(ctx, src))) return rc;
+    if (!empty && (rc = cloud_ensure_omg(ctx, dst))) return rc;
+  }
   CK(ctx, cudaMemcpyAsync(dst->pts + nd, src->pts, 16 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
   CK(ctx, cudaMemcpyAsync(dst->nrm + nd, src->nrm, 16 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
-  CK(ctx, cudaMemcpyAsync(dst->omg + 3 * (size_t)nd, src->omg, 48 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
+  if (!implicit)
+    CK(ctx, cudaMemcpyAsync(dst->omg + 3 * (size_t)nd, src->omg, 48 * (size_t)ns, cudaMemcpyDeviceToDevice, s));
   if (eig && dst->eig)
     CK(ctx, cudaMemcpyAsync(dst->eig + kStatsWords * (size_t)nd, src->eig, 4 * kStatsWords * (size_t)ns,
                             cudaMemcpyDeviceToDevice, s));
@@ -1764,6 +1799,7 @@ extern "C" int nicp_cloud_add(nicp_cloud *dst, nicp_cloud *src, const float T16[
   dst->eig_valid = eig && dst->eig;
   dst->gauss_valid = gauss && dst->gauss;
   dst->omega_structured = structured;
+  dst->omg_valid = !implicit;
   if (empty) std::memcpy(dst->omd, src->omd, sizeof(src->omd));
   return NICP_OK;
   NICP_ABI_CATCH
@@ -2046,6 +2082,10 @@ static int align_impl(nicp_ctx *ctx, const AlignCall &a, nicp_align_result *out)
   if ((rc = plan_pairs(ctx, a.n, a.cams, big.data(), keep_ref, list_mode, pl))) return rc;
   pl.structured = !list_mode;
   for (int i = 0; i < a.n && pl.structured; i++) pl.structured = a.curs[i] && a.curs[i]->omega_structured;
+  // the list linearizer reads the current clouds' matrices (the fused kernel
+  // rebuilds a structured cloud's Omega itself)
+  for (int i = 0; i < a.n && list_mode; i++)
+    if ((rc = cloud_ensure_omg(ctx, a.curs[i]))) return rc;
   size_t up = sizeof(PairDev) * a.n + 48 * (size_t)a.n + 256 * (size_t)a.n;
   char *pin;
   if ((rc = pin_up(ctx, up, &pin))) return rc;
@@ -2271,6 +2311,7 @@ int cloud_set_host_arrays(nicp_cloud *c, int n, const float *pts4, const float *
   c->eig_valid = true;
   c->gauss_valid = false;
   c->omega_structured = structured;
+  c->omg_valid = true;
   std::memcpy(c->omd, omd, sizeof(c->omd));
   return NICP_OK;
 }

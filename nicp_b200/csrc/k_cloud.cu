@@ -770,10 +770,16 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) k_stats(const FrameDev *__
   // (see kNoNormalW)
   reinterpret_cast<float *>(f.pts + idx)[3] =
       (nout.x != 0.0f || nout.y != 0.0f || nout.z != 0.0f) ? 1.0f + (float)omega_class : kNoNormalW;
-  float4 *o = f.omg + 3 * (size_t)idx;
-  o[0] = make_float4(om[0], om[1], om[2], om[3]);
-  o[1] = make_float4(om[4], om[5], om[6], om[7]);
-  o[2] = make_float4(om[8], om[9], om[10], om[11]);
+  // With the converter's structure the information matrices stay implicit:
+  // d1 I + (d0 - d1) n n^T from the normal, the class code in the point's w
+  // and the cloud's (d0, d1) per class (the fused kernel uses them so, and
+  // k_materialize_omg writes them out for a reader that needs the matrices).
+  if (!kLean) {
+    float4 *o = f.omg + 3 * (size_t)idx;
+    o[0] = make_float4(om[0], om[1], om[2], om[3]);
+    o[1] = make_float4(om[4], om[5], om[6], om[7]);
+    o[2] = make_float4(om[8], om[9], om[10], om[11]);
+  }
   if (f.keep_stats) {
     float *e = f.eig + kStatsWords * (size_t)idx;
     if (!reached) { lam[0] = lam[1] = lam[2] = 0; }
@@ -799,27 +805,30 @@ __global__ void k_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *
   float4 n0 = nrm[i];
   float3 n = xform_normal(A, n0);
   nrm[i] = make_float4(n.x, n.y, n.z, n0.w);
-  // Omega' = (R Omega) R^T over the 3x3 block
-  float4 o0 = omg[3 * i], o1 = omg[3 * i + 1], o2 = omg[3 * i + 2];
-  float Op[9] = {o0.x, o0.y, o0.z, o0.y, o0.w, o1.x, o0.z, o1.x, o1.y};
-  float On[9] = {o1.z, o1.w, o2.x, o1.w, o2.y, o2.z, o2.x, o2.z, o2.w};
+  // Omega' = (R Omega) R^T over the 3x3 block (an implicit Omega -- omg
+  // null -- follows the rotated normal by itself)
   float R[9] = {A[0], A[1], A[2], A[4], A[5], A[6], A[8], A[9], A[10]};
-  float res[2][6];
-  for (int w = 0; w < 2; w++) {
-    const float *O = w ? On : Op;
-    float RO[9];
-    for (int a = 0; a < 3; a++)
-      for (int b = 0; b < 3; b++)
-        RO[a * 3 + b] = fa(fa(fm(R[a * 3 + 0], O[0 * 3 + b]), fm(R[a * 3 + 1], O[1 * 3 + b])), fm(R[a * 3 + 2], O[2 * 3 + b]));
-    const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
-    for (int e = 0; e < 6; e++) {
-      int a = ii[e], b = jj[e];
-      res[w][e] = fa(fa(fm(RO[a * 3 + 0], R[b * 3 + 0]), fm(RO[a * 3 + 1], R[b * 3 + 1])), fm(RO[a * 3 + 2], R[b * 3 + 2]));
+  if (omg) {
+    float4 o0 = omg[3 * i], o1 = omg[3 * i + 1], o2 = omg[3 * i + 2];
+    float Op[9] = {o0.x, o0.y, o0.z, o0.y, o0.w, o1.x, o0.z, o1.x, o1.y};
+    float On[9] = {o1.z, o1.w, o2.x, o1.w, o2.y, o2.z, o2.x, o2.z, o2.w};
+    float res[2][6];
+    for (int w = 0; w < 2; w++) {
+      const float *O = w ? On : Op;
+      float RO[9];
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+          RO[a * 3 + b] = fa(fa(fm(R[a * 3 + 0], O[0 * 3 + b]), fm(R[a * 3 + 1], O[1 * 3 + b])), fm(R[a * 3 + 2], O[2 * 3 + b]));
+      const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
+      for (int e = 0; e < 6; e++) {
+        int a = ii[e], b = jj[e];
+        res[w][e] = fa(fa(fm(RO[a * 3 + 0], R[b * 3 + 0]), fm(RO[a * 3 + 1], R[b * 3 + 1])), fm(RO[a * 3 + 2], R[b * 3 + 2]));
+      }
     }
+    omg[3 * i] = make_float4(res[0][0], res[0][1], res[0][2], res[0][3]);
+    omg[3 * i + 1] = make_float4(res[0][4], res[0][5], res[1][0], res[1][1]);
+    omg[3 * i + 2] = make_float4(res[1][2], res[1][3], res[1][4], res[1][5]);
   }
-  omg[3 * i] = make_float4(res[0][0], res[0][1], res[0][2], res[0][3]);
-  omg[3 * i + 1] = make_float4(res[0][4], res[0][5], res[1][0], res[1][1]);
-  omg[3 * i + 2] = make_float4(res[1][2], res[1][3], res[1][4], res[1][5]);
   if (gauss) {
     // Gaussian3fVector::transformInPlace (gaussian3.h:66-73): mean' = R mean + t,
     // covariance' = (R C) R^T
@@ -1101,6 +1110,48 @@ __global__ void k_reset_normal_counts(const FrameDev *__restrict__ frames, int n
 
 void launch_reset_normal_counts(const FrameDev *d_frames, int nframes, cudaStream_t s) {
   if (nframes > 0) k_reset_normal_counts<<<(nframes + 127) / 128, 128, 0, s>>>(d_frames, nframes);
+}
+
+// The information matrices of a cloud whose Omega is implicit (built with
+// the converter's structure): per point with a normal n and class code c in
+// its w, Omega = d1 I + (d0 - d1) n n^T with (d0, d1) of c's flat / non-flat
+// point and normal calculators (omd: point flat, point non-flat, normal flat,
+// normal non-flat), evaluated in double and rounded once; zero for a point
+// without a normal (as the stats kernel leaves it).
+__global__ void k_materialize_omg(const float4 *__restrict__ pts, const float4 *__restrict__ nrm, float4 *omg,
+                                  const int *__restrict__ count, int capacity, OmegaParams op) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= capacity || i >= *count) return;
+  float om[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) om[k] = 0.0f;
+  const float w = pts[i].w;
+  if (point_has_normal(w)) {
+    const int cls = (int)w - 1;
+    const float *dp = op.omd + 2 * (cls & 1), *dn = op.omd + 4 + 2 * ((cls >> 1) & 1);
+    const float4 n = nrm[i];
+    const double u[3] = {(double)n.x, (double)n.y, (double)n.z};
+    const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int e = 0; e < 6; e++) {
+      const int a = ii[e], b = jj[e];
+      const double uu = u[a] * u[b];
+      om[e] = (float)((a == b ? (double)dp[1] : 0.0) + ((double)dp[0] - (double)dp[1]) * uu);
+      om[6 + e] = (float)((a == b ? (double)dn[1] : 0.0) + ((double)dn[0] - (double)dn[1]) * uu);
+    }
+  }
+  float4 *o = omg + 3 * (size_t)i;
+  o[0] = make_float4(om[0], om[1], om[2], om[3]);
+  o[1] = make_float4(om[4], om[5], om[6], om[7]);
+  o[2] = make_float4(om[8], om[9], om[10], om[11]);
+}
+
+void launch_materialize_omg(const float4 *pts, const float4 *nrm, float4 *omg, const int *count, int capacity,
+                            const float omd[8], cudaStream_t s) {
+  OmegaParams op;
+  for (int k = 0; k < 8; k++) op.omd[k] = omd[k];
+  const int blocks = (capacity + 255) / 256;
+  if (blocks > 0) k_materialize_omg<<<blocks, 256, 0, s>>>(pts, nrm, omg, count, capacity, op);
 }
 
 void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,

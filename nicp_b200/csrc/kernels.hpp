@@ -87,6 +87,13 @@ int stats_shape_min_ctas(int shape);
 void launch_stats(int precision, const FrameDev *d_frames, int nframes, int max_pixels, int shape, bool lean,
                   cudaStream_t s, Profiler *prof);
 void launch_reset_normal_counts(const FrameDev *d_frames, int nframes, cudaStream_t s);
+struct OmegaParams {
+  float omd[8];  // (d0, d1) of point flat, point non-flat, normal flat, normal non-flat
+};
+// Writes the information matrices of a cloud whose Omega is implicit.
+void launch_materialize_omg(const float4 *pts, const float4 *nrm, float4 *omg, const int *count, int capacity,
+                            const float omd[8], cudaStream_t s);
+// omg may be null: an implicit Omega follows the rotated normal by itself.
 void launch_cloud_transform(float4 *pts, float4 *nrm, float4 *omg, float *eig, float4 *gauss, const int *count,
                             int capacity, const float *d_m12, cudaStream_t s, Profiler *prof);
 size_t moment_bytes(int precision);
