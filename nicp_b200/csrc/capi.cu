@@ -47,6 +47,7 @@ struct Layout {
 struct nicp_ctx {
   int device = 0;
   int sm_count = 148;
+  int sweep_ctas_per_sm[3] = {0, 0, 0};  // per moment precision, queried on first use
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string err;
@@ -769,7 +770,18 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   cudaStream_t s = ctx->stream;
   const size_t msz = moment_bytes(prm->moments_precision);
   const size_t kChunkMoments = (size_t)3 << 30;  // bytes of integral image per chunk
-  const int kStreamChunkFrames = 32, kStreamFirstChunkFrames = 8;
+  // host frames are built in chunks sized to whole waves of the band sweep
+  // (one CTA per 16-row band and frame): the first chunk one wave, so that
+  // the kernels start after a few frames' copies, the others the number of
+  // waves closest to 32 frames (640x480: 14, then 29 frames)
+  const int prec = std::min(std::max(prm->moments_precision, 0), 2);
+  if (!ctx->sweep_ctas_per_sm[prec]) ctx->sweep_ctas_per_sm[prec] = moment_sweep_ctas_per_sm(prm->moments_precision);
+  const long long wave = (long long)ctx->sweep_ctas_per_sm[prec] * ctx->sm_count;
+  auto stream_chunk = [&](int i0, bool first) {
+    const int bands = std::max(1, (fin[i0].rows + moment_band_rows() - 1) / moment_band_rows());
+    const long long k = first ? 1 : std::max(1LL, (32LL * bands + wave / 2) / wave);
+    return (int)std::max(1LL, std::min(65535LL, k * wave / bands));
+  };
   int rc;
   for (int i = 0; i < n; i++) {
     if (!fin[i].depth || fin[i].rows <= 0 || fin[i].cols <= 0 || !clouds[i] || !valid_camera(&cams[i]))
@@ -799,8 +811,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
     // with host frames the first chunk is short, so the kernels start after
     // a few frames' copies
     // (frames per launch are the grids' y dimension: at most 65535)
-    const int max_frames =
-        std::min(65535, !any_host ? n : (i0 == 0 ? kStreamFirstChunkFrames : kStreamChunkFrames));
+    const int max_frames = std::min(65535, !any_host ? n : stream_chunk(i0, i0 == 0));
     int i1 = i0;
     size_t mom = 0;
     while (i1 < n && i1 - i0 < max_frames) {

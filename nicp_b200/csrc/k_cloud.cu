@@ -1064,6 +1064,24 @@ void launch_moments(int precision, const FrameDev *d_frames, int nframes, int to
                          prof);
 }
 
+template <class M>
+static int sweep_occupancy() {
+  configure_bands<M>();
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_moments_band_sweep<M>, kRowThreads, band_smem_bytes<M>()) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  return n > 0 ? n : 1;
+}
+
+int moment_sweep_ctas_per_sm(int precision) {
+  if (precision == NICP_MOMENTS_F32) return sweep_occupancy<MomF32>();
+  if (precision == NICP_MOMENTS_TWOFLOAT) return sweep_occupancy<MomTwoFloat>();
+  return sweep_occupancy<MomF64>();
+}
+
 // Stats launch shapes: (threads per CTA, CTAs per SM of the register budget).
 #ifdef NICP_STATS_WIDE_DEFAULT
 static const int kStatsShape[kStatsShapes][2] = {{256, 2}, {128, 6}, {64, 12}, {256, 3}};

@@ -74,6 +74,9 @@ int moment_band_rows();
 // sweeping the bands; the planes are bitwise the same.
 bool moments_row_path(int nframes);
 size_t moment_acc_bytes(int precision);
+// Resident band-sweep CTAs per SM (one per 16-row band and frame): frame
+// chunks of whole waves of them leave no half-empty last wave.
+int moment_sweep_ctas_per_sm(int precision);
 void launch_moments(int precision, const FrameDev *d_frames, int nframes, int total_bands, int total_carry_ctas,
                     int max_bands, const int *frame_of_band, const int *frame_of_carry, cudaStream_t s,
                     Profiler *prof);
