@@ -57,6 +57,9 @@
  *     several GPUs.  The one exception is nicp_linearize_noalloc, which
  *     switches nothing and refuses a call whose context's device is not
  *     current (NICP_ESTATE).
+ *   - A cloud is not thread-safe either: calls that read a cloud may write
+ *     out its implicit information matrices (see nicp_cloud_download), so
+ *     two threads must not use one cloud at the same time.
  *   - The library's per-device state (kernel attributes set once per
  *     device, the allocation-free linearizer's array address) does not
  *     survive cudaDeviceReset: destroy every context and server first, and
