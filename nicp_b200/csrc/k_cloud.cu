@@ -345,8 +345,11 @@ constexpr int kRowPix = 5;  // 128 x 5 = 640: one chunk per 640-pixel row
 // keeps the points of its kRowPix pixels (depths d[]); the moments are
 // formed twice (for the thread total, then per pixel for emit) to keep
 // register use low.  emit(k, c, acc) receives pixel c = x0 + t kRowPix + k
-// with its 10 prefix values.  Contains two __syncthreads.
-template <class M, class Emit>
+// with its 10 prefix values.  [kM0, kM0 + kNM) selects the moments the call
+// scans (the band sweep runs two calls of five, which halves the registers
+// the pixels' moments hold and fits 4 CTAs per SM; every moment's additions
+// are the same either way).  Contains two __syncthreads.
+template <class M, int kM0 = 0, int kNM = 10, class Emit>
 __device__ __forceinline__ void row_chunk_scan(const FrameDev &f, int r, int x0, const float d[kRowPix],
                                                typename MomAcc<M>::T carry[10],
                                                typename MomAcc<M>::T (*wtot)[10], Emit &&emit) {
@@ -358,7 +361,7 @@ __device__ __forceinline__ void row_chunk_scan(const FrameDev &f, int r, int x0,
   unsigned vmask = 0;
   A acc[10];
 #pragma unroll
-  for (int m = 0; m < 10; m++) acc[m] = A(0);
+  for (int m = kM0; m < kM0 + kNM; m++) acc[m] = A(0);
 #pragma unroll
   for (int k = 0; k < kRowPix; k++) {
     const int c = c0 + k;
@@ -368,11 +371,11 @@ __device__ __forceinline__ void row_chunk_scan(const FrameDev &f, int r, int x0,
     A mk[10];
     point_moments(pt[k], valid, mk);
 #pragma unroll
-    for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
+    for (int m = kM0; m < kM0 + kNM; m++) acc[m] = acc[m] + mk[m];
   }
   // warp inclusive scan of the thread totals; acc becomes the exclusive offset
 #pragma unroll
-  for (int m = 0; m < 10; m++) {
+  for (int m = kM0; m < kM0 + kNM; m++) {
     A inc = acc[m];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -384,7 +387,7 @@ __device__ __forceinline__ void row_chunk_scan(const FrameDev &f, int r, int x0,
   }
   __syncthreads();
 #pragma unroll
-  for (int m = 0; m < 10; m++) {
+  for (int m = kM0; m < kM0 + kNM; m++) {
     A off = carry[m] + acc[m], tot = A(0);
     for (int w = 0; w < kRowThreads / 32; w++) {
       A t = wtot[w][m];
@@ -400,7 +403,7 @@ __device__ __forceinline__ void row_chunk_scan(const FrameDev &f, int r, int x0,
     A mk[10];
     point_moments(pt[k], (vmask >> k) & 1u, mk);
 #pragma unroll
-    for (int m = 0; m < 10; m++) acc[m] = acc[m] + mk[m];
+    for (int m = kM0; m < kM0 + kNM; m++) acc[m] = acc[m] + mk[m];
     emit(k, c0 + k, acc);
   }
 }
@@ -560,7 +563,7 @@ __global__ void __launch_bounds__(128) k_moments_band_carry(const FrameDev *__re
 // Grid (band, frame): the frame is blockIdx.y, no search over the frame
 // descriptors; CTAs past a smaller frame's last band return at once.
 template <class M>
-__global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const FrameDev *__restrict__ frames, int nframes) {
+__global__ void __launch_bounds__(kRowThreads, 4) k_moments_band_sweep(const FrameDev *__restrict__ frames, int nframes) {
   typedef typename MomAcc<M>::T A;
   extern __shared__ __align__(16) unsigned char band_raw[];
   A *state = reinterpret_cast<A *>(band_raw);  // [10][kChunkPix]: I(r, c) of the current row
@@ -598,10 +601,17 @@ __global__ void __launch_bounds__(kRowThreads, 3) k_moments_band_sweep(const Fra
       for (int m = 0; m < 10; m++) carry[m] = x0 ? rowc[r - r0][m] : A(0);
       // every thread has finished the previous row's copy-out once it has
       // passed the first barrier inside the scan
-      row_chunk_scan<M>(f, r, x0, d, carry, wtot, [&](int, int c, const A *acc) {
+      row_chunk_scan<M, 0, 5>(f, r, x0, d, carry, wtot, [&](int, int c, const A *acc) {
         if (c < cols) {
 #pragma unroll
-          for (int m = 0; m < 10; m++)
+          for (int m = 0; m < 5; m++)
+            state[m * kChunkPix + (c - x0)] = state[m * kChunkPix + (c - x0)] + acc[m];
+        }
+      });
+      row_chunk_scan<M, 5, 5>(f, r, x0, d, carry, wtot, [&](int, int c, const A *acc) {
+        if (c < cols) {
+#pragma unroll
+          for (int m = 5; m < 10; m++)
             state[m * kChunkPix + (c - x0)] = state[m * kChunkPix + (c - x0)] + acc[m];
         }
       });
