@@ -119,3 +119,27 @@ def test_list_linearizer_on_implicit_and_explicit_clouds(ctx):
     # at the true pose b is the small remainder of cancelling terms: bound
     # the Gauss-Newton step it gives instead
     assert np.abs(np.linalg.solve(Hb, ba - bb)).max() < 1e-7
+
+
+def test_merge_keeps_implicit_omega_consistent(ctx):
+    """The merger moves points inside a cloud (its information matrices move
+    with them, or stay implicit): implicit and explicit twins merged the same
+    way give the same points and normals, and Omega a few ulps apart."""
+    d1, _, _, cam = synth.render_pair(36, "320x240")
+    out = []
+    for keep in (False, True):
+        proj, conv = converter(cam, ctx, keep_stats=keep)
+        conv.keepGaussians = True
+        a, b = api.Cloud(ctx), api.Cloud(ctx)
+        conv.compute(a, d1)
+        conv.compute(b, d1)
+        a.add(b, np.eye(4))
+        m = api.Merger(ctx)
+        m.setDepthImageConverter(conv)
+        m.setImageSize(cam["rows"], cam["cols"])
+        m.merge(a, np.eye(4))
+        assert m.removed > 0
+        out.append((a.download(), m.removed))
+    (da, ra), (db, rb) = out
+    assert ra == rb
+    _check_same_omega(da, db, 1e-6)
