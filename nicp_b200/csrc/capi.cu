@@ -942,8 +942,9 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
       cl->gauss_valid = d.gauss != nullptr;
       cl->omega_structured = prm->pim_flat[1] == prm->pim_flat[2] && prm->pim_nonflat[1] == prm->pim_nonflat[2] &&
                              prm->nim_flat[1] == prm->nim_flat[2] && prm->nim_nonflat[1] == prm->nim_nonflat[2];
-      // the stats kernel's lean form (below) leaves Omega implicit
-      if (!unproject_only) cl->omg_valid = !(!prm->keep_stats && cl->omega_structured);
+      // the stats kernel's lean form (below) leaves Omega implicit; an
+      // unprojection-only build writes no normals or matrices at all
+      cl->omg_valid = unproject_only || !(!prm->keep_stats && cl->omega_structured);
       {
         const float od[8] = {prm->pim_flat[0], prm->pim_flat[1], prm->pim_nonflat[0], prm->pim_nonflat[1],
                              prm->nim_flat[0], prm->nim_flat[1], prm->nim_nonflat[0], prm->nim_nonflat[1]};
