@@ -773,7 +773,7 @@ static int build_frames(nicp_ctx *ctx, int n, const FrameIn *fin, const nicp_cam
   // host frames are built in chunks sized to whole waves of the band sweep
   // (one CTA per 16-row band and frame): the first chunk one wave, so that
   // the kernels start after a few frames' copies, the others the number of
-  // waves closest to 32 frames (640x480: 14, then 29 frames)
+  // waves closest to 32 frames (640x480 at 4 sweep CTAs per SM: 19, then 39)
   const int prec = std::min(std::max(prm->moments_precision, 0), 2);
   if (!ctx->sweep_ctas_per_sm[prec]) ctx->sweep_ctas_per_sm[prec] = moment_sweep_ctas_per_sm(prm->moments_precision);
   const long long wave = (long long)ctx->sweep_ctas_per_sm[prec] * ctx->sm_count;
