@@ -654,7 +654,10 @@ __global__ void __launch_bounds__(kFusedThreads, kStructured ? NICP_CORR_S_CTAS 
               const unsigned lo = (unsigned)zI[k];
               ri = (drop_no_normal && (lo & 1u)) ? -1 : (int)(lo >> 1);
               ci[k] = cI[k];
-              if (flags & 2) pd.zbuf[p] = ~0ull;
+              // evict-first: the word is read again only by the next
+              // projection, long after it would have left L2, where it
+              // would displace the gathered clouds
+              if (flags & 2) __stcs(pd.zbuf + p, ~0ull);
               if (flags & 4) pd.ref_index[p] = ri;
             } else {
               ri = cI[k];
